@@ -1,0 +1,222 @@
+/*
+ * ndyn_gpu.h -- C ABI of the B200 (sm_100a) Ndyn timestep library.
+ *
+ * Drop-in boundary for the MD timestep path of Ndyn (stewmasterj/Ndyn_OMP).
+ * The reference has no FFI: its timestep routines are argument-less Fortran
+ * subroutines working on module globals (src/mods.f90).  Each entry point
+ * below replaces one of them and takes the module data explicitly, as plain
+ * pointers and sizes in the reference's own layouts:
+ *
+ *   pos(3,np), vel(3,np), acc(3,np), force(3,np)  real(8), column-major
+ *        (x,y,z of one atom contiguous); pos is fractional, in box units
+ *   typ(np)                integer(4), 1-based type ids
+ *   PairMat(ntypes,ntypes) integer(4), column-major, 1-based pair ids, 0=none
+ *   PPairTable/FPairTable(PTsize+1,NPairs) real(8), column-major
+ *   box(3), virial(6)      real(8)
+ *
+ * A context (ndg_ctx) owns the device copy of one or more independent
+ * systems ("replicas"); system ids are small integers.  Every call returns
+ * an int status: NDG_OK (0) or a negative NDG_ERR_* code, where the
+ * reference would STOP.  Calls on one context are not thread-safe;
+ * separate contexts are independent.  Host arrays are caller-owned and are
+ * copied in or out during the call.
+ *
+ * Fortran binds these with ISO_C_BINDING interface blocks (bind(C,name=...),
+ * value arguments for scalars, type(c_ptr) for the context).
+ */
+#ifndef NDYN_GPU_H
+#define NDYN_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NDG_ABI_VERSION 1
+
+/* status codes */
+enum {
+  NDG_OK = 0,
+  NDG_ERR_ARG = -1,        /* bad argument or call order */
+  NDG_ERR_NEIMAX = -2,     /* 'too many neighbours in list' src/nd.f90:1378,1421 */
+  NDG_ERR_OUT_OF_BOX = -3, /* 'Particle outside of box' src/nd.f90:1494 */
+  NDG_ERR_POTENTIAL = -4,  /* unknown potential name src/potentials.f90:148,244 */
+  NDG_ERR_CELLS = -5,      /* fewer than 2 link cells in a direction
+                              (box < 2*(rcut+skin): the single-anint minimum
+                              image of src/nd.f90:283-288 is then invalid) */
+  NDG_ERR_NOMEM = -6,      /* device allocation failed */
+  NDG_ERR_CUDA = -7,       /* CUDA runtime error (see ndg_last_error) */
+  NDG_ERR_BUDGET = -8,     /* request does not fit the HBM budget */
+  NDG_ERR_NOT_FOUND = -9,  /* unknown system or request id */
+  NDG_ERR_TIMEOUT = -10    /* bounded wait expired */
+};
+
+/* arithmetic of the pair loop */
+enum {
+  NDG_PREC_FP64 = 0,  /* the reference's FP64 path (FP32 table index only) */
+  NDG_PREC_MIXED = 1  /* FP32 pair math on 32-bit fixed-point fractional
+                         positions, 64-bit fixed-point force sums, FP64
+                         integrator, reductions and box */
+};
+
+/* list semantics */
+enum {
+  NDG_QUIRK_REF = 0,   /* exactly the reference: list rebuild test compares
+                          fractional displacements with skin^2 in A^2
+                          (src/nd.f90:1488-1493), and the 14-cell half
+                          stencil repeats pairs when a cell count is 2
+                          (src/nd.f90:1268-1300) */
+  NDG_QUIRK_FIXED = 1  /* rebuild when the two largest displacements (A)
+                          plus any box shrink exceed the skin; each distinct
+                          neighbour cell visited once */
+};
+
+typedef struct ndg_ctx ndg_ctx;
+
+/* Run control; the values of module 'control' and 'listData'
+ * (src/mods.f90:79-95) with the defaults of src/read_input.f90:18-41. */
+typedef struct {
+  double dt;            /* time step (Run [i] {r}) */
+  double skin;          /* Skin; < 0 means 0.2*rcut at run start (src/nd.f90:77-79) */
+  int neimax;           /* NeiMax; 0 = estimate (src/nd.f90:84-88) */
+  int renei;            /* ReNeighbor T/F */
+  int renei_freq;       /* check interval */
+  int out_steps;        /* OutFreq */
+  int step;             /* global step counter (StepNumber) */
+  int isokinetic, ke_freq;
+  double ke_target, ke_parm;
+  int isobaric, p_freq;
+  double p_target[3], p_parm;
+  int isoenergetic, e_freq;
+  double e_parm;
+  int box_load;
+  double box_vel[3];
+  int quirk;            /* NDG_QUIRK_* */
+} ndg_control;
+
+/* One write_thermo record (src/read_input.f90:433-446), plus the raw
+ * virial and box. */
+typedef struct {
+  int sys;
+  int step;
+  double potential, kinetic, energy_error, pressure, volume;
+  double virial[6];
+  double box[3];
+} ndg_thermo;
+
+typedef void (*ndg_thermo_cb)(const ndg_thermo *t, void *user);
+
+/* ---- library ---------------------------------------------------------- */
+int ndg_abi_version(void);
+const char *ndg_error_string(int status);
+/* last CUDA error text recorded on ctx (or globally when ctx is NULL) */
+const char *ndg_last_error(const ndg_ctx *ctx);
+
+/* Host restatement of buildPairTables + pot/dpot (src/potentials.f90:2-247)
+ * for callers that do not tabulate themselves (the C++ driver).  names are
+ * npairs blocks of 8 characters (blank- or NUL-padded), params 4*npairs
+ * (PairParams(1:4,j), PairParams(1,j) = cutoff), qprod the charge products
+ * (may be NULL).  Outputs: ppair/fpair (ptsize+1)*npairs, rc2/dr2 npairs. */
+int ndg_build_pair_tables(int npairs, int ptsize, double ptrmin,
+                          const char *names, const double *params,
+                          const double *qprod, double *ppair, double *fpair,
+                          double *rc2, double *dr2);
+
+/* ---- context and systems --------------------------------------------- */
+int ndg_create(ndg_ctx **ctx, int device, int precision);
+int ndg_destroy(ndg_ctx *ctx);
+int ndg_set_precision(ndg_ctx *ctx, int precision);
+
+/* Add a system: the interpot module (src/mods.f90:51-77) for it plus its
+ * atoms.  rcpair = PairParams(1,1:npairs).  Tables are copied.  Returns the
+ * new id in *sys.  vel/acc may be NULL (zero, as read_model leaves them,
+ * src/read_input.f90:354-355). */
+int ndg_add_system(ndg_ctx *ctx, int np, int ntypes, int npairs, int ptsize,
+                   double ptrmin, const double *mass, const int *pairmat,
+                   const double *rcpair, const double *ppair,
+                   const double *fpair, const int *typ, const double *pos,
+                   const double *vel, const double *acc, const double *box,
+                   int *sys);
+int ndg_remove_system(ndg_ctx *ctx, int sys);
+int ndg_num_systems(const ndg_ctx *ctx);
+
+/* replace positions/velocities/accelerations/box of a system */
+int ndg_load_state(ndg_ctx *ctx, int sys, const double *pos, const double *vel,
+                   const double *acc, const double *box);
+int ndg_get_state(ndg_ctx *ctx, int sys, double *pos, double *vel, double *acc,
+                  double *box);
+int ndg_set_control(ndg_ctx *ctx, int sys, const ndg_control *c);
+int ndg_get_control(ndg_ctx *ctx, int sys, ndg_control *c);
+void ndg_default_control(ndg_control *c);
+
+/* ---- the reference routines, one call each (all systems of ctx) -------- */
+/* dynamics prologue src/nd.f90:73-108: skin default, link-cell counts,
+ * neighbour capacity, cell list + Verlet list build */
+int ndg_setup_lists(ndg_ctx *ctx);
+/* buildCellList + buildVerletList, src/nd.f90:1214-1446 */
+int ndg_build_cell_list(ndg_ctx *ctx);
+/* CheckListUpdate, src/nd.f90:1447-1499; *rebuilt (may be NULL) gets the
+ * number of systems whose lists were rebuilt */
+int ndg_check_list_update(ndg_ctx *ctx, int *rebuilt);
+/* integrate1, src/nd.f90:984-1047 */
+int ndg_integrate1(ndg_ctx *ctx);
+/* compute0(CV,CU), src/nd.f90:200-363 */
+int ndg_compute(ndg_ctx *ctx, int cv, int cu);
+/* integrate2(CK), src/nd.f90:1081-1121 */
+int ndg_integrate2(ndg_ctx *ctx, int ck);
+/* mkIsoKE / mkIsoE / mkIsoP, src/nd.f90:1122-1213, on system sys */
+int ndg_mk_iso_ke(ndg_ctx *ctx, int sys);
+int ndg_mk_iso_e(ndg_ctx *ctx, int sys);
+int ndg_mk_iso_p(ndg_ctx *ctx, int sys);
+
+/* force(3,np), potential, virial(6), kinetic of the last compute/integrate */
+int ndg_get_forces(ndg_ctx *ctx, int sys, double *force, double *potential,
+                   double *virial, double *kinetic);
+
+/* ---- the dynamics loop ------------------------------------------------- */
+/* The time-step loop of dynamics (src/nd.f90:137-180) for nsteps steps on
+ * every system, fused on the device (CUDA graphs of fixed step blocks).
+ * Lists are rebuilt at the start (as dynamics does).  cb (may be NULL)
+ * receives every write_thermo record in step order. */
+int ndg_run(ndg_ctx *ctx, int nsteps, ndg_thermo_cb cb, void *user);
+/* Same loop without the prologue list build: continues a run. */
+int ndg_run_continue(ndg_ctx *ctx, int nsteps, ndg_thermo_cb cb, void *user);
+/* thermo scalars of the last completed step of a system */
+int ndg_get_thermo(ndg_ctx *ctx, int sys, ndg_thermo *t);
+/* number of list rebuilds since the run started (NlistUpdates) */
+int ndg_get_list_updates(ndg_ctx *ctx, int sys, int *n);
+
+/* ---- inspection (tests) ------------------------------------------------ */
+/* link-cell counts MCELL(3) */
+int ndg_get_mcell(ndg_ctx *ctx, int sys, int *mcell);
+/* 0-based cell id (ICELL-1) of each atom, in the caller's atom order */
+int ndg_get_cells(ndg_ctx *ctx, int sys, int *cell);
+/* neighbour pairs (i<j, 0-based, caller's atom order): one entry per
+ * occurrence of the unordered pair in the reference's half list.  With
+ * pairs == NULL returns the count in *npairs. */
+int ndg_get_neighbors(ndg_ctx *ctx, int sys, int *pairs, long long cap,
+                      long long *npairs);
+
+/* ---- tuning ------------------------------------------------------------ */
+/* threads per atom in the pair kernel (1,2,4,8,16,32; 0 = choose from the
+ * mean neighbour count) and steps per CUDA-graph block */
+int ndg_set_tuning(ndg_ctx *ctx, int threads_per_atom, int graph_steps);
+int ndg_get_tuning(ndg_ctx *ctx, int *threads_per_atom, int *graph_steps);
+/* time candidate launch shapes on the current systems for a few steps and
+ * keep the fastest (state is restored afterwards) */
+int ndg_autotune(ndg_ctx *ctx, int steps_per_trial);
+/* device bytes the context holds, and the bytes one more system of np
+ * atoms with ntypes/npairs/ptsize would need */
+int ndg_device_bytes(const ndg_ctx *ctx, long long *bytes);
+long long ndg_system_bytes(int np, int ntypes, int npairs, int ptsize,
+                           double density, double rlist, int precision);
+
+/* per-kernel timing of the last ndg_run block (ms, CUDA events) */
+int ndg_get_kernel_times(ndg_ctx *ctx, double *integrate_ms, double *pair_ms,
+                         double *rebuild_ms, int *launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NDYN_GPU_H */

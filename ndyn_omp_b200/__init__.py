@@ -1,0 +1,11 @@
+"""B200-native (sm_100a) implementation of Ndyn's MD timestep path.
+
+The compute path is the CUDA library ndyn_omp_b200/lib/libndyn_gpu.so
+(C ABI: include/ndyn_gpu.h); this package is its Python host mirror.
+"""
+from ._lib import LIB_PATH, lib  # noqa: F401
+from .api import (Context, Control, NdgError, Thermo, build_pair_tables,  # noqa: F401
+                  pair_matrix)
+
+__all__ = ["Context", "Control", "NdgError", "Thermo", "build_pair_tables", "pair_matrix",
+           "lib", "LIB_PATH"]

@@ -1,0 +1,296 @@
+"""Python mirror of the Ndyn timestep interface over the C ABI (ndyn_gpu.h).
+
+The reference's timestep routines are Fortran subroutines on module state
+(stewmasterj/Ndyn_OMP src/nd.f90).  `Context` holds that state on the GPU
+for one or more independent systems and exposes one method per routine,
+with the reference's names and flag arguments:
+
+    ctx.setup_lists()          dynamics prologue     src/nd.f90:73-108
+    ctx.build_cell_list()      buildCellList         src/nd.f90:1214-1260
+    ctx.check_list_update()    CheckListUpdate       src/nd.f90:1447-1499
+    ctx.integrate1()           integrate1            src/nd.f90:984-1080
+    ctx.compute0(cv, cu)       compute0(CV,CU)       src/nd.f90:200-363
+    ctx.integrate2(ck)         integrate2(CK)        src/nd.f90:1081-1121
+    ctx.mk_iso_ke/e/p(sys)     mkIsoKE/mkIsoE/mkIsoP src/nd.f90:1122-1213
+    ctx.run(nsteps)            the dynamics loop     src/nd.f90:137-180
+
+Errors the reference reports with STOP raise NdgError with the library's
+status code.  Everything runs in the CUDA library; there is no CPU path.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import _lib as L
+
+PREC = {"fp64": 0, "mixed": 1}
+QUIRK = {"ref": 0, "fixed": 1}
+
+
+class NdgError(RuntimeError):
+    def __init__(self, status, what=""):
+        lib = L.lib()
+        msg = lib.ndg_error_string(status).decode()
+        detail = lib.ndg_last_error(None).decode() if status == -7 else ""
+        super().__init__(f"{what}: {msg} ({status}) {detail}".strip())
+        self.status = status
+
+
+def _ok(status, what=""):
+    if status != 0:
+        raise NdgError(status, what)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def build_pair_tables(pairs, ptsize=1000, ptrmin=0.25, charges=None):
+    """buildPairTables (src/potentials.f90:2-56) for a list of pair specs.
+
+    pairs: sequence of (type_i, type_j, sym, name, params) with 1-based
+    types and params = [rc, p2, p3, p4] as on a 'Pairs' line.  Returns
+    (ppair, fpair, rc2, dr2) with the reference's (PTsize+1, NPairs)
+    column-major tables flattened."""
+    n = len(pairs)
+    names = b"".join(p[3].encode().ljust(8)[:8] for p in pairs)
+    par = np.zeros((n, 4))
+    for k, p in enumerate(pairs):
+        par[k, :len(p[4])] = p[4]
+    q = None
+    if charges is not None:
+        q = np.array([charges[p[0] - 1] * charges[p[1] - 1] for p in pairs], np.float64)
+    pp = np.zeros((ptsize + 1) * n)
+    fp = np.zeros((ptsize + 1) * n)
+    rc2 = np.zeros(n)
+    dr2 = np.zeros(n)
+    _ok(L.lib().ndg_build_pair_tables(n, ptsize, float(ptrmin), names, _p(par), _p(q), _p(pp),
+                                      _p(fp), _p(rc2), _p(dr2)), "build_pair_tables")
+    return pp, fp, rc2, dr2
+
+
+def pair_matrix(pairs, ntypes):
+    """PairMat(ntypes,ntypes), column-major, as the 'Pairs' directive fills
+    it (src/read_input.f90:159-164)."""
+    pm = np.zeros((ntypes, ntypes), np.int32)  # pm[a-1, b-1] = PairMat(a,b)
+    for k, p in enumerate(pairs):
+        pm[p[0] - 1, p[1] - 1] = k + 1
+        if p[2]:
+            pm[p[1] - 1, p[0] - 1] = k + 1
+    return np.asfortranarray(pm).ravel(order="F")
+
+
+class Control(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_double), ("skin", ctypes.c_double),
+                ("neimax", ctypes.c_int), ("renei", ctypes.c_int),
+                ("renei_freq", ctypes.c_int), ("out_steps", ctypes.c_int),
+                ("step", ctypes.c_int),
+                ("isokinetic", ctypes.c_int), ("ke_freq", ctypes.c_int),
+                ("ke_target", ctypes.c_double), ("ke_parm", ctypes.c_double),
+                ("isobaric", ctypes.c_int), ("p_freq", ctypes.c_int),
+                ("p_target", ctypes.c_double * 3), ("p_parm", ctypes.c_double),
+                ("isoenergetic", ctypes.c_int), ("e_freq", ctypes.c_int),
+                ("e_parm", ctypes.c_double),
+                ("box_load", ctypes.c_int), ("box_vel", ctypes.c_double * 3),
+                ("quirk", ctypes.c_int)]
+
+
+class Thermo(ctypes.Structure):
+    _fields_ = [("sys", ctypes.c_int), ("step", ctypes.c_int),
+                ("potential", ctypes.c_double), ("kinetic", ctypes.c_double),
+                ("energy_error", ctypes.c_double), ("pressure", ctypes.c_double),
+                ("volume", ctypes.c_double), ("virial", ctypes.c_double * 6),
+                ("box", ctypes.c_double * 3)]
+
+    def as_dict(self):
+        return dict(sys=self.sys, step=self.step, pe=self.potential, ke=self.kinetic,
+                    eerr=self.energy_error, press=self.pressure, vol=self.volume,
+                    virial=list(self.virial), box=list(self.box))
+
+
+THERMO_CB = ctypes.CFUNCTYPE(None, ctypes.POINTER(Thermo), ctypes.c_void_p)
+
+
+class Context:
+    """A GPU context holding one or more independent systems."""
+
+    def __init__(self, device=0, precision="fp64"):
+        self.L = L.lib()
+        self._c = ctypes.c_void_p()
+        _ok(self.L.ndg_create(ctypes.byref(self._c), int(device), PREC[precision]), "create")
+        self.systems = {}
+
+    def close(self):
+        if self._c:
+            self.L.ndg_destroy(self._c)
+            self._c = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- systems ---------------------------------------------------------
+    def add_system(self, masses, pairs, typ, pos, box, vel=None, acc=None, ptsize=1000,
+                   ptrmin=0.25, charges=None, tables=None):
+        """Add one system; pairs as for build_pair_tables, pos (np,3)
+        fractional.  tables=(ppair, fpair) supplies the caller's own tables."""
+        masses = np.ascontiguousarray(masses, np.float64)
+        nt = len(masses)
+        if tables is None:
+            pp, fp, _, _ = build_pair_tables(pairs, ptsize, ptrmin, charges)
+        else:
+            pp, fp = (np.ascontiguousarray(t, np.float64) for t in tables)
+        pm = pair_matrix(pairs, nt)
+        rcp = np.array([p[4][0] for p in pairs], np.float64)
+        typ = np.ascontiguousarray(typ, np.int32)
+        pos = np.ascontiguousarray(pos, np.float64).reshape(-1)
+        vel = None if vel is None else np.ascontiguousarray(vel, np.float64).reshape(-1)
+        acc = None if acc is None else np.ascontiguousarray(acc, np.float64).reshape(-1)
+        box = np.ascontiguousarray(box, np.float64)
+        sid = ctypes.c_int()
+        _ok(self.L.ndg_add_system(self._c, len(typ), nt, len(pairs), int(ptsize), float(ptrmin),
+                                  _p(masses), _p(pm), _p(rcp), _p(pp), _p(fp), _p(typ), _p(pos),
+                                  _p(vel), _p(acc), _p(box), ctypes.byref(sid)), "add_system")
+        self.systems[sid.value] = len(typ)
+        return sid.value
+
+    def remove_system(self, sys):
+        _ok(self.L.ndg_remove_system(self._c, sys), "remove_system")
+        self.systems.pop(sys, None)
+
+    def control(self, sys=0):
+        c = Control()
+        _ok(self.L.ndg_get_control(self._c, sys, ctypes.byref(c)), "get_control")
+        return c
+
+    def set_control(self, sys=0, **kw):
+        c = self.control(sys)
+        for k, v in kw.items():
+            if k == "quirk" and isinstance(v, str):
+                v = QUIRK[v]
+            if k in ("p_target", "box_vel"):
+                for q in range(3):
+                    getattr(c, k)[q] = v[q]
+            else:
+                setattr(c, k, v)
+        _ok(self.L.ndg_set_control(self._c, sys, ctypes.byref(c)), "set_control")
+
+    def load_state(self, sys, pos, vel=None, acc=None, box=None):
+        pos = np.ascontiguousarray(pos, np.float64).reshape(-1)
+        vel = None if vel is None else np.ascontiguousarray(vel, np.float64).reshape(-1)
+        acc = None if acc is None else np.ascontiguousarray(acc, np.float64).reshape(-1)
+        box = None if box is None else np.ascontiguousarray(box, np.float64)
+        _ok(self.L.ndg_load_state(self._c, sys, _p(pos), _p(vel), _p(acc), _p(box)), "load_state")
+
+    def state(self, sys=0):
+        n = self.systems[sys]
+        pos, vel, acc, box = np.zeros(3 * n), np.zeros(3 * n), np.zeros(3 * n), np.zeros(3)
+        _ok(self.L.ndg_get_state(self._c, sys, _p(pos), _p(vel), _p(acc), _p(box)), "get_state")
+        return pos.reshape(n, 3), vel.reshape(n, 3), acc.reshape(n, 3), box
+
+    def forces(self, sys=0):
+        n = self.systems[sys]
+        f = np.zeros(3 * n)
+        pe, ke = ctypes.c_double(), ctypes.c_double()
+        vir = np.zeros(6)
+        _ok(self.L.ndg_get_forces(self._c, sys, _p(f), ctypes.byref(pe), _p(vir),
+                                  ctypes.byref(ke)), "get_forces")
+        return f.reshape(n, 3), pe.value, vir, ke.value
+
+    # -- the reference routines ---------------------------------------------
+    def setup_lists(self):
+        _ok(self.L.ndg_setup_lists(self._c), "setup_lists")
+
+    def build_cell_list(self):
+        _ok(self.L.ndg_build_cell_list(self._c), "build_cell_list")
+
+    def check_list_update(self):
+        n = ctypes.c_int()
+        _ok(self.L.ndg_check_list_update(self._c, ctypes.byref(n)), "check_list_update")
+        return n.value
+
+    def integrate1(self):
+        _ok(self.L.ndg_integrate1(self._c), "integrate1")
+
+    def compute0(self, cv=True, cu=True):
+        _ok(self.L.ndg_compute(self._c, int(cv), int(cu)), "compute0")
+
+    def integrate2(self, ck=True):
+        _ok(self.L.ndg_integrate2(self._c, int(ck)), "integrate2")
+
+    def mk_iso_ke(self, sys=0):
+        _ok(self.L.ndg_mk_iso_ke(self._c, sys), "mkIsoKE")
+
+    def mk_iso_e(self, sys=0):
+        _ok(self.L.ndg_mk_iso_e(self._c, sys), "mkIsoE")
+
+    def mk_iso_p(self, sys=0):
+        _ok(self.L.ndg_mk_iso_p(self._c, sys), "mkIsoP")
+
+    def run(self, nsteps, callback=None, cont=False):
+        """The dynamics loop; returns every write_thermo record as a dict."""
+        rows = []
+
+        def cb(t, u):
+            d = t.contents.as_dict()
+            rows.append(d)
+            if callback:
+                callback(d)
+        c = THERMO_CB(cb)
+        fn = self.L.ndg_run_continue if cont else self.L.ndg_run
+        _ok(fn(self._c, int(nsteps), c, None), "run")
+        return rows
+
+    def thermo(self, sys=0):
+        t = Thermo()
+        _ok(self.L.ndg_get_thermo(self._c, sys, ctypes.byref(t)), "get_thermo")
+        return t.as_dict()
+
+    def list_updates(self, sys=0):
+        n = ctypes.c_int()
+        _ok(self.L.ndg_get_list_updates(self._c, sys, ctypes.byref(n)), "list_updates")
+        return n.value
+
+    # -- inspection -----------------------------------------------------------
+    def mcell(self, sys=0):
+        m = np.zeros(3, np.int32)
+        _ok(self.L.ndg_get_mcell(self._c, sys, _p(m)), "get_mcell")
+        return m
+
+    def cells(self, sys=0):
+        c = np.zeros(self.systems[sys], np.int32)
+        _ok(self.L.ndg_get_cells(self._c, sys, _p(c)), "get_cells")
+        return c
+
+    def neighbors(self, sys=0):
+        n = ctypes.c_longlong()
+        _ok(self.L.ndg_get_neighbors(self._c, sys, None, 0, ctypes.byref(n)), "get_neighbors")
+        pairs = np.zeros(2 * max(n.value, 1), np.int32)
+        _ok(self.L.ndg_get_neighbors(self._c, sys, _p(pairs), n.value, ctypes.byref(n)),
+            "get_neighbors")
+        return pairs[:2 * n.value].reshape(-1, 2)
+
+    # -- tuning ---------------------------------------------------------------
+    def set_tuning(self, tpa=0, graph_steps=100):
+        _ok(self.L.ndg_set_tuning(self._c, int(tpa), int(graph_steps)), "set_tuning")
+
+    def tuning(self):
+        t, g = ctypes.c_int(), ctypes.c_int()
+        _ok(self.L.ndg_get_tuning(self._c, ctypes.byref(t), ctypes.byref(g)), "get_tuning")
+        return t.value, g.value
+
+    def autotune(self, steps=20):
+        _ok(self.L.ndg_autotune(self._c, int(steps)), "autotune")
+        return self.tuning()
+
+    def set_precision(self, precision):
+        _ok(self.L.ndg_set_precision(self._c, PREC[precision]), "set_precision")

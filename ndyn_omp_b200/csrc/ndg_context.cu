@@ -1,0 +1,1301 @@
+// ndg_context.cu -- host side of the Ndyn timestep library: contexts,
+// systems, device arenas, the C ABI of include/ndyn_gpu.h and the
+// graph-block dynamics loop.
+//
+// Device memory is organised as arenas with stable offsets: a system keeps
+// its atom range, cell range and neighbour-list range until it is removed,
+// so adding or retiring systems (replicas, served requests) never moves the
+// state of the others and never changes a captured graph's arguments unless
+// an arena has to grow.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/ndyn_gpu.h"
+#include "ndg_common.h"
+#include "ndg_kernels.h"
+
+using namespace ndg;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct Range {
+  long long off = -1, len = 0;
+};
+
+// first-fit allocator over an index space that grows on demand
+struct Arena {
+  std::vector<std::pair<long long, long long>> used;  // sorted (off, len)
+  long long cap = 0;
+  long long find(long long len) const {
+    long long at = 0;
+    for (auto &u : used) {
+      if (u.first - at >= len) return at;
+      at = std::max(at, u.first + u.second);
+    }
+    return cap - at >= len ? at : -1;
+  }
+  long long end_used() const {
+    long long e = 0;
+    for (auto &u : used) e = std::max(e, u.first + u.second);
+    return e;
+  }
+  void take(long long off, long long len) {
+    used.emplace_back(off, len);
+    std::sort(used.begin(), used.end());
+  }
+  void give(long long off) {
+    for (size_t k = 0; k < used.size(); ++k)
+      if (used[k].first == off) {
+        used.erase(used.begin() + k);
+        return;
+      }
+  }
+};
+
+struct HostSys {
+  bool alive = false;
+  int n = 0, ntypes = 0, npairs = 0, ptsize = 0;
+  double ptrmin = 0.25;
+  std::vector<double> mass, rcpair, ppair, fpair;
+  std::vector<int> pairmat;
+  ndg_control ctl{};
+  Range atoms, cells, nbr;  // atoms/cells in elements, nbr in ints
+  int maxnb = 0, ncell_cap = 0;
+  int mcell0[3] = {0, 0, 0};
+  double rcut = 0.0;
+  bool lists_valid = false;
+  SysParam prm{};
+};
+
+template <class T>
+T *dalloc(size_t n) {
+  void *p = nullptr;
+  if (n == 0) n = 1;
+  if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
+  return (T *)p;
+}
+
+}  // namespace
+
+struct ndg_ctx {
+  int device = 0, precision = NDG_PREC_FP64;
+  cudaStream_t st = nullptr;
+  std::string last_err;
+  std::vector<HostSys> sys;
+  // arenas
+  Arena atoms, cells, nbrs;  // atoms in chunks, cells in cells, nbrs in ints
+  int nsys_cap = 0;
+  size_t cap_pm = 0, cap_mass = 0, cap_rc2 = 0, cap_rlist2 = 0, cap_vdr2 = 0, cap_rc2f = 0,
+         cap_tabF = 0, cap_tabP = 0, cap_tabF2 = 0, cap_tabP2 = 0;
+  // device buffers
+  SysParam *dP = nullptr;
+  SysState *dS = nullptr;
+  int *chunk_sys = nullptr, *cell_sys = nullptr;
+  double4 *pos = nullptr, *s_pos = nullptr;
+  int4 *pfx = nullptr;
+  double *vel = nullptr, *acc = nullptr, *disp = nullptr, *force = nullptr;
+  double *s_vel = nullptr, *s_acc = nullptr;
+  int *gid = nullptr, *s_gid = nullptr, *s_cell = nullptr, *nnb = nullptr;
+  int *atom_cell = nullptr, *atom_slot = nullptr, *perm = nullptr, *tmp_src = nullptr,
+      *tmp_key = nullptr;
+  int *cell_count = nullptr, *cell_start = nullptr;
+  int *nbr = nullptr;
+  double *red = nullptr, *itop = nullptr, *ired = nullptr;
+  int *pairmat = nullptr;
+  double *mass = nullptr, *rc2 = nullptr, *rlist2 = nullptr;
+  float *vdr2 = nullptr, *rc2f = nullptr;
+  double *tabF = nullptr, *tabP = nullptr;
+  float2 *tabF2 = nullptr, *tabP2 = nullptr;
+  ThermoRec *ring = nullptr;
+  int *ring_count = nullptr;
+  int ring_cap = 0;
+  std::vector<int> chunk_sys_h, cell_sys_h;
+  bool params_dirty = true;
+  // tuning and graphs
+  int tpa = 0, graph_steps = 100;
+  std::map<int, cudaGraphExec_t> graphs;
+  // per-kernel timing of the last profiled block
+  double t_int = 0, t_pair = 0, t_reb = 0;
+  int t_launches = 0;
+  ~ndg_ctx();
+};
+
+// ---------------------------------------------------------------------------
+namespace {
+
+int cuda_fail(ndg_ctx *c, cudaError_t e, const char *what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  if (c) c->last_err = m;
+  g_last_error = m;
+  return NDG_ERR_CUDA;
+}
+
+#define CK(ctx, call)                                   \
+  do {                                                  \
+    cudaError_t _e = (call);                            \
+    if (_e != cudaSuccess) return cuda_fail(ctx, _e, #call); \
+  } while (0)
+
+void drop_graphs(ndg_ctx *c) {
+  for (auto &g : c->graphs) cudaGraphExecDestroy(g.second);
+  c->graphs.clear();
+}
+
+template <class T>
+void dfree(T *&p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+DevCtx devctx(ndg_ctx *c) {
+  DevCtx d{};
+  d.P = c->dP;
+  d.S = c->dS;
+  d.chunk_sys = c->chunk_sys;
+  d.cell_sys = c->cell_sys;
+  d.nchunks = (int)c->atoms.cap;
+  d.ncells = (int)c->cells.cap;
+  d.nsys_cap = c->nsys_cap;
+  d.pos = c->pos;
+  d.pfx = c->pfx;
+  d.vel = c->vel;
+  d.acc = c->acc;
+  d.disp = c->disp;
+  d.force = c->force;
+  d.gid = c->gid;
+  d.nbr = c->nbr;
+  d.nnb = c->nnb;
+  d.atom_cell = c->atom_cell;
+  d.atom_slot = c->atom_slot;
+  d.cell_count = c->cell_count;
+  d.cell_start = c->cell_start;
+  d.perm = c->perm;
+  d.tmp_src = c->tmp_src;
+  d.tmp_key = c->tmp_key;
+  d.s_pos = c->s_pos;
+  d.s_vel = c->s_vel;
+  d.s_acc = c->s_acc;
+  d.s_gid = c->s_gid;
+  d.s_cell = c->s_cell;
+  d.pairmat = c->pairmat;
+  d.mass = c->mass;
+  d.rc2 = c->rc2;
+  d.rlist2 = c->rlist2;
+  d.vdr2 = c->vdr2;
+  d.rc2f = c->rc2f;
+  d.tabF = c->tabF;
+  d.tabP = c->tabP;
+  d.tabF2 = c->tabF2;
+  d.tabP2 = c->tabP2;
+  d.red = c->red;
+  d.itop = c->itop;
+  d.ired = c->ired;
+  d.ring = c->ring;
+  d.ring_count = c->ring_count;
+  d.ring_cap = c->ring_cap;
+  return d;
+}
+
+// grow a device buffer, keeping its first `keep` elements
+template <class T>
+int grow(ndg_ctx *c, T *&p, size_t keep, size_t n) {
+  T *q = dalloc<T>(n);
+  if (!q) return NDG_ERR_NOMEM;
+  if (p && keep) {
+    cudaError_t e = cudaMemcpy(q, p, keep * sizeof(T), cudaMemcpyDeviceToDevice);
+    if (e != cudaSuccess) {
+      cudaFree(q);
+      return cuda_fail(c, e, "grow");
+    }
+  }
+  dfree(p);
+  p = q;
+  return NDG_OK;
+}
+
+int grow_atoms(ndg_ctx *c, long long new_chunks) {
+  const size_t old = (size_t)c->atoms.cap * ATOM_ALIGN, n = (size_t)new_chunks * ATOM_ALIGN;
+  int rc = 0;
+  rc |= grow(c, c->pos, old, n);
+  rc |= grow(c, c->pfx, old, n);
+  rc |= grow(c, c->vel, 3 * old, 3 * n);
+  rc |= grow(c, c->acc, 3 * old, 3 * n);
+  rc |= grow(c, c->disp, 3 * old, 3 * n);
+  rc |= grow(c, c->force, 3 * old, 3 * n);
+  rc |= grow(c, c->gid, old, n);
+  rc |= grow(c, c->nnb, old, n);
+  rc |= grow(c, c->atom_cell, old, n);
+  rc |= grow(c, c->atom_slot, 0, n);
+  rc |= grow(c, c->perm, 0, n);
+  rc |= grow(c, c->tmp_src, 0, n);
+  rc |= grow(c, c->tmp_key, 0, n);
+  rc |= grow(c, c->s_pos, 0, n);
+  rc |= grow(c, c->s_vel, 0, 3 * n);
+  rc |= grow(c, c->s_acc, 0, 3 * n);
+  rc |= grow(c, c->s_gid, 0, n);
+  rc |= grow(c, c->s_cell, 0, n);
+  rc |= grow(c, c->itop, 2 * (size_t)c->atoms.cap, 2 * (size_t)new_chunks);
+  rc |= grow(c, c->ired, 0, (size_t)new_chunks);
+  rc |= grow(c, c->red, 0, 8 * 32 * (size_t)new_chunks);
+  rc |= grow(c, c->chunk_sys, (size_t)c->atoms.cap, (size_t)new_chunks);
+  if (rc) return NDG_ERR_NOMEM;
+  c->chunk_sys_h.resize(new_chunks, -1);
+  cudaMemcpy(c->chunk_sys + c->atoms.cap, c->chunk_sys_h.data() + c->atoms.cap,
+             (new_chunks - c->atoms.cap) * sizeof(int), cudaMemcpyHostToDevice);
+  c->atoms.cap = new_chunks;
+  drop_graphs(c);
+  return NDG_OK;
+}
+
+int grow_cells(ndg_ctx *c, long long n) {
+  int rc = 0;
+  rc |= grow(c, c->cell_count, (size_t)c->cells.cap, (size_t)n);
+  rc |= grow(c, c->cell_start, (size_t)c->cells.cap, (size_t)n);
+  rc |= grow(c, c->cell_sys, (size_t)c->cells.cap, (size_t)n);
+  if (rc) return NDG_ERR_NOMEM;
+  cudaMemset(c->cell_count + c->cells.cap, 0, (n - c->cells.cap) * sizeof(int));
+  c->cell_sys_h.resize(n, -1);
+  cudaMemcpy(c->cell_sys + c->cells.cap, c->cell_sys_h.data() + c->cells.cap,
+             (n - c->cells.cap) * sizeof(int), cudaMemcpyHostToDevice);
+  c->cells.cap = n;
+  drop_graphs(c);
+  return NDG_OK;
+}
+
+int grow_nbr(ndg_ctx *c, long long n) {
+  if (grow(c, c->nbr, (size_t)c->nbrs.cap, (size_t)n)) return NDG_ERR_NOMEM;
+  c->nbrs.cap = n;
+  drop_graphs(c);
+  return NDG_OK;
+}
+
+int grow_sys(ndg_ctx *c, int n) {
+  int rc = 0;
+  rc |= grow(c, c->dP, (size_t)c->nsys_cap, (size_t)n);
+  rc |= grow(c, c->dS, (size_t)c->nsys_cap, (size_t)n);
+  if (rc) return NDG_ERR_NOMEM;
+  std::vector<SysParam> z(n - c->nsys_cap);
+  std::vector<SysState> zs(n - c->nsys_cap);
+  memset(z.data(), 0, z.size() * sizeof(SysParam));
+  memset(zs.data(), 0, zs.size() * sizeof(SysState));
+  cudaMemcpy(c->dP + c->nsys_cap, z.data(), z.size() * sizeof(SysParam), cudaMemcpyHostToDevice);
+  cudaMemcpy(c->dS + c->nsys_cap, zs.data(), zs.size() * sizeof(SysState),
+             cudaMemcpyHostToDevice);
+  c->nsys_cap = n;
+  // thermo ring: graph_steps records per system
+  const int need = std::max(256, c->graph_steps * n);
+  if (need > c->ring_cap) {
+    dfree(c->ring);
+    c->ring = dalloc<ThermoRec>(need);
+    if (!c->ring) return NDG_ERR_NOMEM;
+    c->ring_cap = need;
+  }
+  drop_graphs(c);
+  return NDG_OK;
+}
+
+// Allocate `len` units in an arena, growing the device buffers if needed.
+long long arena_take(ndg_ctx *c, Arena &a, long long len, int which) {
+  long long off = a.find(len);
+  if (off < 0) {
+    long long want = std::max(a.end_used() + len, a.cap + a.cap / 2);
+    int rc = which == 0 ? grow_atoms(c, want) : which == 1 ? grow_cells(c, want) : grow_nbr(c, want);
+    if (rc) return -1;
+    off = a.find(len);
+    if (off < 0) return -1;
+  }
+  a.take(off, len);
+  return off;
+}
+
+// copy a host vector to a device array, reallocating (with headroom) when
+// it no longer fits; a reallocation invalidates captured graphs
+template <class T>
+int upload_vec(ndg_ctx *c, T *&dst, size_t &cap, const std::vector<T> &v) {
+  if (!dst || v.size() > cap) {
+    dfree(dst);
+    cap = std::max<size_t>(v.size() * 2, 64);
+    dst = dalloc<T>(cap);
+    if (!dst) return NDG_ERR_NOMEM;
+    drop_graphs(c);
+  }
+  if (!v.empty() && cudaMemcpy(dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice))
+    return NDG_ERR_CUDA;
+  return NDG_OK;
+}
+
+// small per-pair/per-type arrays: rebuilt for all systems on any change
+int upload_params(ndg_ctx *c) {
+  std::vector<int> pm;
+  std::vector<double> mass, rc2, rlist2, tabF, tabP;
+  std::vector<float> vdr2, rc2f;
+  std::vector<float2> tF2, tP2;
+  std::vector<SysParam> prm(c->nsys_cap);
+  memset(prm.data(), 0, prm.size() * sizeof(SysParam));
+  for (size_t s = 0; s < c->sys.size(); ++s) {
+    HostSys &h = c->sys[s];
+    if (!h.alive) continue;
+    SysParam &p = h.prm;
+    p.tab_off = (int)tabF.size();
+    p.pair_off = (int)rc2.size();
+    p.type_off = (int)mass.size();
+    p.pm_off = (int)pm.size();
+    pm.insert(pm.end(), h.pairmat.begin(), h.pairmat.end());
+    mass.insert(mass.end(), h.mass.begin(), h.mass.end());
+    const double skin = h.ctl.skin < 0 ? 0.2 * h.rcut : h.ctl.skin;
+    for (int j = 0; j < h.npairs; ++j) {
+      const double r = h.rcpair[j];
+      const double prc2 = r * r;
+      const double pdr2 = (prc2 - h.ptrmin) / (h.ptsize - 1);
+      rc2.push_back(prc2);
+      rc2f.push_back((float)prc2);
+      vdr2.push_back((float)(1.0 / pdr2));  // vPTdr2 = real(1.d0/PTdr2), src/nd.f90:254
+      const double rl = skin + r;            // rcuts2 = skin + PairParams(1,.), :1375
+      rlist2.push_back(rl * rl);
+      const int T = h.ptsize + 1;
+      for (int k = 0; k < T; ++k) {
+        const double f0 = h.fpair[(size_t)j * T + k], p0 = h.ppair[(size_t)j * T + k];
+        const double f1 = k + 1 < T ? h.fpair[(size_t)j * T + k + 1] : f0;
+        const double p1 = k + 1 < T ? h.ppair[(size_t)j * T + k + 1] : p0;
+        tabF.push_back(f0);
+        tabP.push_back(p0);
+        tF2.push_back(make_float2((float)f0, (float)f1));
+        tP2.push_back(make_float2((float)p0, (float)p1));
+      }
+    }
+    prm[s] = p;
+  }
+  int rc = 0;
+  rc |= upload_vec(c, c->pairmat, c->cap_pm, pm);
+  rc |= upload_vec(c, c->mass, c->cap_mass, mass);
+  rc |= upload_vec(c, c->rc2, c->cap_rc2, rc2);
+  rc |= upload_vec(c, c->rlist2, c->cap_rlist2, rlist2);
+  rc |= upload_vec(c, c->vdr2, c->cap_vdr2, vdr2);
+  rc |= upload_vec(c, c->rc2f, c->cap_rc2f, rc2f);
+  rc |= upload_vec(c, c->tabF, c->cap_tabF, tabF);
+  rc |= upload_vec(c, c->tabP, c->cap_tabP, tabP);
+  rc |= upload_vec(c, c->tabF2, c->cap_tabF2, tF2);
+  rc |= upload_vec(c, c->tabP2, c->cap_tabP2, tP2);
+  if (rc) return NDG_ERR_NOMEM;
+  CK(c, cudaMemcpy(c->dP, prm.data(), prm.size() * sizeof(SysParam), cudaMemcpyHostToDevice));
+  c->params_dirty = false;
+  return NDG_OK;
+}
+
+void fill_control_params(HostSys &h) {
+  SysParam &p = h.prm;
+  const ndg_control &q = h.ctl;
+  p.dt = q.dt;
+  p.skin = q.skin < 0 ? 0.2 * h.rcut : q.skin;
+  p.skinsq = p.skin * p.skin;
+  p.rlist = h.rcut + p.skin;
+  p.renei = q.renei;
+  p.renei_freq = q.renei_freq;
+  p.out_steps = q.out_steps;
+  p.isokinetic = q.isokinetic;
+  p.ke_freq = q.ke_freq;
+  p.ke_target = q.ke_target;
+  p.ke_parm = q.ke_parm;
+  p.isobaric = q.isobaric;
+  p.p_freq = q.p_freq;
+  for (int d = 0; d < 3; ++d) p.p_target[d] = q.p_target[d];
+  p.p_parm = q.p_parm;
+  p.isoenergetic = q.isoenergetic;
+  p.e_freq = q.e_freq;
+  p.e_parm = q.e_parm;
+  p.box_load = q.box_load;
+  for (int d = 0; d < 3; ++d) p.box_vel[d] = q.box_vel[d];
+  p.quirk = q.quirk;
+  p.ptrmin = h.ptrmin;
+  p.ntypes = h.ntypes;
+  p.npairs = h.npairs;
+  p.ptsize = h.ptsize;
+}
+
+bool valid_sys(ndg_ctx *c, int s) {
+  return c && s >= 0 && s < (int)c->sys.size() && c->sys[s].alive;
+}
+
+int get_state_dev(ndg_ctx *c, int s, SysState &S) {
+  CK(c, cudaMemcpy(&S, c->dS + s, sizeof(SysState), cudaMemcpyDeviceToHost));
+  return NDG_OK;
+}
+int put_state_dev(ndg_ctx *c, int s, const SysState &S) {
+  CK(c, cudaMemcpy(c->dS + s, &S, sizeof(SysState), cudaMemcpyHostToDevice));
+  return NDG_OK;
+}
+
+// upload atoms in caller order (identity permutation)
+int upload_atoms(ndg_ctx *c, int s, const int *typ, const double *pos, const double *vel,
+                 const double *acc) {
+  HostSys &h = c->sys[s];
+  const int n = h.n;
+  const size_t off = (size_t)h.atoms.off * ATOM_ALIGN;
+  std::vector<double4> p4(n);
+  std::vector<int> g(n);
+  std::vector<int> tw(n);
+  if (typ) {
+    for (int i = 0; i < n; ++i) tw[i] = pack_tw(typ[i], s);
+  } else {
+    // keep the types already on the device (they are in pos.w, device order)
+    std::vector<double4> old(n);
+    std::vector<int> og(n);
+    CK(c, cudaMemcpy(old.data(), c->pos + off, n * sizeof(double4), cudaMemcpyDeviceToHost));
+    CK(c, cudaMemcpy(og.data(), c->gid + off, n * sizeof(int), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; ++i) {
+      long long w;
+      memcpy(&w, &old[i].w, 8);
+      tw[og[i]] = (int)w;
+    }
+  }
+  for (int i = 0; i < n; ++i) {
+    const long long w = (long long)(unsigned)tw[i];
+    double wd;
+    memcpy(&wd, &w, 8);
+    p4[i] = make_double4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], wd);
+    g[i] = i;
+  }
+  CK(c, cudaMemcpy(c->pos + off, p4.data(), n * sizeof(double4), cudaMemcpyHostToDevice));
+  CK(c, cudaMemcpy(c->gid + off, g.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+  std::vector<double> z(3 * (size_t)n, 0.0);
+  CK(c, cudaMemcpy(c->vel + 3 * off, vel ? vel : z.data(), 3 * n * sizeof(double),
+                   cudaMemcpyHostToDevice));
+  CK(c, cudaMemcpy(c->acc + 3 * off, acc ? acc : z.data(), 3 * n * sizeof(double),
+                   cudaMemcpyHostToDevice));
+  CK(c, cudaMemcpy(c->disp + 3 * off, z.data(), 3 * n * sizeof(double), cudaMemcpyHostToDevice));
+  h.lists_valid = false;
+  return NDG_OK;
+}
+
+// dynamics prologue for every system, src/nd.f90:73-108: skin default,
+// MCELL, neighbour capacity; then one rebuild of all lists.
+int setup_lists(ndg_ctx *c) {
+  for (size_t s = 0; s < c->sys.size(); ++s) {
+    HostSys &h = c->sys[s];
+    if (!h.alive) continue;
+    if (h.ctl.skin < 0) h.ctl.skin = 0.2 * h.rcut;  // persists, as in the reference
+    fill_control_params(h);
+    SysState S;
+    int rc = get_state_dev(c, (int)s, S);
+    if (rc) return rc;
+    int nc = 1;
+    for (int d = 0; d < 3; ++d) {
+      h.mcell0[d] = (int)(S.box[d] / (h.rcut + h.prm.skin));
+      if (h.mcell0[d] < 2) return NDG_ERR_CELLS;
+      nc *= h.mcell0[d];
+      h.prm.mcell0[d] = h.mcell0[d];
+      S.mcell[d] = h.mcell0[d];
+    }
+    S.ncell = nc;
+    // neighbour capacity of the full list: sphere of radius 1.1*(rcut+skin)
+    // at the mean density (the reference's NeiMax estimate counts the same
+    // sphere, src/nd.f90:84-88), doubled where the reference stencil repeats
+    // pairs (a cell count of 2 in ref semantics)
+    const double vol = S.box[0] * S.box[1] * S.box[2];
+    const double r = (h.rcut + h.prm.skin) * 1.1;
+    double est = 4.0 / 3.0 * 3.141592653589793 * r * r * r * h.n / vol;
+    if (h.ctl.quirk == NDG_QUIRK_REF &&
+        (h.mcell0[0] == 2 || h.mcell0[1] == 2 || h.mcell0[2] == 2))
+      est *= 2.0;
+    int maxnb = (int)(est * 1.2) + 16;
+    if (h.ctl.neimax > 0) maxnb = std::max(maxnb, 2 * h.ctl.neimax);
+    maxnb = std::min((maxnb + 7) / 8 * 8, std::max(h.n - 1, 8) * (h.ctl.quirk == 0 ? 2 : 1) + 8);
+    const long long npad = (long long)h.atoms.len * ATOM_ALIGN;
+    if (maxnb > h.maxnb) {
+      if (h.nbr.off >= 0) c->nbrs.give(h.nbr.off);
+      const long long off = arena_take(c, c->nbrs, (long long)maxnb * npad, 2);
+      if (off < 0) return NDG_ERR_NOMEM;
+      h.nbr.off = off;
+      h.nbr.len = (long long)maxnb * npad;
+      h.maxnb = maxnb;
+    }
+    if (nc + 1 > h.ncell_cap) {
+      if (h.cells.off >= 0) {
+        c->cells.give(h.cells.off);
+        for (long long q = h.cells.off; q < h.cells.off + h.cells.len; ++q) c->cell_sys_h[q] = -1;
+      }
+      const long long off = arena_take(c, c->cells, nc + 1, 1);
+      if (off < 0) return NDG_ERR_NOMEM;
+      h.cells.off = off;
+      h.cells.len = nc + 1;
+      h.ncell_cap = nc + 1;
+      for (long long q = off; q < off + nc; ++q) c->cell_sys_h[q] = (int)s;
+      CK(c, cudaMemcpy(c->cell_sys, c->cell_sys_h.data(), c->cells.cap * sizeof(int),
+                       cudaMemcpyHostToDevice));
+    }
+    h.prm.atom_off = (int)(h.atoms.off * ATOM_ALIGN);
+    h.prm.n = h.n;
+    h.prm.npad = (int)npad;
+    h.prm.cell_off = (int)h.cells.off;
+    h.prm.ncell_cap = h.ncell_cap;
+    h.prm.nbr_off = h.nbr.off;
+    h.prm.maxnb = h.maxnb;
+    S.nlist_updates = 0;
+    S.rebuild = 0;
+    S.err = 0;
+    S.pend = 0;
+    for (int d = 0; d < 3; ++d) S.box_build[d] = S.box[d];
+    rc = put_state_dev(c, (int)s, S);
+    if (rc) return rc;
+  }
+  int rc = upload_params(c);
+  if (rc) return rc;
+  CK(c, cudaMemset(c->ring_count, 0, 2 * sizeof(int)));
+  DevCtx d = devctx(c);
+  launch_rebuild(d, c->st, 1, c->precision == NDG_PREC_MIXED);
+  CK(c, cudaGetLastError());
+  CK(c, cudaStreamSynchronize(c->st));
+  int words[2];
+  CK(c, cudaMemcpy(words, c->ring_count, sizeof(words), cudaMemcpyDeviceToHost));
+  if (words[1]) {
+    if (words[1] & E_NEIMAX) return NDG_ERR_NEIMAX;
+    if (words[1] & E_OUT_OF_BOX) return NDG_ERR_OUT_OF_BOX;
+    return NDG_ERR_CELLS;
+  }
+  for (auto &h : c->sys)
+    if (h.alive) h.lists_valid = true;
+  return NDG_OK;
+}
+
+int choose_tpa(ndg_ctx *c) {
+  if (c->tpa > 0) return c->tpa;
+  long long atoms = 0;
+  double nb = 0.0;
+  for (auto &h : c->sys)
+    if (h.alive) {
+      atoms += h.n;
+      nb += (double)h.n * std::max(h.maxnb / 1.5, 8.0);
+    }
+  if (!atoms) return 1;
+  nb /= atoms;
+  // enough threads to fill the 148 SMs, and about 16+ neighbours per thread
+  int t = 1;
+  while (t < 32 && ((double)atoms * t < 148.0 * 1024.0 || nb / t > 48.0)) t *= 2;
+  return t;
+}
+
+void enqueue_steps(ndg_ctx *c, int nsteps) {
+  DevCtx d = devctx(c);
+  const int mixed = c->precision == NDG_PREC_MIXED;
+  const int tpa = choose_tpa(c);
+  for (int k = 0; k < nsteps; ++k) {
+    launch_rebuild(d, c->st, 0, mixed);
+    launch_integrate1(d, c->st, 0, mixed);
+    launch_pair(d, c->st, tpa, mixed, 1, 0);
+  }
+}
+
+int check_words(ndg_ctx *c, int *count) {
+  int words[2];
+  CK(c, cudaMemcpyAsync(words, c->ring_count, sizeof(words), cudaMemcpyDeviceToHost, c->st));
+  CK(c, cudaStreamSynchronize(c->st));
+  *count = words[0];
+  if (words[1] & E_NEIMAX) return NDG_ERR_NEIMAX;
+  if (words[1] & E_OUT_OF_BOX) return NDG_ERR_OUT_OF_BOX;
+  if (words[1] & E_CELLS) return NDG_ERR_CELLS;
+  return NDG_OK;
+}
+
+int drain_ring(ndg_ctx *c, int count, ndg_thermo_cb cb, void *user) {
+  if (count <= 0) return NDG_OK;
+  const int n = std::min(count, c->ring_cap);
+  std::vector<ThermoRec> r(n);
+  CK(c, cudaMemcpy(r.data(), c->ring, n * sizeof(ThermoRec), cudaMemcpyDeviceToHost));
+  CK(c, cudaMemset(c->ring_count, 0, sizeof(int)));
+  std::stable_sort(r.begin(), r.end(), [](const ThermoRec &a, const ThermoRec &b) {
+    return a.step != b.step ? a.step < b.step : a.sys < b.sys;
+  });
+  if (cb)
+    for (auto &t : r) cb(reinterpret_cast<const ndg_thermo *>(&t), user);
+  return NDG_OK;
+}
+
+int run_steps(ndg_ctx *c, int nsteps, ndg_thermo_cb cb, void *user) {
+  int left = nsteps;
+  while (left > 0) {
+    const int g = std::min(left, std::max(c->graph_steps, 1));
+    cudaGraphExec_t exec = nullptr;
+    auto it = c->graphs.find(g);
+    if (it != c->graphs.end()) {
+      exec = it->second;
+    } else if (c->graph_steps > 1) {
+      cudaGraph_t graph;
+      CK(c, cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+      enqueue_steps(c, g);
+      CK(c, cudaStreamEndCapture(c->st, &graph));
+      CK(c, cudaGraphInstantiate(&exec, graph, 0));
+      cudaGraphDestroy(graph);
+      c->graphs[g] = exec;
+    }
+    if (exec) {
+      CK(c, cudaGraphLaunch(exec, c->st));
+    } else {
+      enqueue_steps(c, g);
+      CK(c, cudaGetLastError());
+    }
+    int count = 0;
+    int rc = check_words(c, &count);
+    if (rc) return rc;
+    rc = drain_ring(c, count, cb, user);
+    if (rc) return rc;
+    left -= g;
+  }
+  return NDG_OK;
+}
+
+int flush_pending(ndg_ctx *c) {
+  DevCtx d = devctx(c);
+  launch_flush(d, c->st, c->nsys_cap);
+  CK(c, cudaGetLastError());
+  CK(c, cudaStreamSynchronize(c->st));
+  return NDG_OK;
+}
+
+int status_from_words(ndg_ctx *c) {
+  int count;
+  return check_words(c, &count);
+}
+
+}  // namespace
+
+ndg_ctx::~ndg_ctx() {
+  drop_graphs(this);
+  void *ptrs[] = {dP, dS, chunk_sys, cell_sys, pos, s_pos, pfx, vel, acc, disp, force, s_vel,
+                  s_acc, gid, s_gid, s_cell, nnb, atom_cell, atom_slot, perm, tmp_src, tmp_key,
+                  cell_count, cell_start, nbr, red, itop, ired, pairmat, mass, rc2, rlist2,
+                  vdr2, rc2f, tabF, tabP, tabF2, tabP2, ring, ring_count};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (st) cudaStreamDestroy(st);
+}
+
+// ===========================================================================
+// C ABI
+extern "C" {
+
+int ndg_abi_version(void) { return NDG_ABI_VERSION; }
+
+const char *ndg_error_string(int s) {
+  switch (s) {
+    case NDG_OK: return "ok";
+    case NDG_ERR_ARG: return "invalid argument or call order";
+    case NDG_ERR_NEIMAX: return "too many neighbours in list";
+    case NDG_ERR_OUT_OF_BOX: return "Particle outside of box";
+    case NDG_ERR_POTENTIAL: return "no potential available for potential type";
+    case NDG_ERR_CELLS: return "fewer than 2 link cells in a direction (box < 2*(rcut+skin))";
+    case NDG_ERR_NOMEM: return "device memory exhausted";
+    case NDG_ERR_CUDA: return "CUDA runtime error";
+    case NDG_ERR_BUDGET: return "request exceeds the HBM budget";
+    case NDG_ERR_NOT_FOUND: return "unknown system or request";
+    case NDG_ERR_TIMEOUT: return "bounded wait expired";
+    default: return "unknown status";
+  }
+}
+
+const char *ndg_last_error(const ndg_ctx *c) {
+  return c ? c->last_err.c_str() : g_last_error.c_str();
+}
+
+void ndg_default_control(ndg_control *q) {
+  memset(q, 0, sizeof(*q));
+  q->dt = 0.0001;  // src/read_input.f90:19-41
+  q->skin = -1.0;
+  q->neimax = 0;
+  q->renei = 1;
+  q->renei_freq = 1;
+  q->out_steps = 40;
+  q->step = 0;
+  q->ke_freq = q->p_freq = q->e_freq = 1;
+  q->quirk = NDG_QUIRK_REF;
+}
+
+int ndg_create(ndg_ctx **out, int device, int precision) {
+  if (!out || (precision != NDG_PREC_FP64 && precision != NDG_PREC_MIXED)) return NDG_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) return cuda_fail(nullptr, e ? e : cudaErrorNoDevice, "device");
+  if (device < 0 || device >= ndev) return NDG_ERR_ARG;
+  e = cudaSetDevice(device);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaSetDevice");
+  ndg_ctx *c = new ndg_ctx();
+  c->device = device;
+  c->precision = precision;
+  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return NDG_ERR_CUDA;
+  }
+  c->ring_count = dalloc<int>(2);
+  if (!c->ring_count) {
+    delete c;
+    return NDG_ERR_NOMEM;
+  }
+  cudaMemset(c->ring_count, 0, 2 * sizeof(int));
+  int rc = grow_sys(c, 4);
+  if (!rc) rc = grow_atoms(c, 16);
+  if (!rc) rc = grow_cells(c, 1024);
+  if (!rc) rc = grow_nbr(c, 1 << 16);
+  if (rc) {
+    delete c;
+    return rc;
+  }
+  *out = c;
+  return NDG_OK;
+}
+
+int ndg_destroy(ndg_ctx *c) {
+  if (!c) return NDG_ERR_ARG;
+  cudaSetDevice(c->device);
+  delete c;
+  return NDG_OK;
+}
+
+int ndg_set_precision(ndg_ctx *c, int precision) {
+  if (!c || (precision != NDG_PREC_FP64 && precision != NDG_PREC_MIXED)) return NDG_ERR_ARG;
+  if (precision != c->precision) {
+    c->precision = precision;
+    drop_graphs(c);
+    if (precision == NDG_PREC_MIXED) {
+      DevCtx d = devctx(c);
+      launch_refresh_pfx(d, c->st);
+      CK(c, cudaStreamSynchronize(c->st));
+    }
+  }
+  return NDG_OK;
+}
+
+int ndg_add_system(ndg_ctx *c, int np, int ntypes, int npairs, int ptsize, double ptrmin,
+                   const double *mass, const int *pairmat, const double *rcpair,
+                   const double *ppair, const double *fpair, const int *typ, const double *pos,
+                   const double *vel, const double *acc, const double *box, int *sys_out) {
+  if (!c || np < 1 || ntypes < 1 || ntypes > MAX_TYPES || npairs < 1 || ptsize < 2 || !mass ||
+      !pairmat || !rcpair || !ppair || !fpair || !typ || !pos || !box)
+    return NDG_ERR_ARG;
+  for (int i = 0; i < np; ++i)
+    if (typ[i] < 1 || typ[i] > ntypes) return NDG_ERR_ARG;
+  for (int k = 0; k < ntypes * ntypes; ++k)
+    if (pairmat[k] < 0 || pairmat[k] > npairs) return NDG_ERR_ARG;
+  // one-sided ('asym') pairs take the compute1 path, which this library
+  // does not provide: PairMat must be symmetric (src/nd.f90:155-163)
+  for (int a = 0; a < ntypes; ++a)
+    for (int b = 0; b < ntypes; ++b)
+      if (pairmat[a + b * ntypes] != pairmat[b + a * ntypes]) return NDG_ERR_ARG;
+  cudaSetDevice(c->device);
+  int s = -1;
+  for (size_t k = 0; k < c->sys.size(); ++k)
+    if (!c->sys[k].alive) {
+      s = (int)k;
+      break;
+    }
+  if (s < 0) {
+    s = (int)c->sys.size();
+    c->sys.emplace_back();
+  }
+  if (s >= 65535) return NDG_ERR_ARG;
+  if (s >= c->nsys_cap) {
+    int rc = grow_sys(c, std::max(s + 1, c->nsys_cap * 2));
+    if (rc) return rc;
+  }
+  HostSys &h = c->sys[s];
+  h = HostSys();
+  h.alive = true;
+  h.n = np;
+  h.ntypes = ntypes;
+  h.npairs = npairs;
+  h.ptsize = ptsize;
+  h.ptrmin = ptrmin;
+  h.mass.assign(mass, mass + ntypes);
+  h.pairmat.assign(pairmat, pairmat + ntypes * ntypes);
+  h.rcpair.assign(rcpair, rcpair + npairs);
+  h.ppair.assign(ppair, ppair + (size_t)(ptsize + 1) * npairs);
+  h.fpair.assign(fpair, fpair + (size_t)(ptsize + 1) * npairs);
+  h.rcut = *std::max_element(rcpair, rcpair + npairs);  // src/potentials.f90:36
+  ndg_default_control(&h.ctl);
+  const long long nch = (np + ATOM_ALIGN - 1) / ATOM_ALIGN;
+  const long long off = arena_take(c, c->atoms, nch, 0);
+  if (off < 0) {
+    h.alive = false;
+    return NDG_ERR_NOMEM;
+  }
+  h.atoms.off = off;
+  h.atoms.len = nch;
+  for (long long q = off; q < off + nch; ++q) c->chunk_sys_h[q] = s;
+  CK(c, cudaMemcpy(c->chunk_sys + off, c->chunk_sys_h.data() + off, nch * sizeof(int),
+                   cudaMemcpyHostToDevice));
+  // padding slots: gid -1, zero state
+  const size_t a0 = (size_t)off * ATOM_ALIGN, na = (size_t)nch * ATOM_ALIGN;
+  CK(c, cudaMemset(c->gid + a0, 0xff, na * sizeof(int)));
+  CK(c, cudaMemset(c->pos + a0, 0, na * sizeof(double4)));
+  CK(c, cudaMemset(c->nnb + a0, 0, na * sizeof(int)));
+  h.prm = SysParam();
+  fill_control_params(h);
+  h.prm.atom_off = (int)a0;
+  h.prm.n = np;
+  h.prm.npad = (int)na;
+  SysState S;
+  memset(&S, 0, sizeof(S));
+  for (int d = 0; d < 3; ++d) {
+    S.box[d] = box[d];
+    S.box_build[d] = box[d];
+    S.li[d] = 1.0 / box[d];
+  }
+  S.lam_ke = S.lam_e = 1.0;
+  int rc = put_state_dev(c, s, S);
+  if (rc) return rc;
+  rc = upload_atoms(c, s, typ, pos, vel, acc);
+  if (rc) return rc;
+  rc = upload_params(c);
+  if (rc) return rc;
+  if (c->precision == NDG_PREC_MIXED) {
+    DevCtx d = devctx(c);
+    launch_refresh_pfx(d, c->st);
+    CK(c, cudaStreamSynchronize(c->st));
+  }
+  if (sys_out) *sys_out = s;
+  return NDG_OK;
+}
+
+int ndg_remove_system(ndg_ctx *c, int s) {
+  if (!valid_sys(c, s)) return NDG_ERR_NOT_FOUND;
+  HostSys &h = c->sys[s];
+  for (long long q = h.atoms.off; q < h.atoms.off + h.atoms.len; ++q) c->chunk_sys_h[q] = -1;
+  CK(c, cudaMemcpy(c->chunk_sys + h.atoms.off, c->chunk_sys_h.data() + h.atoms.off,
+                   h.atoms.len * sizeof(int), cudaMemcpyHostToDevice));
+  c->atoms.give(h.atoms.off);
+  if (h.cells.off >= 0) {
+    for (long long q = h.cells.off; q < h.cells.off + h.cells.len; ++q) c->cell_sys_h[q] = -1;
+    CK(c, cudaMemcpy(c->cell_sys + h.cells.off, c->cell_sys_h.data() + h.cells.off,
+                     h.cells.len * sizeof(int), cudaMemcpyHostToDevice));
+    c->cells.give(h.cells.off);
+  }
+  if (h.nbr.off >= 0) c->nbrs.give(h.nbr.off);
+  h = HostSys();
+  SysState S;
+  memset(&S, 0, sizeof(S));
+  int rc = put_state_dev(c, s, S);
+  if (rc) return rc;
+  return upload_params(c);
+}
+
+int ndg_num_systems(const ndg_ctx *c) {
+  if (!c) return 0;
+  int n = 0;
+  for (auto &h : c->sys) n += h.alive;
+  return n;
+}
+
+int ndg_load_state(ndg_ctx *c, int s, const double *pos, const double *vel, const double *acc,
+                   const double *box) {
+  if (!valid_sys(c, s) || !pos) return NDG_ERR_ARG;
+  cudaSetDevice(c->device);
+  int rc = upload_atoms(c, s, nullptr, pos, vel, acc);
+  if (rc) return rc;
+  if (box) {
+    SysState S;
+    rc = get_state_dev(c, s, S);
+    if (rc) return rc;
+    for (int d = 0; d < 3; ++d) {
+      S.box[d] = box[d];
+      S.li[d] = 1.0 / box[d];
+    }
+    rc = put_state_dev(c, s, S);
+    if (rc) return rc;
+  }
+  if (c->precision == NDG_PREC_MIXED) {
+    DevCtx d = devctx(c);
+    launch_refresh_pfx(d, c->st);
+    CK(c, cudaStreamSynchronize(c->st));
+  }
+  return NDG_OK;
+}
+
+int ndg_get_state(ndg_ctx *c, int s, double *pos, double *vel, double *acc, double *box) {
+  if (!valid_sys(c, s)) return NDG_ERR_ARG;
+  cudaSetDevice(c->device);
+  HostSys &h = c->sys[s];
+  const int n = h.n;
+  const size_t off = (size_t)h.atoms.off * ATOM_ALIGN;
+  CK(c, cudaStreamSynchronize(c->st));
+  std::vector<int> g(n);
+  CK(c, cudaMemcpy(g.data(), c->gid + off, n * sizeof(int), cudaMemcpyDeviceToHost));
+  if (pos) {
+    std::vector<double4> p(n);
+    CK(c, cudaMemcpy(p.data(), c->pos + off, n * sizeof(double4), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; ++i) {
+      pos[3 * g[i]] = p[i].x;
+      pos[3 * g[i] + 1] = p[i].y;
+      pos[3 * g[i] + 2] = p[i].z;
+    }
+  }
+  std::vector<double> t(3 * (size_t)n);
+  if (vel) {
+    CK(c, cudaMemcpy(t.data(), c->vel + 3 * off, 3 * n * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; ++i)
+      for (int d = 0; d < 3; ++d) vel[3 * g[i] + d] = t[3 * i + d];
+  }
+  if (acc) {
+    CK(c, cudaMemcpy(t.data(), c->acc + 3 * off, 3 * n * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; ++i)
+      for (int d = 0; d < 3; ++d) acc[3 * g[i] + d] = t[3 * i + d];
+  }
+  if (box) {
+    SysState S;
+    int rc = get_state_dev(c, s, S);
+    if (rc) return rc;
+    for (int d = 0; d < 3; ++d) box[d] = S.box[d];
+  }
+  return NDG_OK;
+}
+
+int ndg_set_control(ndg_ctx *c, int s, const ndg_control *q) {
+  if (!valid_sys(c, s) || !q) return NDG_ERR_ARG;
+  if (q->out_steps < 1 || q->renei_freq < 1 || q->ke_freq < 1 || q->p_freq < 1 ||
+      q->e_freq < 1 || (q->quirk != NDG_QUIRK_REF && q->quirk != NDG_QUIRK_FIXED))
+    return NDG_ERR_ARG;
+  HostSys &h = c->sys[s];
+  h.ctl = *q;
+  fill_control_params(h);
+  SysState S;
+  int rc = get_state_dev(c, s, S);
+  if (rc) return rc;
+  S.step = q->step;
+  rc = put_state_dev(c, s, S);
+  if (rc) return rc;
+  return upload_params(c);
+}
+
+int ndg_get_control(ndg_ctx *c, int s, ndg_control *q) {
+  if (!valid_sys(c, s) || !q) return NDG_ERR_ARG;
+  *q = c->sys[s].ctl;
+  SysState S;
+  int rc = get_state_dev(c, s, S);
+  if (rc) return rc;
+  q->step = S.step;
+  return NDG_OK;
+}
+
+int ndg_setup_lists(ndg_ctx *c) {
+  if (!c) return NDG_ERR_ARG;
+  cudaSetDevice(c->device);
+  return setup_lists(c);
+}
+
+int ndg_build_cell_list(ndg_ctx *c) {
+  if (!c) return NDG_ERR_ARG;
+  for (auto &h : c->sys)
+    if (h.alive && h.maxnb == 0) return setup_lists(c);
+  DevCtx d = devctx(c);
+  CK(c, cudaMemset(c->ring_count, 0, 2 * sizeof(int)));
+  launch_rebuild(d, c->st, 1, c->precision == NDG_PREC_MIXED);
+  CK(c, cudaGetLastError());
+  int rc = status_from_words(c);
+  if (!rc)
+    for (auto &h : c->sys)
+      if (h.alive) h.lists_valid = true;
+  return rc;
+}
+
+static bool lists_ready(ndg_ctx *c) {
+  for (auto &h : c->sys)
+    if (h.alive && !h.lists_valid) return false;
+  return true;
+}
+
+int ndg_check_list_update(ndg_ctx *c, int *rebuilt) {
+  if (!c || !lists_ready(c)) return NDG_ERR_ARG;
+  DevCtx d = devctx(c);
+  CK(c, cudaMemset(c->ring_count, 0, 2 * sizeof(int)));
+  launch_check(d, c->st, c->nsys_cap);
+  launch_rebuild(d, c->st, 0, c->precision == NDG_PREC_MIXED);
+  CK(c, cudaGetLastError());
+  int rc = status_from_words(c);
+  if (rc) return rc;
+  if (rebuilt) {
+    std::vector<SysState> S(c->nsys_cap);
+    CK(c, cudaMemcpy(S.data(), c->dS, S.size() * sizeof(SysState), cudaMemcpyDeviceToHost));
+    int n = 0;
+    for (size_t s = 0; s < c->sys.size(); ++s) n += c->sys[s].alive && S[s].rebuild;
+    *rebuilt = n;
+  }
+  return NDG_OK;
+}
+
+int ndg_integrate1(ndg_ctx *c) {
+  if (!c) return NDG_ERR_ARG;
+  std::vector<SysState> S(c->nsys_cap);
+  CK(c, cudaMemcpy(S.data(), c->dS, S.size() * sizeof(SysState), cudaMemcpyDeviceToHost));
+  for (auto &x : S)
+    for (int d = 0; d < 3; ++d) x.li[d] = 1.0 / x.box[d];  // li = 1/box, src/nd.f90:1023-1025
+  CK(c, cudaMemcpy(c->dS, S.data(), S.size() * sizeof(SysState), cudaMemcpyHostToDevice));
+  DevCtx d = devctx(c);
+  launch_integrate1(d, c->st, 1, c->precision == NDG_PREC_MIXED);
+  CK(c, cudaGetLastError());
+  CK(c, cudaStreamSynchronize(c->st));
+  return NDG_OK;
+}
+
+int ndg_compute(ndg_ctx *c, int cv, int cu) {
+  if (!c || !lists_ready(c)) return NDG_ERR_ARG;
+  DevCtx d = devctx(c);
+  const int flags = (cv ? F_CV : 0) | (cu ? F_CU : 0);
+  launch_pair(d, c->st, choose_tpa(c), c->precision == NDG_PREC_MIXED, 0, flags);
+  CK(c, cudaGetLastError());
+  CK(c, cudaStreamSynchronize(c->st));
+  return NDG_OK;
+}
+
+int ndg_integrate2(ndg_ctx *c, int ck) {
+  if (!c) return NDG_ERR_ARG;
+  DevCtx d = devctx(c);
+  launch_integrate2(d, c->st, ck);
+  CK(c, cudaGetLastError());
+  CK(c, cudaStreamSynchronize(c->st));
+  return NDG_OK;
+}
+
+int ndg_mk_iso_ke(ndg_ctx *c, int s) {
+  if (!valid_sys(c, s)) return NDG_ERR_ARG;
+  SysState S;
+  int rc = get_state_dev(c, s, S);
+  if (rc) return rc;
+  const double lam = lam_iso_ke(c->sys[s].prm, S.kinetic, c->sys[s].n);
+  DevCtx d = devctx(c);
+  launch_scale_vel(d, c->st, s, lam);
+  CK(c, cudaGetLastError());
+  CK(c, cudaStreamSynchronize(c->st));
+  return NDG_OK;
+}
+
+int ndg_mk_iso_e(ndg_ctx *c, int s) {
+  if (!valid_sys(c, s)) return NDG_ERR_ARG;
+  SysState S;
+  int rc = get_state_dev(c, s, S);
+  if (rc) return rc;
+  const double lam = lam_iso_e(c->sys[s].prm, S.e0, S.potential, S.kinetic);
+  DevCtx d = devctx(c);
+  launch_scale_vel(d, c->st, s, lam);
+  CK(c, cudaGetLastError());
+  CK(c, cudaStreamSynchronize(c->st));
+  return NDG_OK;
+}
+
+int ndg_mk_iso_p(ndg_ctx *c, int s) {
+  if (!valid_sys(c, s)) return NDG_ERR_ARG;
+  SysState S;
+  int rc = get_state_dev(c, s, S);
+  if (rc) return rc;
+  iso_p_box(c->sys[s].prm, S.virial, S.box);
+  for (int d = 0; d < 3; ++d) S.li[d] = 1.0 / S.box[d];
+  return put_state_dev(c, s, S);
+}
+
+int ndg_get_forces(ndg_ctx *c, int s, double *force, double *potential, double *virial,
+                   double *kinetic) {
+  if (!valid_sys(c, s)) return NDG_ERR_ARG;
+  CK(c, cudaStreamSynchronize(c->st));
+  HostSys &h = c->sys[s];
+  const int n = h.n;
+  const size_t off = (size_t)h.atoms.off * ATOM_ALIGN;
+  if (force) {
+    std::vector<int> g(n);
+    std::vector<double> f(3 * (size_t)n);
+    CK(c, cudaMemcpy(g.data(), c->gid + off, n * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(c, cudaMemcpy(f.data(), c->force + 3 * off, 3 * n * sizeof(double),
+                     cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; ++i)
+      for (int d = 0; d < 3; ++d) force[3 * g[i] + d] = f[3 * i + d];
+  }
+  SysState S;
+  int rc = get_state_dev(c, s, S);
+  if (rc) return rc;
+  if (potential) *potential = S.potential;
+  if (virial)
+    for (int k = 0; k < 6; ++k) virial[k] = S.virial[k];
+  if (kinetic) *kinetic = S.kinetic;
+  return NDG_OK;
+}
+
+static int run_impl(ndg_ctx *c, int nsteps, ndg_thermo_cb cb, void *user, int cont) {
+  if (!c || nsteps < 0) return NDG_ERR_ARG;
+  if (nsteps == 0) return NDG_OK;
+  cudaSetDevice(c->device);
+  int rc;
+  if (!cont || !lists_ready(c)) {
+    rc = setup_lists(c);
+    if (rc) return rc;
+    cont = 0;
+  } else if (c->params_dirty) {
+    rc = upload_params(c);
+    if (rc) return rc;
+  }
+  // controls may have changed between runs
+  for (auto &h : c->sys)
+    if (h.alive) fill_control_params(h);
+  rc = upload_params(c);
+  if (rc) return rc;
+  CK(c, cudaMemset(c->ring_count, 0, 2 * sizeof(int)));
+  DevCtx d = devctx(c);
+  launch_begin_run(d, c->st, c->nsys_cap, nsteps, cont);
+  CK(c, cudaGetLastError());
+  rc = run_steps(c, nsteps, cb, user);
+  int rf = flush_pending(c);
+  return rc ? rc : rf;
+}
+
+int ndg_run(ndg_ctx *c, int nsteps, ndg_thermo_cb cb, void *user) {
+  return run_impl(c, nsteps, cb, user, 0);
+}
+
+int ndg_run_continue(ndg_ctx *c, int nsteps, ndg_thermo_cb cb, void *user) {
+  return run_impl(c, nsteps, cb, user, 1);
+}
+
+int ndg_get_thermo(ndg_ctx *c, int s, ndg_thermo *t) {
+  if (!valid_sys(c, s) || !t) return NDG_ERR_ARG;
+  SysState S;
+  int rc = get_state_dev(c, s, S);
+  if (rc) return rc;
+  ThermoRec r;
+  make_thermo(r, s, S.step, S.potential, S.kinetic, S.e0, S.virial, S.box);
+  memcpy(t, &r, sizeof(r));
+  return NDG_OK;
+}
+
+int ndg_get_list_updates(ndg_ctx *c, int s, int *n) {
+  if (!valid_sys(c, s) || !n) return NDG_ERR_ARG;
+  SysState S;
+  int rc = get_state_dev(c, s, S);
+  if (rc) return rc;
+  *n = S.nlist_updates;
+  return NDG_OK;
+}
+
+int ndg_get_mcell(ndg_ctx *c, int s, int *m) {
+  if (!valid_sys(c, s) || !m) return NDG_ERR_ARG;
+  SysState S;
+  int rc = get_state_dev(c, s, S);
+  if (rc) return rc;
+  for (int d = 0; d < 3; ++d) m[d] = S.mcell[d];
+  return NDG_OK;
+}
+
+int ndg_get_cells(ndg_ctx *c, int s, int *cell) {
+  if (!valid_sys(c, s) || !cell || !c->sys[s].lists_valid) return NDG_ERR_ARG;
+  HostSys &h = c->sys[s];
+  const int n = h.n;
+  const size_t off = (size_t)h.atoms.off * ATOM_ALIGN;
+  std::vector<int> g(n), a(n);
+  CK(c, cudaStreamSynchronize(c->st));
+  CK(c, cudaMemcpy(g.data(), c->gid + off, n * sizeof(int), cudaMemcpyDeviceToHost));
+  CK(c, cudaMemcpy(a.data(), c->atom_cell + off, n * sizeof(int), cudaMemcpyDeviceToHost));
+  for (int i = 0; i < n; ++i) cell[g[i]] = a[i];
+  return NDG_OK;
+}
+
+int ndg_get_neighbors(ndg_ctx *c, int s, int *pairs, long long cap, long long *npairs) {
+  if (!valid_sys(c, s) || !c->sys[s].lists_valid) return NDG_ERR_ARG;
+  HostSys &h = c->sys[s];
+  const int n = h.n;
+  const size_t off = (size_t)h.atoms.off * ATOM_ALIGN;
+  const long long npad = h.atoms.len * ATOM_ALIGN;
+  CK(c, cudaStreamSynchronize(c->st));
+  std::vector<int> g(n), cnt(n);
+  std::vector<int> nb((size_t)h.maxnb * npad);
+  CK(c, cudaMemcpy(g.data(), c->gid + off, n * sizeof(int), cudaMemcpyDeviceToHost));
+  CK(c, cudaMemcpy(cnt.data(), c->nnb + off, n * sizeof(int), cudaMemcpyDeviceToHost));
+  CK(c, cudaMemcpy(nb.data(), c->nbr + h.nbr.off, nb.size() * sizeof(int),
+                   cudaMemcpyDeviceToHost));
+  long long m = 0;
+  for (int i = 0; i < n; ++i) {
+    const int k1 = std::min(cnt[i], h.maxnb);
+    for (int k = 0; k < k1; ++k) {
+      const int j = nb[(size_t)k * npad + i] - (int)off;
+      const int gi = g[i], gj = g[j];
+      if (gi < gj) {
+        if (pairs && m < cap) {
+          pairs[2 * m] = gi;
+          pairs[2 * m + 1] = gj;
+        }
+        ++m;
+      }
+    }
+  }
+  if (npairs) *npairs = m;
+  return NDG_OK;
+}
+
+int ndg_set_tuning(ndg_ctx *c, int tpa, int graph_steps) {
+  if (!c) return NDG_ERR_ARG;
+  if (tpa != 0 && tpa != 1 && tpa != 2 && tpa != 4 && tpa != 8 && tpa != 16 && tpa != 32)
+    return NDG_ERR_ARG;
+  if (graph_steps < 1) return NDG_ERR_ARG;
+  if (tpa != c->tpa || graph_steps != c->graph_steps) drop_graphs(c);
+  c->tpa = tpa;
+  if (graph_steps != c->graph_steps) {
+    c->graph_steps = graph_steps;
+    const int need = std::max(256, graph_steps * c->nsys_cap);
+    if (need > c->ring_cap) {
+      dfree(c->ring);
+      c->ring = dalloc<ThermoRec>(need);
+      if (!c->ring) return NDG_ERR_NOMEM;
+      c->ring_cap = need;
+    }
+  }
+  return NDG_OK;
+}
+
+int ndg_get_tuning(ndg_ctx *c, int *tpa, int *graph_steps) {
+  if (!c) return NDG_ERR_ARG;
+  if (tpa) *tpa = choose_tpa(c);
+  if (graph_steps) *graph_steps = c->graph_steps;
+  return NDG_OK;
+}
+
+int ndg_device_bytes(const ndg_ctx *c, long long *bytes) {
+  if (!c || !bytes) return NDG_ERR_ARG;
+  const long long A = c->atoms.cap * ATOM_ALIGN;
+  long long b = A * (2 * 32 + 16 + 4 * 24 + 2 * 24 + 4 * 10) + c->cells.cap * 12 +
+                c->nbrs.cap * 4 + (long long)c->nsys_cap * (sizeof(SysParam) + sizeof(SysState)) +
+                (long long)c->ring_cap * sizeof(ThermoRec);
+  *bytes = b;
+  return NDG_OK;
+}
+
+long long ndg_system_bytes(int np, int ntypes, int npairs, int ptsize, double density,
+                           double rlist, int precision) {
+  (void)ntypes;
+  (void)precision;
+  const long long npad = ((long long)np + ATOM_ALIGN - 1) / ATOM_ALIGN * ATOM_ALIGN;
+  const double r = rlist * 1.1;
+  const long long maxnb =
+      (long long)(4.0 / 3.0 * 3.141592653589793 * r * r * r * density * 1.2 * 2.0) + 24;
+  const long long per_atom = 2 * 32 + 16 + 4 * 24 + 2 * 24 + 4 * 10;
+  const long long ncell = (long long)(np / std::max(density * rlist * rlist * rlist, 1e-9)) + 8;
+  return npad * per_atom + npad * maxnb * 4 + ncell * 12 +
+         (long long)npairs * (ptsize + 1) * 32;
+}
+
+int ndg_autotune(ndg_ctx *c, int steps) {
+  (void)steps;
+  return c ? NDG_OK : NDG_ERR_ARG;
+}
+
+int ndg_get_kernel_times(ndg_ctx *c, double *ti, double *tp, double *tr, int *launches) {
+  if (!c) return NDG_ERR_ARG;
+  if (ti) *ti = c->t_int;
+  if (tp) *tp = c->t_pair;
+  if (tr) *tr = c->t_reb;
+  if (launches) *launches = c->t_launches;
+  return NDG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,97 @@
+// ndg_kernels.h -- kernel launch interface of the Ndyn timestep library.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "ndg_common.h"
+
+namespace ndg {
+
+// Everything a kernel needs, passed by value (pointers into the arenas).
+struct DevCtx {
+  const SysParam *P;
+  SysState *S;
+  const int *chunk_sys;  // per ATOM_ALIGN-atom chunk: system id or -1
+  const int *cell_sys;   // per global cell: system id or -1
+  int nchunks, ncells, nsys_cap;
+  double4 *pos;
+  int4 *pfx;
+  double *vel, *acc, *disp, *force;
+  int *gid;
+  int *nbr, *nnb;
+  int *atom_cell, *atom_slot, *cell_count, *cell_start;
+  int *perm, *tmp_src, *tmp_key;
+  double4 *s_pos;
+  double *s_vel, *s_acc;
+  int *s_gid, *s_cell;
+  const int *pairmat;
+  const double *mass, *rc2, *rlist2;
+  const float *vdr2, *rc2f;
+  const double *tabF, *tabP;
+  const float2 *tabF2, *tabP2;
+  double *red;   // pair-kernel block partials, 8 per block
+  double *itop;  // integrate1 chunk partials, 2 per chunk
+  double *ired;  // integrate2 (standalone) chunk partials
+  ThermoRec *ring;
+  int *ring_count;  // [0] records written, [1] error bits of any system
+  int ring_cap;
+};
+
+// launchers (stream-ordered; safe to capture in a CUDA graph)
+void launch_integrate1(const DevCtx &c, cudaStream_t st, int standalone, int mixed);
+void launch_pair(const DevCtx &c, cudaStream_t st, int tpa, int mixed, int fuse, int host_flags);
+void launch_integrate2(const DevCtx &c, cudaStream_t st, int ck);
+void launch_rebuild(const DevCtx &c, cudaStream_t st, int force_all, int mixed);
+void launch_begin_run(const DevCtx &c, cudaStream_t st, int nsys_cap, int nsteps, int cont);
+void launch_flush(const DevCtx &c, cudaStream_t st, int nsys_cap);
+void launch_check(const DevCtx &c, cudaStream_t st, int nsys_cap);
+void launch_scale_vel(const DevCtx &c, cudaStream_t st, int sys, double lam);
+void launch_refresh_pfx(const DevCtx &c, cudaStream_t st);
+
+// stencil of neighbour cells for a link-cell grid (shared host/device)
+NDG_HD int make_stencil(const int *mcell, int quirk, int *out) {
+  // the 13 forward offsets of getJcellNP cases 2..14, src/nd.f90:1270-1282
+  const int fwd[13][3] = {{0, 0, 1}, {0, 1, 0},  {0, 1, -1},  {0, 1, 1},  {1, 0, 0},
+                          {1, 0, -1}, {1, 0, 1}, {1, 1, 0},   {1, 1, -1}, {1, 1, 1},
+                          {1, -1, 0}, {1, -1, -1}, {1, -1, 1}};
+  int n = 0;
+  out[n++] = (1) | (1 << 4) | (1 << 8) | (1 << 12);  // the cell itself
+  int seen[27][3];
+  int nseen = 0;
+  for (int dz = -1; dz <= 1; ++dz)
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dx = -1; dx <= 1; ++dx) {
+        if (!dx && !dy && !dz) continue;
+        const int o[3] = {dx, dy, dz};
+        int f[3];
+        for (int d = 0; d < 3; ++d) f[d] = ((o[d] % mcell[d]) + mcell[d]) % mcell[d];
+        if (!f[0] && !f[1] && !f[2]) continue;  // folds onto itself (1 cell)
+        bool dup = false;
+        for (int q = 0; q < nseen; ++q)
+          dup |= seen[q][0] == f[0] && seen[q][1] == f[1] && seen[q][2] == f[2];
+        if (dup) continue;
+        seen[nseen][0] = f[0];
+        seen[nseen][1] = f[1];
+        seen[nseen][2] = f[2];
+        ++nseen;
+        int mult = 1;
+        if (quirk == 0) {
+          // times the reference's half stencil reaches this cell from either
+          // side: forward offsets equal to +f or to -f modulo the cell count
+          mult = 0;
+          for (int k = 0; k < 13; ++k) {
+            bool pos = true, neg = true;
+            for (int d = 0; d < 3; ++d) {
+              int t = ((fwd[k][d] % mcell[d]) + mcell[d]) % mcell[d];
+              pos &= t == f[d];
+              neg &= t == (mcell[d] - f[d]) % mcell[d];
+            }
+            mult += pos + neg;
+          }
+        }
+        for (int m = 0; m < mult && n < MAX_STENCIL; ++m)
+          out[n++] = (dx + 1) | ((dy + 1) << 4) | ((dz + 1) << 8);
+      }
+  return n;
+}
+
+}  // namespace ndg

@@ -1,0 +1,246 @@
+"""GPU parity: the CUDA library (through its C ABI) against the CPU oracle on
+identical seeded inputs.
+
+Bars (stated per test):
+  * link-cell assignment and neighbour pairs: bit-exact (cells equal, pair
+    multisets equal, both in the reference semantics and the fixed one);
+  * FP64 path: per-atom forces within 1e-12 relative L2 of the oracle
+    (only the summation order differs), PE/virial within 1e-12;
+  * mixed path: forces within 1e-5 relative L2 (the stated force error),
+    PE within 1e-6, virial within 1e-5;
+  * integrate1 bit-exact; full runs follow the oracle's thermo rows.
+"""
+import numpy as np
+import pytest
+
+from helpers import gpu_from_spec, oracle_from_spec, pair_multiset, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+nd = pytest.importorskip("ndyn_omp_b200")
+from ndyn_omp_b200 import workloads as W  # noqa: E402
+
+
+def small_specs():
+    return {
+        "cu_ref": W.cu_crystal(8, 300.0, seed=11, quirk="ref"),          # 2048 atoms, M=4
+        "ar_fixed": W.ar_liquid(6, 120.0, seed=12, quirk="fixed"),        # 864 atoms, M=3
+        "nacl_fixed": W.nacl_solid((6, 6, 6), 600.0, seed=13, quirk="fixed"),  # 1728 atoms
+        "cu_m2_ref": W.cu_crystal(5, 900.0, seed=14, quirk="ref"),        # 500 atoms, M=2
+        "cu_m2_fixed": W.cu_crystal(5, 900.0, seed=14, quirk="fixed"),
+    }
+
+
+def _jitter(spec, amp, seed):
+    rng = np.random.default_rng(seed)
+    spec = dict(spec)
+    spec["pos"] = W.jitter(spec["pos"], spec["box"], amp, rng)
+    return spec
+
+
+@pytest.fixture(scope="module")
+def specs():
+    s = small_specs()
+    s["cu_ref"] = _jitter(s["cu_ref"], 0.05, 99)
+    return s
+
+
+@pytest.mark.parametrize("name", ["cu_ref", "ar_fixed", "nacl_fixed", "cu_m2_ref", "cu_m2_fixed"])
+def test_cells_and_neighbour_pairs_bit_exact(specs, name):
+    spec = specs[name]
+    o = oracle_from_spec(spec)
+    assert o.setup_lists() == 0
+    with nd.Context(0, "fp64") as ctx:
+        sid = gpu_from_spec(ctx, spec)
+        ctx.setup_lists()
+        assert list(ctx.mcell(sid)) == list(o.mcell())
+        assert np.array_equal(ctx.cells(sid), o.cells()), "link-cell assignment differs"
+        g = pair_multiset(ctx.neighbors(sid))
+        r = pair_multiset(o.neighbors())
+        assert len(g) == len(r)
+        assert np.array_equal(g, r), "neighbour pair multiset differs"
+    if name == "cu_m2_ref":
+        # 2 link cells per direction: the reference stencil repeats pairs
+        assert len(r) > len(np.unique(r))
+    if name == "cu_m2_fixed":
+        assert len(r) == len(np.unique(r))
+
+
+@pytest.mark.parametrize("name", ["cu_ref", "ar_fixed", "nacl_fixed", "cu_m2_ref"])
+def test_compute0_fp64(specs, name):
+    spec = specs[name]
+    o = oracle_from_spec(spec)
+    o.setup_lists()
+    o.compute0(1, 1)
+    fo, peo, viro, _ = o.forces()
+    with nd.Context(0, "fp64") as ctx:
+        sid = gpu_from_spec(ctx, spec)
+        ctx.setup_lists()
+        ctx.compute0(True, True)
+        fg, peg, virg, _ = ctx.forces(sid)
+    assert rel_l2(fg, fo) < 1e-12
+    assert abs(peg - peo) <= 1e-12 * abs(peo)
+    assert rel_l2(virg, viro) < 1e-12
+
+
+@pytest.mark.parametrize("name", ["cu_ref", "ar_fixed", "nacl_fixed"])
+def test_compute0_mixed_force_error(specs, name):
+    """Mixed precision: FP32 pair math + 64-bit fixed-point sums; the
+    stated bar is 1e-5 relative L2 force error against the FP64 oracle."""
+    spec = specs[name]
+    o = oracle_from_spec(spec)
+    o.setup_lists()
+    o.compute0(1, 1)
+    fo, peo, viro, _ = o.forces()
+    with nd.Context(0, "mixed") as ctx:
+        sid = gpu_from_spec(ctx, spec)
+        ctx.setup_lists()
+        ctx.compute0(True, True)
+        fg, peg, virg, _ = ctx.forces(sid)
+    err = rel_l2(fg, fo)
+    assert err < 1e-5, err
+    assert abs(peg - peo) <= 1e-6 * abs(peo)
+    assert rel_l2(virg, viro) < 1e-5
+
+
+def test_integrate1_bit_exact(specs):
+    spec = dict(specs["ar_fixed"])
+    rng = np.random.default_rng(5)
+    spec["acc"] = rng.standard_normal(spec["pos"].shape) * 1e-3
+    o = oracle_from_spec(spec)
+    o.setup_lists()
+    o.integrate1()
+    po, _, _, _ = o.state()
+    with nd.Context(0, "fp64") as ctx:
+        sid = gpu_from_spec(ctx, spec)
+        ctx.setup_lists()
+        ctx.integrate1()
+        pg, _, _, _ = ctx.state(sid)
+    assert np.array_equal(pg, po)
+
+
+def test_routines_step_by_step_match_oracle(specs):
+    """integrate1 -> compute0 -> integrate2 -> mkIsoKE -> mkIsoP called one
+    by one through the ABI, as dynamics calls them."""
+    spec = dict(specs["nacl_fixed"])
+    o = oracle_from_spec(spec)
+    o.setup_lists()
+    with nd.Context(0, "fp64") as ctx:
+        sid = gpu_from_spec(ctx, spec)
+        ctx.setup_lists()
+        for _ in range(3):
+            o.check_list_update()
+            ctx.check_list_update()
+            o.integrate1()
+            ctx.integrate1()
+            o.compute0(1, 1)
+            ctx.compute0(True, True)
+            o.integrate2(1)
+            ctx.integrate2(True)
+            o.L.ora_mk_iso_ke(o.s)
+            ctx.mk_iso_ke(sid)
+            o.L.ora_mk_iso_p(o.s)
+            ctx.mk_iso_p(sid)
+        po, vo, ao, bo = o.state()
+        pg, vg, ag, bg = ctx.state(sid)
+        _, peo, viro, keo = o.forces()
+        _, peg, virg, keg = ctx.forces(sid)
+    assert rel_l2(pg, po) < 1e-13
+    assert rel_l2(vg, vo) < 1e-10
+    assert rel_l2(bg, bo) < 1e-13
+    assert abs(keg - keo) <= 1e-10 * abs(keo)
+    assert abs(peg - peo) <= 1e-12 * abs(peo)
+
+
+def _run_both(spec, nsteps, precision="fp64", threads=None):
+    o = oracle_from_spec(spec, threads=threads)
+    rc, rows_o = o.run(nsteps, spec["control"]["dt"])
+    assert rc == 0
+    with nd.Context(0, precision) as ctx:
+        sid = gpu_from_spec(ctx, spec)
+        rows_g = ctx.run(nsteps)
+        st = ctx.state(sid)
+        nup = ctx.list_updates(sid)
+    return o, rows_o, rows_g, st, nup
+
+
+def test_run_nve_crystal_fp64(specs):
+    spec = specs["cu_ref"]
+    spec = dict(spec)
+    spec["control"] = dict(spec["control"], out_steps=10)
+    o, ro, rg, (pg, vg, _, _), nup = _run_both(spec, 100)
+    assert [r["step"] for r in rg] == [r["step"] for r in ro]
+    for a, b in zip(rg, ro):
+        assert a["pe"] == pytest.approx(b["pe"], rel=1e-11)
+        assert a["ke"] == pytest.approx(b["ke"], rel=1e-9)
+        assert a["press"] == pytest.approx(b["press"], rel=1e-9, abs=1e-12)
+        assert a["vol"] == b["vol"]
+    po, vo, _, _ = o.state()
+    assert rel_l2(pg, po) < 1e-12
+    assert nup == o.list_updates
+
+
+def test_run_nvt_liquid_fixed_rebuilds(specs):
+    """LJ liquid with the fixed rebuild criterion: lists are rebuilt on the
+    same steps as the oracle and the thermostat trajectory follows it."""
+    spec = dict(specs["ar_fixed"])
+    spec["control"] = dict(spec["control"], out_steps=20)
+    o, ro, rg, _, nup = _run_both(spec, 200)
+    assert nup == o.list_updates and nup > 0
+    for a, b in zip(rg, ro):
+        assert a["pe"] == pytest.approx(b["pe"], rel=1e-8)
+        assert a["ke"] == pytest.approx(b["ke"], rel=1e-8)
+
+
+def test_run_npt_barostat(specs):
+    spec = dict(specs["nacl_fixed"])
+    spec["control"] = dict(spec["control"], out_steps=25)
+    o, ro, rg, (_, _, _, box), _ = _run_both(spec, 100)
+    _, _, _, bo = o.state()
+    assert np.allclose(box, bo, rtol=1e-12)
+    for a, b in zip(rg, ro):
+        assert a["vol"] == pytest.approx(b["vol"], rel=1e-12)
+        assert a["press"] == pytest.approx(b["press"], rel=1e-8, abs=1e-12)
+
+
+def test_run_skin0_rebuilds_every_step():
+    """Reference semantics with skin 0: CheckListUpdate fires every step
+    (examples/testCAF/OMP_4/out reports 98 updates in 100 steps)."""
+    spec = W.cu_crystal(6, 300.0, seed=21, quirk="ref")
+    spec["control"] = dict(spec["control"], skin=0.0, out_steps=10)
+    o, ro, rg, _, nup = _run_both(spec, 30)
+    assert nup == o.list_updates
+    assert nup >= 28
+    for a, b in zip(rg, ro):
+        assert a["pe"] == pytest.approx(b["pe"], rel=1e-11)
+
+
+def test_batch_equals_alone(specs):
+    """Several systems in one context (one launch per kernel) give bitwise
+    the same trajectories as each system alone."""
+    names = ["cu_ref", "ar_fixed", "nacl_fixed", "cu_m2_ref"]
+    alone = {}
+    for n in names:
+        with nd.Context(0, "mixed") as ctx:
+            sid = gpu_from_spec(ctx, specs[n])
+            ctx.run(50)
+            alone[n] = ctx.state(sid)
+    with nd.Context(0, "mixed") as ctx:
+        ids = {n: gpu_from_spec(ctx, specs[n]) for n in names}
+        ctx.run(50)
+        for n in names:
+            got = ctx.state(ids[n])
+            for a, b in zip(got, alone[n]):
+                assert np.array_equal(a, b), n
+
+
+def test_deterministic_repeat(specs):
+    out = []
+    for _ in range(2):
+        with nd.Context(0, "fp64") as ctx:
+            sid = gpu_from_spec(ctx, specs["ar_fixed"])
+            rows = ctx.run(60)
+            out.append((ctx.state(sid), rows))
+    for a, b in zip(out[0][0], out[1][0]):
+        assert np.array_equal(a, b)
+    assert out[0][1] == out[1][1]
