@@ -1,0 +1,415 @@
+"""Benchmark of the Ndyn MD timestep path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c2]
+                    [--impl ours|reference] [--precision mixed|fp64]
+
+A step is one MD timestep (the dynamics loop body, src/nd.f90:138-178) of
+the configured system.  Default workload (c2): LJ argon liquid, 256,000
+atoms on a +-0.05 sigma jittered FCC lattice at reduced density 0.8442,
+Berendsen thermostat to 120 K (tau = 100 steps), dt = 0.1, mixed precision,
+fixed list-rebuild semantics.  Other workloads: c1 (Cu Morse crystal 4000
+atoms, FP64, NVE), c3 (rocksalt Buckingham 1,048,576 atoms, NPT), c4 (512
+replicas in one launch).
+
+Multi-GPU: the workload does not shard (one system per GPU, no exchange),
+so N ranks run N independent replicas ("replicas only"): value is the
+aggregate atom-steps/s, time is the max over ranks.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+MEASURED = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+L2_BYTES = 126e6
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default=None, choices=["mixed", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tpa", type=int, default=0, help="threads per atom (0 = library choice)")
+    ap.add_argument("--graph-steps", type=int, default=100,
+                    help="steps per CUDA graph (1 = eager launches, as ncu needs)")
+    return ap.parse_args()
+
+
+def workload(cfg, scale_cells=None):
+    from ndyn_omp_b200 import workloads as W
+    if cfg == "c1":
+        return [W.cu_crystal(scale_cells or 10, 300.0, seed=1, quirk="ref")], "fp64"
+    if cfg == "c2":
+        return [W.ar_liquid(scale_cells or 40, 120.0, seed=2, quirk="fixed")], "mixed"
+    if cfg == "c3":
+        c = scale_cells or (64, 64, 32)
+        return [W.nacl_solid(c, 600.0, seed=3, quirk="fixed")], "mixed"
+    return W.replica_ensemble(512, seed=4, quirk="fixed"), "mixed"
+
+
+WORKLOAD_TEXT = {
+    "c1": "Cu FCC 10^3 cells (4000 atoms) Morse D=0.3429 a=1.3588 r0=2.866 rc=6.0 skin 0.5, "
+          "NVE, FP64, reference list semantics",
+    "c2": "LJ argon liquid 256000 atoms (FCC 40^3, rho*=0.8442, +-0.05 sigma jitter), "
+          "eps=0.0104 sigma=3.405 rc=2.5 sigma skin=0.3 sigma, Berendsen 120 K tau=100 steps",
+    "c3": "rocksalt Buckingham 1048576 atoms (64x64x32 cells, a=5.64, +-0.02 A), rc=8 "
+          "skin 1.6, thermostat 600 K + barostat P=0 (Pparm 10)",
+    "c4": "512 replicas (half Cu Morse crystals, half LJ Ar liquids), N log-uniform "
+          "[500,20000] in whole FCC cells, T uniform [100,1500] K, own thermostats",
+}
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """NVML sampling of SM clock and throttle reasons while timing."""
+
+    REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap",
+               0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting"}
+
+    def __init__(self, index):
+        self.samples, self.reasons, self.ok = [], 0, False
+        self.max_mhz = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            # NVML numbers all GPUs of the node; find ours by PCI bus id
+            p = torch.cuda.get_device_properties(index)
+            bus = "%08X:%02X:%02X.0" % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)
+            self.h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            self.ok = False
+        self._stop = threading.Event()
+
+    def _loop(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+                self.reasons |= self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+            except Exception:
+                pass
+            time.sleep(0.005)
+
+    def __enter__(self):
+        if self.ok:
+            self.t = threading.Thread(target=self._loop, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self.ok:
+            self._stop.set()
+            self.t.join()
+
+    def summary(self):
+        if not self.ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"],
+                    "samples": 0}
+        rs = [n for b, n in self.REASONS.items() if self.reasons & b and n != "gpu_idle"]
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": rs, "samples": len(self.samples)}
+
+
+def hbm_peak():
+    try:
+        return float(json.load(open(MEASURED))["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_per_atom(cfg):
+    """DRAM bytes per atom of one pair-kernel launch from the committed ncu
+    summary (profiles/), or None."""
+    p = os.path.join(ROOT, "profiles", f"k_pair_{cfg}_traffic.txt")
+    try:
+        for ln in open(p):
+            if ln.startswith("dram_bytes_per_atom:"):
+                return float(ln.split(":")[1])
+    except OSError:
+        return None
+    return None
+
+
+# ---------------------------------------------------------------------------
+def cpu_rate(spec, target_s, threads=None, fixed_steps=None):
+    """Oracle (the reference's FP64 OpenMP path restated) on the host cores:
+    setup untimed, then the step loop timed.  Returns (atom-steps/s, steps,
+    seconds, threads)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_py
+    from helpers import oracle_from_spec
+    threads = threads or os.cpu_count()
+    o = oracle_from_spec(spec, threads=threads)
+    assert o.setup_lists() == 0
+    dt = spec["control"]["dt"]
+    if fixed_steps is None:
+        t0 = time.perf_counter()
+        rc, _ = o.run(1, dt, loop_only=True)
+        t1 = time.perf_counter() - t0
+        steps = int(max(2, min(200, target_s / max(t1, 1e-6))))
+    else:
+        steps = fixed_steps
+    t0 = time.perf_counter()
+    rc, _ = o.run(steps, dt, loop_only=True)
+    el = time.perf_counter() - t0
+    assert rc == 0, rc
+    n = len(spec["typ"])
+    return n * steps / el, steps, el, threads
+
+
+def n_atoms(specs):
+    return sum(len(s["typ"]) for s in specs)
+
+
+# ---------------------------------------------------------------------------
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allmax(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_reference(args, ws, rank):
+    """--impl reference: the reference's CPU path (the oracle port; the
+    Fortran reference cannot be compiled in this image) on all host threads,
+    same workload, metric and unit.  Each step is one MD step of a bounded
+    sample of the workload."""
+    if rank != 0:
+        return
+    specs, _ = workload(args.config)
+    threads = os.cpu_count()
+    budget = 150.0
+    # calibrate on a small sample of the same material, then size the sample
+    # so the K+W steps fit the budget
+    if args.config in ("c2", "c1"):
+        base = 40 if args.config == "c2" else 10
+        probe_cells = 12 if args.config == "c2" else 6
+        probe = workload(args.config, probe_cells)[0][0]
+        r, _, _, _ = cpu_rate(probe, 2.0, threads)
+        want_atoms = r * budget / max(args.steps + args.warmup, 1)
+        cells = int(min(base, max(6, round((want_atoms / 4) ** (1 / 3)))))
+        sample = workload(args.config, cells)[0][0]
+        sample_txt = f"{len(sample['typ'])} atoms ({cells}^3 FCC cells) of the same liquid"
+    elif args.config == "c3":
+        probe = workload("c3", (8, 8, 8))[0][0]
+        r, _, _, _ = cpu_rate(probe, 2.0, threads)
+        want_atoms = r * budget / max(args.steps + args.warmup, 1)
+        n = int(min(64, max(6, round((want_atoms / 8) ** (1 / 3)))))
+        sample = workload("c3", (n, n, n))[0][0]
+        sample_txt = f"{len(sample['typ'])} atoms ({n}^3 rocksalt cells)"
+    else:
+        # c4: replicas run one after another (the plain path in sequence)
+        sample = specs[1]
+        sample_txt = f"replica 1 of 512 ({len(sample['typ'])} atoms)"
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import oracle_from_spec
+    o = oracle_from_spec(sample, threads=threads)
+    assert o.setup_lists() == 0
+    dt = sample["control"]["dt"]
+    if args.warmup:
+        o.run(args.warmup, dt, loop_only=True)
+    t0 = time.perf_counter()
+    rc, _ = o.run(args.steps, dt, loop_only=True)
+    el = time.perf_counter() - t0
+    assert rc == 0
+    n = len(sample["typ"])
+    v = n * args.steps / el
+    line = {
+        "impl": "reference", "metric": "atom-steps/s", "value": v, "unit": "atom-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_TEXT[args.config], "sample": sample_txt},
+        "cpu_baseline": {"value": v, "unit": "atom-steps/s", "cores": threads, "kind": "port",
+                         "sample": sample_txt + f", {args.steps} steps"},
+        "e2e": {"value": v, "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_init()
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    import torch
+
+    import ndyn_omp_b200 as nd
+    from ndyn_omp_b200 import workloads as W
+    torch.cuda.set_device(local)
+    specs, prec = workload(args.config)
+    prec = args.precision or prec
+    N = n_atoms(specs)
+
+    # stated force error of this precision against the FP64 path (the FP64
+    # path itself matches the CPU oracle to 1e-12, tests/test_gpu_parity.py)
+    force_err = None
+    if prec == "mixed":
+        fs = {}
+        probe = specs[:1] if args.config != "c4" else specs[:8]
+        for p in ("fp64", "mixed"):
+            with nd.Context(local, p) as cx:
+                ids = [W.add_to_context(cx, s) for s in probe]
+                cx.setup_lists()
+                cx.compute0(True, True)
+                fs[p] = np.concatenate([cx.forces(i)[0].ravel() for i in ids])
+        force_err = float(np.linalg.norm(fs["mixed"] - fs["fp64"]) / np.linalg.norm(fs["fp64"]))
+
+    ctx = nd.Context(local, prec)
+    ids = [W.add_to_context(ctx, s) for s in specs]
+    ctx.set_tuning(args.tpa, args.graph_steps)
+    if args.config == "c4":
+        ctx.autotune(10)
+    # warm-up (includes the dynamics prologue: cell + Verlet list build)
+    ctx.run(max(args.warmup, 3))
+    nb_half = None
+    if args.config != "c4":
+        nb_half = len(ctx.neighbors(ids[0])) / len(specs[0]["typ"])
+    s = torch.cuda.ExternalStream(ctx.stream_ptr)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(ws)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        e0.record(s)
+        ctx.run(args.steps, cont=True)
+        e1.record(s)
+        torch.cuda.synchronize()
+    barrier(ws)
+    ms = e0.elapsed_time(e1)
+    ms = allmax(ms, ws)
+    value = N * args.steps * ws / (ms / 1e3)
+    clocks = clk.summary()
+
+    # per-kernel mean launch time over the same kind of steps (eager launches
+    # with CUDA events on the library's stream)
+    prof = ctx.profile_run(min(200, max(20, args.steps // 10)))
+    tpa, gsteps = ctx.tuning()
+    peak, peak_kind = hbm_peak()
+    roof = None
+    if nb_half is not None:
+        # algorithmic bytes of the fused pair kernel per atom: half-list
+        # indices 4*n_half + own position/type 28 + neighbour positions 24
+        # (each read once) + integrate2 state (read vel, acc; write vel, acc) 96
+        alg_atom = 4.0 * nb_half + 148.0
+        achieved = N * alg_atom / (prof["pair_ms"] / 1e3) / 1e9
+        tr = traffic_per_atom(args.config)
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": (tr * N if tr else None),
+                "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+                "alg_bytes_per_atom": alg_atom, "n_half": nb_half,
+                "pair_ms": prof["pair_ms"], "integrate_ms": prof["integrate_ms"],
+                "rebuild_ms_per_step": prof["rebuild_ms"]}
+
+    # end to end through the C ABI with host buffers: load state, run, read
+    # state back (what a caller of ndg_load_state/ndg_run/ndg_get_state pays)
+    e2e = None
+    if args.config != "c4":
+        sp = specs[0]
+        pos0, vel0, acc0, box0 = ctx.state(ids[0])
+        pin = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+               for a in (pos0, vel0, acc0)]
+        barrier(ws)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.load_state(ids[0], pin[0], pin[1], pin[2], box0)
+        rows = ctx.run(args.steps)
+        out = ctx.state(ids[0])
+        torch.cuda.synchronize()
+        el = allmax(time.perf_counter() - t0, ws)
+        n = len(sp["typ"])
+        h2d = n * (32 + 24 * 3 + 4)            # pos(+type) double4, vel, acc, disp, gid
+        d2h = n * (36 + 4 + 32 + 24 * 2) + 120 * len(rows)  # types for load, gid, pos, vel, acc, thermo
+        e2e = {"value": n * args.steps * ws / el, "unit": "atom-steps/s",
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+               "what": "ndg_load_state + ndg_run(K) (incl. list build) + ndg_get_state"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        sample = specs[0] if args.config != "c4" else specs[1]
+        if args.config == "c3":
+            sample = workload("c3", (24, 24, 24))[0][0]
+        r, st, el, th = cpu_rate(sample, 15.0)
+        cpu = {"value": r, "unit": "atom-steps/s", "cores": th, "kind": "port",
+               "sample": f"{len(sample['typ'])} atoms x {st} steps ({el:.1f} s), "
+                         f"oracle restatement of the reference OpenMP FP64 loop"}
+
+    touched = N * (4.0 * 2 * (nb_half or 40) + 200.0)
+    line = {
+        "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 pair math + i64 fixed-point sums + f64 integrator" if prec == "mixed"
+        else "f64",
+        "data": "synthetic (seeded lattice + Maxwell-Boltzmann velocities)",
+        "config": {"workload": WORKLOAD_TEXT[args.config], "atoms": N, "precision": prec,
+                   "list_semantics": specs[0]["control"].get("quirk", "ref"),
+                   "parallelism": f"replicas x{ws} (one system per GPU)" if ws > 1 else "1 GPU",
+                   "l2": f"inputs larger than L2: ~{touched / 1e6:.0f} MB touched per step "
+                         f"vs 126 MB L2" if touched > L2_BYTES else "L2-resident workload",
+                   "threads_per_atom": tpa, "graph_steps": gsteps,
+                   "baseline_metric": "atom-steps/s at 1 GPU, batched mixed vs plain FP64 at "
+                                      "stated force error; p50/p99"},
+        "force_rel_err_vs_fp64": force_err,
+        "gpu_launches": 9 * args.steps + 3,
+        "clocks": clocks,
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -212,7 +212,12 @@ int ndg_device_bytes(const ndg_ctx *ctx, long long *bytes);
 long long ndg_system_bytes(int np, int ntypes, int npairs, int ptsize,
                            double density, double rlist, int precision);
 
-/* per-kernel timing of the last ndg_run block (ms, CUDA events) */
+/* the CUDA stream every kernel of ctx is launched on (cudaStream_t) */
+int ndg_get_stream(ndg_ctx *ctx, void **stream);
+/* Continue the run for nsteps with eager launches and a CUDA event pair
+ * around every kernel group; the mean duration per launch is then read with
+ * ndg_get_kernel_times (integrate1, pair loop, list-rebuild group). */
+int ndg_profile_run(ndg_ctx *ctx, int nsteps);
 int ndg_get_kernel_times(ndg_ctx *ctx, double *integrate_ms, double *pair_ms,
                          double *rebuild_ms, int *launches);
 

@@ -51,6 +51,8 @@ SIGNATURES = [
     ("ndg_device_bytes", i, [vp, vp]),
     ("ndg_system_bytes", ll, [i, i, i, i, d, d, i]),
     ("ndg_get_kernel_times", i, [vp, vp, vp, vp, vp]),
+    ("ndg_get_stream", i, [vp, vp]),
+    ("ndg_profile_run", i, [vp, i]),
 ]
 
 

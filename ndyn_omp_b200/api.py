@@ -279,6 +279,25 @@ class Context:
             "get_neighbors")
         return pairs[:2 * n.value].reshape(-1, 2)
 
+    # -- timing -----------------------------------------------------------------
+    @property
+    def stream_ptr(self):
+        """cudaStream_t of the library's launches (for CUDA events)"""
+        p = ctypes.c_void_p()
+        _ok(self.L.ndg_get_stream(self._c, ctypes.byref(p)), "get_stream")
+        return p.value
+
+    def profile_run(self, nsteps):
+        """continue the run eagerly with events around each kernel group;
+        returns mean ms per launch (integrate1, pair, rebuild group)"""
+        _ok(self.L.ndg_profile_run(self._c, int(nsteps)), "profile_run")
+        ti, tp, tr = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        n = ctypes.c_int()
+        _ok(self.L.ndg_get_kernel_times(self._c, ctypes.byref(ti), ctypes.byref(tp),
+                                        ctypes.byref(tr), ctypes.byref(n)), "kernel_times")
+        return dict(integrate_ms=ti.value, pair_ms=tp.value, rebuild_ms=tr.value,
+                    launches=n.value)
+
     # -- tuning ---------------------------------------------------------------
     def set_tuning(self, tpa=0, graph_steps=100):
         _ok(self.L.ndg_set_tuning(self._c, int(tpa), int(graph_steps)), "set_tuning")

@@ -12,8 +12,10 @@
 //           fractions of the box (2^32 = one box length; integer wrap-around
 //           is the periodic minimum image), w as in pos.
 //   * vel, acc, disp, force: (3,np) FP64, the reference's own layout.
-//   * nbr   full neighbour list, padded SoA per system:
-//           nbr[nbr_off + k*npad + local_i], k < maxnb; nnb[i] = count.
+//   * nbr   full neighbour list, blocked SoA per system: tiles of 32 atoms,
+//           nbr[nbr_off + (local_i/32)*maxnb*32 + k*32 + local_i%32],
+//           k < maxnb; nnb[i] = count.  A tile's list is one contiguous
+//           region, so the pair kernel streams it with dense DRAM access.
 //   * atoms are kept sorted by link cell (cell-major, original id inside a
 //     cell); gid[i] maps back to the caller's order.
 #pragma once
@@ -31,6 +33,7 @@ constexpr int ATOM_ALIGN = 256;   // padding unit of a system's atom range
 constexpr int BLOCK = 256;        // threads of the atom-parallel kernels
 constexpr int MAX_STENCIL = 27;   // neighbour-cell entries incl. repeats
 constexpr int MAX_TYPES = 64;
+constexpr int NB_TILE = 32;       // atoms per tile of the blocked neighbour list
 constexpr double FX_ONE = 4294967296.0;  // 2^32: one box length in pfx units
 constexpr double FORCE_FX = 4294967296.0; // 2^32 fixed-point units per eV/A
 
@@ -84,6 +87,8 @@ struct SysState {
   int pend;              // bit0: lam_ke pending, bit1: lam_e pending
   int rebuild;           // rebuild lists before the next integrate1
   int nlist_updates;
+  int nstencil;                  // neighbour-cell stencil of the current grid
+  int stencil[MAX_STENCIL];
   int err;
   unsigned int ticket;   // last-block election of the pair kernel
   unsigned int ticket_i; // last-block election of integrate2 (standalone)

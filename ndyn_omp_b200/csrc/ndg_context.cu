@@ -89,6 +89,7 @@ T *dalloc(size_t n) {
 struct ndg_ctx {
   int device = 0, precision = NDG_PREC_FP64;
   cudaStream_t st = nullptr;
+  cudaStream_t st2 = nullptr;  // captures the conditional rebuild bodies
   std::string last_err;
   std::vector<HostSys> sys;
   // arenas
@@ -109,6 +110,9 @@ struct ndg_ctx {
       *tmp_key = nullptr;
   int *cell_count = nullptr, *cell_start = nullptr;
   int *nbr = nullptr;
+  int *tile_rows = nullptr;
+  int *tile_nc = nullptr, *tile_cell = nullptr, *tile_coff = nullptr;
+  int cand_cap = 6144;  // candidates a tile stages in the pair kernel
   double *red = nullptr, *itop = nullptr, *ired = nullptr;
   int *pairmat = nullptr;
   double *mass = nullptr, *rc2 = nullptr, *rlist2 = nullptr;
@@ -122,6 +126,9 @@ struct ndg_ctx {
   bool params_dirty = true;
   // tuning and graphs
   int tpa = 0, graph_steps = 100;
+  int stab_smem = 0;  // staged-table bytes of the pair kernel (0: tables from global)
+  int nb_smem = 0;  // neighbour-build dynamic smem
+  int one_pair = 0;  // every system has one type and one pair (pair-kernel variant)
   std::map<int, cudaGraphExec_t> graphs;
   // per-kernel timing of the last profiled block
   double t_int = 0, t_pair = 0, t_reb = 0;
@@ -173,6 +180,12 @@ DevCtx devctx(ndg_ctx *c) {
   d.force = c->force;
   d.gid = c->gid;
   d.nbr = c->nbr;
+  d.tile_rows = c->tile_rows;
+  d.tile_nc = c->tile_nc;
+  d.tile_cell = c->tile_cell;
+  d.tile_coff = c->tile_coff;
+  d.cand_cap = c->cand_cap;
+  d.one_pair = c->one_pair;
   d.nnb = c->nnb;
   d.atom_cell = c->atom_cell;
   d.atom_slot = c->atom_slot;
@@ -202,6 +215,8 @@ DevCtx devctx(ndg_ctx *c) {
   d.ring = c->ring;
   d.ring_count = c->ring_count;
   d.ring_cap = c->ring_cap;
+  d.stab_smem = c->stab_smem;
+  d.nb_smem = c->nb_smem;
   return d;
 }
 
@@ -247,6 +262,14 @@ int grow_atoms(ndg_ctx *c, long long new_chunks) {
   rc |= grow(c, c->ired, 0, (size_t)new_chunks);
   rc |= grow(c, c->red, 0, 8 * 32 * (size_t)new_chunks);
   rc |= grow(c, c->chunk_sys, (size_t)c->atoms.cap, (size_t)new_chunks);
+  {
+    const size_t t_old = 2 * (size_t)c->atoms.cap, t_new = 2 * (size_t)new_chunks;
+    rc |= grow(c, c->tile_nc, t_old, t_new);
+    rc |= grow(c, c->tile_rows, t_old, t_new);
+    if (!rc) cudaMemset(c->tile_rows + t_old, 0, (t_new - t_old) * sizeof(int));
+    rc |= grow(c, c->tile_cell, t_old * 256, t_new * 256);
+    rc |= grow(c, c->tile_coff, t_old * 257, t_new * 257);
+  }
   if (rc) return NDG_ERR_NOMEM;
   c->chunk_sys_h.resize(new_chunks, -1);
   cudaMemcpy(c->chunk_sys + c->atoms.cap, c->chunk_sys_h.data() + c->atoms.cap,
@@ -373,6 +396,35 @@ int upload_params(ndg_ctx *c) {
       }
     }
     prm[s] = p;
+  }
+  // stage the tables in shared memory when every system's fit (B200 allows
+  // 227 KB per block; keep room for two resident blocks per SM)
+  int stab = 0;
+  for (auto &h : c->sys)
+    if (h.alive) stab = std::max(stab, stab_bytes(h.ntypes, h.npairs, h.ptsize));
+  if (stab > 100 * 1024) stab = 0;
+  if (stab != c->stab_smem) {
+    c->stab_smem = stab;
+    drop_graphs(c);
+  }
+  // the single-pair pair-kernel variant applies only while every system has
+  // one type and one pair potential
+  int one = 1;
+  for (auto &h : c->sys)
+    if (h.alive && (h.ntypes != 1 || h.npairs != 1)) one = 0;
+  if (one != c->one_pair) {
+    c->one_pair = one;
+    drop_graphs(c);
+  }
+  // neighbour build: 4096 staged candidates (16 B each) plus the 16-bit
+  // lists of the tile's 128 atoms
+  int mx = 8;
+  for (auto &h : c->sys)
+    if (h.alive) mx = std::max(mx, h.maxnb);
+  const int nbs = 4096 * 16 + 128 * mx * 2;
+  if (nbs != c->nb_smem) {
+    c->nb_smem = nbs;
+    drop_graphs(c);
   }
   int rc = 0;
   rc |= upload_vec(c, c->pairmat, c->cap_pm, pm);
@@ -509,6 +561,9 @@ int setup_lists(ndg_ctx *c) {
     int maxnb = (int)(est * 1.2) + 16;
     if (h.ctl.neimax > 0) maxnb = std::max(maxnb, 2 * h.ctl.neimax);
     maxnb = std::min((maxnb + 7) / 8 * 8, std::max(h.n - 1, 8) * (h.ctl.quirk == 0 ? 2 : 1) + 8);
+    // the build keeps a tile's 128 lists in shared memory: 512 entries each
+    // at most (a denser neighbourhood reports NDG_ERR_NEIMAX)
+    maxnb = std::min(maxnb, 512);
     const long long npad = (long long)h.atoms.len * ATOM_ALIGN;
     if (maxnb > h.maxnb) {
       if (h.nbr.off >= 0) c->nbrs.give(h.nbr.off);
@@ -549,12 +604,12 @@ int setup_lists(ndg_ctx *c) {
   }
   int rc = upload_params(c);
   if (rc) return rc;
-  CK(c, cudaMemset(c->ring_count, 0, 2 * sizeof(int)));
+  CK(c, cudaMemset(c->ring_count, 0, 4 * sizeof(int)));
   DevCtx d = devctx(c);
   launch_rebuild(d, c->st, 1, c->precision == NDG_PREC_MIXED);
   CK(c, cudaGetLastError());
   CK(c, cudaStreamSynchronize(c->st));
-  int words[2];
+  int words[4];
   CK(c, cudaMemcpy(words, c->ring_count, sizeof(words), cudaMemcpyDeviceToHost));
   if (words[1]) {
     if (words[1] & E_NEIMAX) return NDG_ERR_NEIMAX;
@@ -619,6 +674,54 @@ int drain_ring(ndg_ctx *c, int count, ndg_thermo_cb cb, void *user) {
   return NDG_OK;
 }
 
+// Capture a block of g steps as one graph.  Each step's list-rebuild group
+// sits in a conditional IF node whose handle the previous step's pair
+// kernel sets when a system's CheckListUpdate fires (the first step's is
+// seeded by k_decide), so steps without a rebuild launch no rebuild kernel.
+int capture_block(ndg_ctx *c, int g, cudaGraphExec_t *out) {
+  DevCtx d = devctx(c);
+  const int mixed = c->precision == NDG_PREC_MIXED;
+  const int tpa = choose_tpa(c);
+  if (!c->st2) CK(c, cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking));
+  cudaGraph_t graph;
+  CK(c, cudaGraphCreate(&graph, 0));
+  std::vector<cudaGraphConditionalHandle> h(g);
+  for (int k = 0; k < g; ++k)
+    CK(c, cudaGraphConditionalHandleCreate(&h[k], graph, 0, cudaGraphCondAssignDefault));
+  CK(c, cudaStreamBeginCaptureToGraph(c->st, graph, nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal));
+  launch_decide(d, c->st, h[0]);
+  for (int k = 0; k < g; ++k) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t cg;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    CK(c, cudaStreamGetCaptureInfo(c->st, &cs, nullptr, &cg, &deps, &ndeps));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h[k];
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cn;
+    CK(c, cudaGraphAddNode(&cn, cg, deps, ndeps, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CK(c, cudaStreamUpdateCaptureDependencies(c->st, &cn, 1, cudaStreamSetCaptureDependencies));
+    CK(c, cudaStreamBeginCaptureToGraph(c->st2, body, nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeThreadLocal));
+    launch_rebuild(d, c->st2, 0, mixed);
+    cudaGraph_t body_out;
+    CK(c, cudaStreamEndCapture(c->st2, &body_out));
+    launch_integrate1(d, c->st, 0, mixed);
+    launch_pair(d, c->st, tpa, mixed, 1, 0, k + 1 < g ? (unsigned long long)h[k + 1] : 0ull);
+  }
+  cudaGraph_t done;
+  CK(c, cudaStreamEndCapture(c->st, &done));
+  cudaError_t e = cudaGraphInstantiate(out, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate");
+  return NDG_OK;
+}
+
 int run_steps(ndg_ctx *c, int nsteps, ndg_thermo_cb cb, void *user) {
   int left = nsteps;
   while (left > 0) {
@@ -628,12 +731,8 @@ int run_steps(ndg_ctx *c, int nsteps, ndg_thermo_cb cb, void *user) {
     if (it != c->graphs.end()) {
       exec = it->second;
     } else if (c->graph_steps > 1) {
-      cudaGraph_t graph;
-      CK(c, cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
-      enqueue_steps(c, g);
-      CK(c, cudaStreamEndCapture(c->st, &graph));
-      CK(c, cudaGraphInstantiate(&exec, graph, 0));
-      cudaGraphDestroy(graph);
+      int rc = capture_block(c, g, &exec);
+      if (rc) return rc;
       c->graphs[g] = exec;
     }
     if (exec) {
@@ -671,11 +770,12 @@ ndg_ctx::~ndg_ctx() {
   drop_graphs(this);
   void *ptrs[] = {dP, dS, chunk_sys, cell_sys, pos, s_pos, pfx, vel, acc, disp, force, s_vel,
                   s_acc, gid, s_gid, s_cell, nnb, atom_cell, atom_slot, perm, tmp_src, tmp_key,
-                  cell_count, cell_start, nbr, red, itop, ired, pairmat, mass, rc2, rlist2,
+                  cell_count, cell_start, nbr, tile_rows, tile_nc, tile_cell, tile_coff, red, itop, ired, pairmat, mass, rc2, rlist2,
                   vdr2, rc2f, tabF, tabP, tabF2, tabP2, ring, ring_count};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (st) cudaStreamDestroy(st);
+  if (st2) cudaStreamDestroy(st2);
 }
 
 // ===========================================================================
@@ -734,12 +834,12 @@ int ndg_create(ndg_ctx **out, int device, int precision) {
     delete c;
     return NDG_ERR_CUDA;
   }
-  c->ring_count = dalloc<int>(2);
+  c->ring_count = dalloc<int>(4);  // records, error bits, max tile candidates
   if (!c->ring_count) {
     delete c;
     return NDG_ERR_NOMEM;
   }
-  cudaMemset(c->ring_count, 0, 2 * sizeof(int));
+  cudaMemset(c->ring_count, 0, 4 * sizeof(int));
   int rc = grow_sys(c, 4);
   if (!rc) rc = grow_atoms(c, 16);
   if (!rc) rc = grow_cells(c, 1024);
@@ -994,7 +1094,7 @@ int ndg_build_cell_list(ndg_ctx *c) {
   for (auto &h : c->sys)
     if (h.alive && h.maxnb == 0) return setup_lists(c);
   DevCtx d = devctx(c);
-  CK(c, cudaMemset(c->ring_count, 0, 2 * sizeof(int)));
+  CK(c, cudaMemset(c->ring_count, 0, 4 * sizeof(int)));
   launch_rebuild(d, c->st, 1, c->precision == NDG_PREC_MIXED);
   CK(c, cudaGetLastError());
   int rc = status_from_words(c);
@@ -1013,7 +1113,7 @@ static bool lists_ready(ndg_ctx *c) {
 int ndg_check_list_update(ndg_ctx *c, int *rebuilt) {
   if (!c || !lists_ready(c)) return NDG_ERR_ARG;
   DevCtx d = devctx(c);
-  CK(c, cudaMemset(c->ring_count, 0, 2 * sizeof(int)));
+  CK(c, cudaMemset(c->ring_count, 0, 4 * sizeof(int)));
   launch_check(d, c->st, c->nsys_cap);
   launch_rebuild(d, c->st, 0, c->precision == NDG_PREC_MIXED);
   CK(c, cudaGetLastError());
@@ -1142,7 +1242,7 @@ static int run_impl(ndg_ctx *c, int nsteps, ndg_thermo_cb cb, void *user, int co
     if (h.alive) fill_control_params(h);
   rc = upload_params(c);
   if (rc) return rc;
-  CK(c, cudaMemset(c->ring_count, 0, 2 * sizeof(int)));
+  CK(c, cudaMemset(c->ring_count, 0, 4 * sizeof(int)));
   DevCtx d = devctx(c);
   launch_begin_run(d, c->st, c->nsys_cap, nsteps, cont);
   CK(c, cudaGetLastError());
@@ -1218,7 +1318,7 @@ int ndg_get_neighbors(ndg_ctx *c, int s, int *pairs, long long cap, long long *n
   for (int i = 0; i < n; ++i) {
     const int k1 = std::min(cnt[i], h.maxnb);
     for (int k = 0; k < k1; ++k) {
-      const int j = nb[(size_t)k * npad + i] - (int)off;
+      const int j = nb[(size_t)(i / 128) * h.maxnb * 128 + (size_t)k * 128 + (i % 128)] - (int)off;
       const int gi = g[i], gj = g[j];
       if (gi < gj) {
         if (pairs && m < cap) {
@@ -1287,6 +1387,57 @@ long long ndg_system_bytes(int np, int ntypes, int npairs, int ptsize, double de
 int ndg_autotune(ndg_ctx *c, int steps) {
   (void)steps;
   return c ? NDG_OK : NDG_ERR_ARG;
+}
+
+int ndg_get_stream(ndg_ctx *c, void **stream) {
+  if (!c || !stream) return NDG_ERR_ARG;
+  *stream = (void *)c->st;
+  return NDG_OK;
+}
+
+int ndg_profile_run(ndg_ctx *c, int nsteps) {
+  if (!c || nsteps < 1 || !lists_ready(c)) return NDG_ERR_ARG;
+  cudaSetDevice(c->device);
+  int rc = upload_params(c);
+  if (rc) return rc;
+  CK(c, cudaMemset(c->ring_count, 0, 4 * sizeof(int)));
+  DevCtx d = devctx(c);
+  const int mixed = c->precision == NDG_PREC_MIXED;
+  const int tpa = choose_tpa(c);
+  launch_begin_run(d, c->st, c->nsys_cap, nsteps, 1);
+  std::vector<cudaEvent_t> ev(4 * (size_t)nsteps);
+  for (auto &e : ev) CK(c, cudaEventCreate(&e));
+  for (int k = 0; k < nsteps; ++k) {
+    CK(c, cudaEventRecord(ev[4 * k], c->st));
+    launch_rebuild(d, c->st, 0, mixed);
+    CK(c, cudaEventRecord(ev[4 * k + 1], c->st));
+    launch_integrate1(d, c->st, 0, mixed);
+    CK(c, cudaEventRecord(ev[4 * k + 2], c->st));
+    launch_pair(d, c->st, tpa, mixed, 1, 0);
+    CK(c, cudaEventRecord(ev[4 * k + 3], c->st));
+  }
+  CK(c, cudaGetLastError());
+  CK(c, cudaStreamSynchronize(c->st));
+  double tr = 0, ti = 0, tp = 0;
+  for (int k = 0; k < nsteps; ++k) {
+    float a, b, e;
+    cudaEventElapsedTime(&a, ev[4 * k], ev[4 * k + 1]);
+    cudaEventElapsedTime(&b, ev[4 * k + 1], ev[4 * k + 2]);
+    cudaEventElapsedTime(&e, ev[4 * k + 2], ev[4 * k + 3]);
+    tr += a;
+    ti += b;
+    tp += e;
+  }
+  for (auto &e : ev) cudaEventDestroy(e);
+  c->t_reb = tr / nsteps;
+  c->t_int = ti / nsteps;
+  c->t_pair = tp / nsteps;
+  c->t_launches = 9 * nsteps;
+  int count = 0;
+  rc = check_words(c, &count);
+  if (!rc) rc = drain_ring(c, count, nullptr, nullptr);
+  int rf = flush_pending(c);
+  return rc ? rc : rf;
 }
 
 int ndg_get_kernel_times(ndg_ctx *c, double *ti, double *tp, double *tr, int *launches) {

@@ -145,7 +145,7 @@ __global__ __launch_bounds__(BLOCK) void k_integrate1(DevCtx c, int standalone, 
 // kernel to finish (dynamics, src/nd.f90:164-178 and the next step's head
 // :138-151).
 __device__ void finalize_system(const DevCtx &c, int sys, int blk0, int nblk, int flags,
-                                int fuse) {
+                                int fuse, unsigned long long next_h) {
   const SysParam *__restrict__ P = c.P + sys;
   SysState *S = c.S + sys;
   __shared__ double sm[8 * 32];
@@ -227,213 +227,11 @@ __device__ void finalize_system(const DevCtx &c, int sys, int blk0, int nblk, in
       S->ncell = nc;
     }
     S->rebuild = rb;
+    // inside a captured step block: switch on the next step's rebuild node
+    if (rb && next_h) cudaGraphSetConditional((cudaGraphConditionalHandle)next_h, 1u);
   } else {
     S->flags = 0;
     S->rebuild = 0;
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Pair loop: compute0 (src/nd.f90:273-333) over the full neighbour list,
-// TPA threads per atom, and with FUSE the integrate2 update
-// (src/nd.f90:1094-1116) of the atom as soon as its force is complete.
-template <int TPA, bool MIXED, bool FUSE>
-__global__ __launch_bounds__(BLOCK) void k_pair(DevCtx c, int host_flags) {
-  constexpr int APB = BLOCK / TPA;
-  const int a0 = blockIdx.x * APB;
-  const int sys = c.chunk_sys[a0 / ATOM_ALIGN];
-  if (sys < 0) return;
-  const SysParam *__restrict__ P = c.P + sys;
-  SysState *S = c.S + sys;
-  const int flags = FUSE ? S->flags : host_flags;
-  if (FUSE && !(flags & F_ACTIVE)) return;
-  if (!FUSE && P->n == 0) return;
-
-  const int g = threadIdx.x / TPA, la = threadIdx.x % TPA;
-  const int i = a0 + g;
-  const int local = i - P->atom_off;
-  const bool valid = local < P->n;
-  const bool cu = flags & F_CU, cv = flags & F_CV;
-
-  double pe = 0.0, vir[6] = {0, 0, 0, 0, 0, 0};
-  double fx = 0.0, fy = 0.0, fz = 0.0;
-  long long qx = 0, qy = 0, qz = 0;  // mixed: 64-bit fixed-point force
-  int ti = 1;
-  if (valid) {
-    const int ntypes = P->ntypes, ptsize1 = P->ptsize + 1;
-    const int *__restrict__ pm = c.pairmat + P->pm_off;
-    const int *__restrict__ nb = c.nbr + P->nbr_off + local;
-    const long long stride = P->npad;
-    int cnt = c.nnb[i];
-    cnt = cnt < P->maxnb ? cnt : P->maxnb;
-    if (!MIXED) {
-      const double4 pi = c.pos[i];
-      ti = tw_type(tw_of(pi.w));
-      const double b0 = S->box[0], b1 = S->box[1], b2 = S->box[2];
-      const double ptrmin = P->ptrmin;
-      const double *__restrict__ rc2 = c.rc2 + P->pair_off;
-      const float *__restrict__ vdr2 = c.vdr2 + P->pair_off;
-      const double *__restrict__ tF = c.tabF + P->tab_off;
-      const double *__restrict__ tP = c.tabP + P->tab_off;
-      for (int k = la; k < cnt; k += TPA) {
-        const int j = __ldg(nb + k * stride);
-        const double4 pj = c.pos[j];
-        const int tj = tw_type(tw_of(pj.w));
-        const int pt = __ldg(pm + (ti - 1) + (tj - 1) * ntypes);
-        if (pt <= 0) continue;
-        double s0 = pi.x - pj.x, s1 = pi.y - pj.y, s2 = pi.z - pj.z;
-        s0 = s0 - round(s0);
-        s1 = s1 - round(s1);
-        s2 = s2 - round(s2);
-        const double r0 = b0 * s0, r1 = b1 * s1, r2 = b2 * s2;
-        double d2 = r0 * r0;
-        d2 = d2 + r1 * r1;
-        d2 = d2 + r2 * r2;
-        if (d2 > __ldg(rc2 + pt - 1)) continue;
-        const float rk = (float)(d2 - ptrmin) * __ldg(vdr2 + pt - 1) + 1.0f;
-        int kk = (int)rk;
-        if (kk < 1) kk = 1;
-        const double w = (double)rk - (double)kk;
-        const int base = (pt - 1) * ptsize1 + kk - 1;
-        double df = w * __ldg(tF + base + 1) + (1.0 - w) * __ldg(tF + base);
-        df = df / d2;
-        fx = fx + r0 * df;
-        fy = fy + r1 * df;
-        fz = fz + r2 * df;
-        if (cu) pe = pe + (w * __ldg(tP + base + 1) + (1.0 - w) * __ldg(tP + base));
-        if (cv) {
-          vir[0] = vir[0] + r0 * r0 * df;
-          vir[1] = vir[1] + r1 * r1 * df;
-          vir[2] = vir[2] + r2 * r2 * df;
-          vir[3] = vir[3] + r0 * r1 * df;
-          vir[4] = vir[4] + r0 * r2 * df;
-          vir[5] = vir[5] + r1 * r2 * df;
-        }
-      }
-    } else {
-      const int4 pi = c.pfx[i];
-      ti = tw_type(pi.w);
-      const float sb0 = (float)(S->box[0] * (1.0 / FX_ONE));
-      const float sb1 = (float)(S->box[1] * (1.0 / FX_ONE));
-      const float sb2 = (float)(S->box[2] * (1.0 / FX_ONE));
-      const float ptrmin = (float)P->ptrmin;
-      const float *__restrict__ rc2 = c.rc2f + P->pair_off;
-      const float *__restrict__ vdr2 = c.vdr2 + P->pair_off;
-      const float2 *__restrict__ tF = c.tabF2 + P->tab_off;
-      const float2 *__restrict__ tP = c.tabP2 + P->tab_off;
-      float ax = 0.f, ay = 0.f, az = 0.f, ape = 0.f;
-      float av0 = 0.f, av1 = 0.f, av2 = 0.f, av3 = 0.f, av4 = 0.f, av5 = 0.f;
-      int nacc = 0;
-      for (int k = la; k < cnt; k += TPA) {
-        const int j = __ldg(nb + k * stride);
-        const int4 pj = c.pfx[j];
-        const int tj = tw_type(pj.w);
-        const int pt = __ldg(pm + (ti - 1) + (tj - 1) * ntypes);
-        if (pt <= 0) continue;
-        const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * sb0;
-        const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * sb1;
-        const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * sb2;
-        const float d2 = __fmaf_rn(r0, r0, __fmaf_rn(r1, r1, __fmul_rn(r2, r2)));
-        if (d2 > __ldg(rc2 + pt - 1)) continue;
-        const float rk = __fmaf_rn(d2 - ptrmin, __ldg(vdr2 + pt - 1), 1.0f);
-        int kk = (int)rk;
-        if (kk < 1) kk = 1;
-        const float w = rk - (float)kk;
-        const int base = (pt - 1) * (P->ptsize + 1) + kk - 1;
-        const float2 F = __ldg(tF + base);
-        const float df = __fdividef(__fmaf_rn(w, F.y - F.x, F.x), d2);
-        ax = __fmaf_rn(r0, df, ax);
-        ay = __fmaf_rn(r1, df, ay);
-        az = __fmaf_rn(r2, df, az);
-        if (cu) {
-          const float2 Pp = __ldg(tP + base);
-          ape += __fmaf_rn(w, Pp.y - Pp.x, Pp.x);
-        }
-        if (cv) {
-          const float r0d = r0 * df, r1d = r1 * df;
-          av0 = __fmaf_rn(r0d, r0, av0);
-          av1 = __fmaf_rn(r1d, r1, av1);
-          av2 = __fmaf_rn(r2 * df, r2, av2);
-          av3 = __fmaf_rn(r0d, r1, av3);
-          av4 = __fmaf_rn(r0d, r2, av4);
-          av5 = __fmaf_rn(r1d, r2, av5);
-        }
-        if (++nacc == 8) {
-          // flush the FP32 partial sums into the 64-bit fixed-point totals
-          qx += __float2ll_rn(ax * (float)FORCE_FX);
-          qy += __float2ll_rn(ay * (float)FORCE_FX);
-          qz += __float2ll_rn(az * (float)FORCE_FX);
-          ax = ay = az = 0.f;
-          nacc = 0;
-        }
-      }
-      qx += __float2ll_rn(ax * (float)FORCE_FX);
-      qy += __float2ll_rn(ay * (float)FORCE_FX);
-      qz += __float2ll_rn(az * (float)FORCE_FX);
-      pe = (double)ape;
-      vir[0] = av0; vir[1] = av1; vir[2] = av2; vir[3] = av3; vir[4] = av4; vir[5] = av5;
-    }
-  }
-  if (!MIXED) {
-    // combine the TPA partial forces of an atom (fixed tree: deterministic)
-#pragma unroll
-    for (int o = TPA / 2; o > 0; o >>= 1) {
-      fx += __shfl_xor_sync(0xffffffffu, fx, o);
-      fy += __shfl_xor_sync(0xffffffffu, fy, o);
-      fz += __shfl_xor_sync(0xffffffffu, fz, o);
-    }
-  } else {
-    // fixed-point sums are exact, so any combination order gives one result
-#pragma unroll
-    for (int o = TPA / 2; o > 0; o >>= 1) {
-      qx += __shfl_xor_sync(0xffffffffu, qx, o);
-      qy += __shfl_xor_sync(0xffffffffu, qy, o);
-      qz += __shfl_xor_sync(0xffffffffu, qz, o);
-    }
-    fx = (double)qx * (1.0 / FORCE_FX);
-    fy = (double)qy * (1.0 / FORCE_FX);
-    fz = (double)qz * (1.0 / FORCE_FX);
-  }
-  double ke = 0.0;
-  if (valid && la == 0) {
-    if (FUSE) {
-      const double rmass = 1.0 / c.mass[P->type_off + ti - 1];
-      const double dt = P->dt;
-      double *v = c.vel + 3 * (size_t)i;
-      double *a = c.acc + 3 * (size_t)i;
-      const double v0 = v[0] + 0.5 * dt * (fx * rmass + a[0]);
-      const double v1 = v[1] + 0.5 * dt * (fy * rmass + a[1]);
-      const double v2 = v[2] + 0.5 * dt * (fz * rmass + a[2]);
-      v[0] = v0; v[1] = v1; v[2] = v2;
-      a[0] = fx * rmass; a[1] = fy * rmass; a[2] = fz * rmass;
-      if (flags & F_CK) {
-        double kt = v0 * v0;
-        kt = kt + v1 * v1;
-        kt = kt + v2 * v2;
-        ke = kt * c.mass[P->type_off + ti - 1];
-      }
-    } else {
-      double *f = c.force + 3 * (size_t)i;
-      f[0] = fx; f[1] = fy; f[2] = fz;
-    }
-  }
-  __shared__ double sm[8 * 32];
-  double red[8] = {pe, vir[0], vir[1], vir[2], vir[3], vir[4], vir[5], ke};
-  block_sum<8>(red, sm);
-  __shared__ int last;
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int k = 0; k < 8; ++k) c.red[8 * (size_t)blockIdx.x + k] = red[k];
-    __threadfence();
-    const unsigned nblk = (unsigned)(P->npad / APB);
-    const unsigned t = atomicAdd(&S->ticket, 1u);
-    last = (t == nblk - 1);
-  }
-  __syncthreads();
-  if (last) {
-    __threadfence();
-    finalize_system(c, sys, P->atom_off / APB, P->npad / APB, flags, FUSE);
-    if (threadIdx.x == 0) S->ticket = 0;
   }
 }
 
@@ -701,6 +499,7 @@ __global__ __launch_bounds__(1024) void k_scan(DevCtx c, int nsys_cap, int force
   }
   if (threadIdx.x == 0) {
     start[ncell] = carry;
+    S->nstencil = make_stencil(S->mcell, P->quirk, S->stencil);
     for (int d = 0; d < 3; ++d) S->box_build[d] = S->box[d];
     if (!force_all) S->nlist_updates += 1;
   }
@@ -784,122 +583,637 @@ __global__ __launch_bounds__(BLOCK) void k_copyback(DevCtx c, int force_all, int
   c.atom_cell[i] = c.s_cell[i];
 }
 
-// Neighbour build: one CTA per link cell stages the atoms of its stencil
-// cells in shared memory; a warp takes one atom i of the cell, tests 32
-// candidates per pass and compacts the hits with __ballot_sync/__popc into
-// the padded SoA list.  Criteria of buildVerletList (src/nd.f90:1356-1383
-// for the cell itself, :1403-1426 for the neighbour cells).
-constexpr int NB_THREADS = 128;
-constexpr int NB_CAP = 768;    // candidates staged per pass
-constexpr int NB_IBATCH = 128; // own atoms per pass
+// Neighbour build, one CTA per 128-atom tile (atoms are sorted by link cell,
+// so a tile covers a short run of cells).
+//   1. The cells its atoms' stencils reach are collected in a shared-memory
+//      hash set, sorted, and recorded with their candidate offsets
+//      (tile_cell / tile_coff); the pair kernel stages exactly these atoms.
+//   2. The candidates are staged as 32-bit fixed-point positions; a warp
+//      takes one own atom and tests the candidates of each stencil entry, 32
+//      per pass.  An FP32 distance decides every pair farther than a 1e-5
+//      relative margin from the cutoff (and from PTrMin); pairs inside the
+//      margin take the reference's exact FP64 test, so membership is
+//      bit-identical to buildVerletList (src/nd.f90:1356-1383 for the cell
+//      itself, :1403-1426 for the neighbour cells).
+//   3. Hits are compacted with __ballot_sync/__popc into 16-bit tile-local
+//      candidate indices and written to the blocked list row by row.
+constexpr int TILE = 128;      // atoms per tile
+constexpr int TC_MAX = 256;    // link cells a tile may stage
+constexpr int HSLOTS = 1024;   // shared hash slots for the tile's cell set
+constexpr float NB_MARGIN = 1e-5f;
+constexpr int BUILD_CAP = 4096;  // candidates the build stages per tile
+constexpr int NBT = 512;         // threads of the build CTA (16 warps)
 
-__global__ __launch_bounds__(NB_THREADS) void k_build(DevCtx c, int force_all) {
-  const int gc = blockIdx.x;
-  const int sys = c.cell_sys[gc];
+__device__ __forceinline__ int stencil_cell(int cl, int st, int M0, int M1, int M2) {
+  const int cx = cl % M0, cy = (cl / M0) % M1, cz = cl / (M0 * M1);
+  const int dx = (st & 15) - 1, dy = ((st >> 4) & 15) - 1, dz = ((st >> 8) & 15) - 1;
+  const int nx = (cx + dx + M0) % M0, ny = (cy + dy + M1) % M1, nz = (cz + dz + M2) % M2;
+  return nx + ny * M0 + nz * M0 * M1;
+}
+
+__device__ __forceinline__ int find_cell(const int *ucell, int nu, int cell) {
+  int lo = 0, hi = nu - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (ucell[mid] < cell) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ __launch_bounds__(NBT) void k_build(DevCtx c, int force_all) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  const int tile = blockIdx.x;
+  const int a0 = tile * TILE;
+  const int sys = c.chunk_sys[a0 / ATOM_ALIGN];
   if (sys < 0 || !rebuilding(c, sys, force_all)) return;
   const SysParam *__restrict__ P = c.P + sys;
   SysState *S = c.S + sys;
-  const int cl = gc - P->cell_off;
-  const int M0 = S->mcell[0], M1 = S->mcell[1], M2 = S->mcell[2];
-  if (cl >= S->ncell) return;
-
-  __shared__ double4 cpos[NB_CAP];
-  __shared__ int cj[NB_CAP];
-  __shared__ int ent_start[MAX_STENCIL + 1], ent_cell[MAX_STENCIL], ent_center[MAX_STENCIL];
-  __shared__ int ncnt[NB_IBATCH];
-  __shared__ int nent;
-
-  const int *cst = c.cell_start + P->cell_off;
-  if (threadIdx.x == 0) {
-    int st[MAX_STENCIL];
-    const int m[3] = {M0, M1, M2};
-    const int ne = make_stencil(m, P->quirk, st);
-    const int cx = cl % M0, cy = (cl / M0) % M1, cz = cl / (M0 * M1);
-    int tot = 0;
-    for (int e = 0; e < ne; ++e) {
-      const int dx = (st[e] & 15) - 1, dy = ((st[e] >> 4) & 15) - 1, dz = ((st[e] >> 8) & 15) - 1;
-      const int nx = (cx + dx + M0) % M0, ny = (cy + dy + M1) % M1, nz = (cz + dz + M2) % M2;
-      const int nc = nx + ny * M0 + nz * M0 * M1;
-      ent_cell[e] = nc;
-      ent_center[e] = (st[e] >> 12) & 1;
-      ent_start[e] = tot;
-      tot += cst[nc + 1] - cst[nc];
+  const int local0 = a0 - P->atom_off;
+  const int nown = min(TILE, P->n - local0);
+  if (nown <= 0) {
+    if (threadIdx.x == 0) {
+      c.tile_nc[tile] = 0;
+      c.tile_rows[tile] = 0;
     }
-    ent_start[ne] = tot;
-    nent = ne;
+    return;
+  }
+  const int M0 = S->mcell[0], M1 = S->mcell[1], M2 = S->mcell[2];
+  const int ne = S->nstencil;
+  const int maxnb = P->maxnb;
+  int4 *cpf = (int4 *)dsm;                                   // BUILD_CAP candidates
+  unsigned short *lst = (unsigned short *)(cpf + BUILD_CAP);  // TILE * maxnb
+  __shared__ int hset[HSLOTS];
+  __shared__ int ucell[TC_MAX + 1], coff[TC_MAX + 1], ustart[TC_MAX];
+  __shared__ int stc[MAX_STENCIL];
+  __shared__ int ncnt[TILE];
+  __shared__ short run_of[TILE];               // own atom -> run of equal cells
+  __shared__ int run_cell[TILE];
+  __shared__ short ent_u[TILE * MAX_STENCIL];  // run x stencil entry -> staged cell
+  __shared__ int nu, bad, nruns, rows_s;
+  __shared__ int pm_s[16 * 16];
+  __shared__ float rl2f_s[136];
+  __shared__ double rl2_s[136];
+  const int nt = P->ntypes, npr = P->npairs;
+  const bool small = nt <= 16 && npr <= 136;
+  const int *cst = c.cell_start + P->cell_off;
+  for (int k = threadIdx.x; k < HSLOTS; k += NBT) hset[k] = -1;
+  if (threadIdx.x < ne) stc[threadIdx.x] = S->stencil[threadIdx.x];
+  if (threadIdx.x == 0) {
+    nu = 0;
+    bad = 0;
+  }
+  if (small) {
+    for (int k = threadIdx.x; k < nt * nt; k += NBT) pm_s[k] = c.pairmat[P->pm_off + k];
+    for (int k = threadIdx.x; k < npr; k += NBT) {
+      rl2_s[k] = c.rlist2[P->pair_off + k];
+      rl2f_s[k] = (float)rl2_s[k];
+    }
   }
   __syncthreads();
-  const int ne = nent;
-  const int ncand = ent_start[ne];
-  const int own0 = cst[cl], own1 = cst[cl + 1];
-  const double b0 = S->box[0], b1 = S->box[1], b2 = S->box[2];
-  const double ptrmin = P->ptrmin;
-  const int ntypes = P->ntypes;
-  const int *__restrict__ pm = c.pairmat + P->pm_off;
-  const double *__restrict__ rl2 = c.rlist2 + P->pair_off;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const long long stride = P->npad;
-  const int maxnb = P->maxnb;
-
-  for (int ib = own0; ib < own1; ib += NB_IBATCH) {
-    const int ie = min(ib + NB_IBATCH, own1);
-    for (int t = threadIdx.x; t < NB_IBATCH; t += NB_THREADS) ncnt[t] = 0;
-    for (int q0 = 0; q0 < ncand; q0 += NB_CAP) {
-      const int q1 = min(q0 + NB_CAP, ncand);
-      __syncthreads();
-      for (int q = q0 + threadIdx.x; q < q1; q += NB_THREADS) {
-        int e = 0;
-        while (ent_start[e + 1] <= q) ++e;
-        const int j = P->atom_off + cst[ent_cell[e]] + (q - ent_start[e]);
-        cpos[q - q0] = c.pos[j];
-        cj[q - q0] = j | (ent_center[e] << 31);
+  // 1. the set of cells the tile's stencils reach
+  {
+    const int t = threadIdx.x;
+    if (t < nown) {
+      const int cl = c.atom_cell[a0 + t];
+      if (t == 0 || cl != c.atom_cell[a0 + t - 1]) {
+        for (int e = 0; e < ne; ++e) {
+          const int nc = stencil_cell(cl, stc[e], M0, M1, M2);
+          int h = (nc * 2654435761u) & (HSLOTS - 1);
+          for (int probe = 0; probe < HSLOTS; ++probe) {
+            const int prev = atomicCAS(&hset[h], -1, nc);
+            if (prev == -1) {
+              atomicAdd(&nu, 1);
+              break;
+            }
+            if (prev == nc) break;
+            h = (h + 1) & (HSLOTS - 1);
+          }
+        }
       }
-      __syncthreads();
-      for (int il = ib + warp; il < ie; il += NB_THREADS / 32) {
-        const int i = P->atom_off + il;
-        const double4 pi = c.pos[i];
-        const int ti = tw_type(tw_of(pi.w));
-        int cnt = ncnt[il - ib];
-        for (int qb = 0; qb < q1 - q0; qb += 32) {
-          const int q = qb + lane;
-          bool hit = false;
-          int j = 0;
-          if (q < q1 - q0) {
-            const int raw = cj[q];
-            j = raw & 0x7fffffff;
-            const bool center = raw < 0;
-            const double4 pj = cpos[q];
-            const int tj = tw_type(tw_of(pj.w));
-            const int a = __ldg(pm + (ti - 1) + (tj - 1) * ntypes);
-            const int b = __ldg(pm + (tj - 1) + (ti - 1) * ntypes);
-            const int mx = a > b ? a : b;
-            if (j != i && mx > 0) {
-              double s0 = pi.x - pj.x, s1 = pi.y - pj.y, s2 = pi.z - pj.z;
+    }
+  }
+  __syncthreads();
+  if (nu > TC_MAX) bad = 1;
+  __syncthreads();
+  if (!bad) {
+    // compact and sort the cell ids (bitonic over TC_MAX slots)
+    __shared__ int cursor;
+    if (threadIdx.x == 0) cursor = 0;
+    for (int k = threadIdx.x; k < TC_MAX; k += NBT) ucell[k] = 0x7fffffff;
+    __syncthreads();
+    for (int k = threadIdx.x; k < HSLOTS; k += NBT)
+      if (hset[k] >= 0) ucell[atomicAdd(&cursor, 1)] = hset[k];
+    __syncthreads();
+    for (int size = 2; size <= TC_MAX; size <<= 1)
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        for (int k = threadIdx.x; k < TC_MAX; k += NBT) {
+          const int p = k ^ stride;
+          if (p > k) {
+            const bool up = (k & size) == 0;
+            const int a = ucell[k], b = ucell[p];
+            if ((a > b) == up) {
+              ucell[k] = b;
+              ucell[p] = a;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    if (threadIdx.x == 0) {
+      int tot = 0;
+      for (int u = 0; u < nu; ++u) {
+        coff[u] = tot;
+        ustart[u] = cst[ucell[u]];
+        tot += cst[ucell[u] + 1] - cst[ucell[u]];
+      }
+      coff[nu] = tot;
+      if (tot > BUILD_CAP) bad = 1;
+    }
+  }
+  __syncthreads();
+  if (bad) {
+    if (threadIdx.x == 0) {
+      c.tile_nc[tile] = 0;
+      c.tile_rows[tile] = 0;
+      set_err(c, S, E_NEIMAX);
+    }
+    if (threadIdx.x < nown) c.nnb[a0 + threadIdx.x] = 0;
+    return;
+  }
+  const int U = nu, C = coff[nu];
+  if (threadIdx.x == 0) {
+    atomicMax(c.ring_count + 2, C);
+    c.tile_nc[tile] = U;
+  }
+  for (int u = threadIdx.x; u <= U; u += NBT) {
+    if (u < U) c.tile_cell[(size_t)tile * TC_MAX + u] = ucell[u];
+    c.tile_coff[(size_t)tile * (TC_MAX + 1) + u] = coff[u];
+  }
+  // 2. stage the candidates
+  for (int u = threadIdx.x >> 5; u < U; u += NBT / 32) {
+    const int q0 = coff[u], len = coff[u + 1] - q0;
+    const int j0 = P->atom_off + ustart[u];
+    for (int e = threadIdx.x & 31; e < len; e += 32) {
+      const double4 p = c.pos[j0 + e];
+      cpf[q0 + e] = make_int4(fx32(p.x), fx32(p.y), fx32(p.z), tw_of(p.w));
+    }
+  }
+  __syncthreads();
+  const int *pm = small ? pm_s : c.pairmat + P->pm_off;
+  const double b0 = S->box[0], b1 = S->box[1], b2 = S->box[2];
+  const float sb0 = (float)(b0 * (1.0 / FX_ONE)), sb1 = (float)(b1 * (1.0 / FX_ONE)),
+              sb2 = (float)(b2 * (1.0 / FX_ONE));
+  const double ptrmin = P->ptrmin;
+  const float ptrlo = (float)ptrmin * (1.f - NB_MARGIN), ptrhi = (float)ptrmin * (1.f + NB_MARGIN);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // the stencil cells of each run of equal own cells, resolved once per run
+  if (threadIdx.x == 0) {
+    int r = -1, prev = -1;
+    for (int t = 0; t < nown; ++t) {
+      const int cl = c.atom_cell[a0 + t];
+      if (cl != prev) {
+        run_cell[++r] = cl;
+        prev = cl;
+      }
+      run_of[t] = (short)r;
+    }
+    nruns = r + 1;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < nruns * ne; idx += NBT) {
+    const int r = idx / ne, e = idx - r * ne;
+    ent_u[r * MAX_STENCIL + e] =
+        (short)find_cell(ucell, U, stencil_cell(run_cell[r], stc[e], M0, M1, M2));
+  }
+  __syncthreads();
+  // 3. one warp per own atom
+  for (int t = warp; t < nown; t += NBT / 32) {
+    const int i = a0 + t;
+    const double4 pid = c.pos[i];
+    const int4 pi = make_int4(fx32(pid.x), fx32(pid.y), fx32(pid.z), tw_of(pid.w));
+    const int ti = tw_type(pi.w);
+    const short *eu = ent_u + run_of[t] * MAX_STENCIL;
+    unsigned short *mylst = lst + t * maxnb;
+    int cnt = 0;
+    for (int e = 0; e < ne; ++e) {
+      const bool center = (stc[e] >> 12) & 1;
+      const int u = eu[e];
+      const int q0 = coff[u], q1 = coff[u + 1];
+      for (int qb = q0; qb < q1; qb += 32) {
+        const int q = qb + lane;
+        bool hit = false;
+        if (q < q1) {
+          const int j = P->atom_off + ustart[u] + (q - q0);
+          const int4 pj = cpf[q];
+          const int tj = tw_type(pj.w);
+          const int a = pm[(ti - 1) + (tj - 1) * nt];
+          const int b = pm[(tj - 1) + (ti - 1) * nt];
+          const int mx = a > b ? a : b;
+          if (j != i && mx > 0) {
+            const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * sb0;
+            const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * sb1;
+            const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * sb2;
+            const float d2f = r0 * r0 + r1 * r1 + r2 * r2;
+            const float rlf = small ? rl2f_s[mx - 1] : (float)c.rlist2[P->pair_off + mx - 1];
+            const bool near_cut = fabsf(d2f - rlf) <= NB_MARGIN * rlf;
+            const bool near_min = center && d2f >= ptrlo && d2f <= ptrhi;
+            if (near_cut || near_min) {
+              // the reference's FP64 test (src/nd.f90:1362-1377)
+              const double4 pjd = c.pos[j];
+              double s0 = pid.x - pjd.x, s1 = pid.y - pjd.y, s2 = pid.z - pjd.z;
               s0 = s0 - round(s0);
               s1 = s1 - round(s1);
               s2 = s2 - round(s2);
-              const double r0 = b0 * s0, r1 = b1 * s1, r2 = b2 * s2;
-              double d2 = r0 * r0;
-              d2 = d2 + r1 * r1;
-              d2 = d2 + r2 * r2;
-              hit = !(center && d2 < ptrmin) && !(d2 > __ldg(rl2 + mx - 1));
+              const double x0 = b0 * s0, x1 = b1 * s1, x2 = b2 * s2;
+              double d2 = x0 * x0;
+              d2 = d2 + x1 * x1;
+              d2 = d2 + x2 * x2;
+              const double rl = small ? rl2_s[mx - 1] : c.rlist2[P->pair_off + mx - 1];
+              hit = !(center && d2 < ptrmin) && !(d2 > rl);
+            } else {
+              hit = !(center && d2f < ptrlo) && d2f < rlf;
             }
           }
-          const unsigned bal = __ballot_sync(0xffffffffu, hit);
-          if (hit) {
-            const int k = cnt + __popc(bal & ((1u << lane) - 1u));
-            if (k < maxnb) c.nbr[P->nbr_off + (long long)k * stride + il] = j;
-          }
-          cnt += __popc(bal);
         }
-        if (lane == 0) ncnt[il - ib] = cnt;
+        const unsigned bal = __ballot_sync(0xffffffffu, hit);
+        if (hit) {
+          const int k = cnt + __popc(bal & ((1u << lane) - 1u));
+          if (k < maxnb) mylst[k] = (unsigned short)q;
+        }
+        cnt += __popc(bal);
       }
     }
+    if (lane == 0) ncnt[t] = cnt;
+  }
+  __syncthreads();
+  // 4. write the tile's lists row by row (consecutive threads, consecutive atoms)
+  if (threadIdx.x == 0) {
+    int r = 0;
+    for (int t = 0; t < nown; ++t) r = max(r, min(ncnt[t], maxnb));
+    rows_s = r;
+  }
+  __syncthreads();
+  const int rows = rows_s;
+  int *dst = c.nbr + P->nbr_off + (long long)(local0 / TILE) * maxnb * TILE;
+  for (int idx = threadIdx.x; idx < rows * TILE; idx += NBT) {
+    const int k = idx / TILE, t = idx - k * TILE;
+    if (t < nown && k < min(ncnt[t], maxnb)) {
+      // staged candidate -> its atom slot
+      const int q = lst[t * maxnb + k];
+      const int u = find_cell(coff + 1, U, q + 1);
+      dst[k * TILE + t] = P->atom_off + ustart[u] + (q - coff[u]);
+    }
+  }
+  if (threadIdx.x == 0) c.tile_rows[tile] = rows;
+  if (threadIdx.x < nown) {
+    c.nnb[a0 + threadIdx.x] = ncnt[threadIdx.x];
+    if (ncnt[threadIdx.x] > maxnb) set_err(c, S, E_NEIMAX);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Pair loop: compute0 (src/nd.f90:273-333) over the full neighbour list,
+// TPA threads per atom, and with FUSE the integrate2 update
+// (src/nd.f90:1094-1116) of each atom as soon as its force is complete.
+//
+// One CTA (TILE*TPA threads) works on one 128-atom tile at a time; CTAs are
+// persistent and own contiguous tile ranges.  Per tile it stages the
+// positions of the tile's candidate atoms (the cells recorded by k_build)
+// in shared memory, so every neighbour gather of the pair loop is a
+// shared-memory load addressed by the 16-bit tile-local index of the list;
+// the pair matrix, cutoffs and interpolation tables of the system are
+// staged once per system change.
+constexpr int UNR = 4;    // mixed: pairs in flight per thread
+constexpr int UNR_D = 2;  // FP64
+
+struct TabView {
+  const int *pm;
+  const double *rc2;
+  const float *rc2f, *vdr2;
+  const double *tF, *tP;    // FP64 tables
+  const float2 *tF2, *tP2;  // FP32 (k, k+1) pairs
+};
+
+template <bool MIXED>
+__device__ void stage_tables(const DevCtx &c, const SysParam *P, unsigned char *sm, TabView &tv) {
+  const int nt = P->ntypes, np = P->npairs, T = P->ptsize + 1;
+  int *pm = (int *)sm;
+  int off = (nt * nt * 4 + 15) / 16 * 16;
+  double *rc2 = (double *)(sm + off);
+  float *rc2f = (float *)(sm + off + np * 8);
+  float *vdr2 = (float *)(sm + off + np * 12);
+  off = (off + np * 16 + 15) / 16 * 16;
+  for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) pm[k] = c.pairmat[P->pm_off + k];
+  for (int k = threadIdx.x; k < np; k += blockDim.x) {
+    rc2[k] = c.rc2[P->pair_off + k];
+    rc2f[k] = c.rc2f[P->pair_off + k];
+    vdr2[k] = c.vdr2[P->pair_off + k];
+  }
+  tv.pm = pm;
+  tv.rc2 = rc2;
+  tv.rc2f = rc2f;
+  tv.vdr2 = vdr2;
+  if (MIXED) {
+    float2 *dF = (float2 *)(sm + off), *dP = dF + np * T;
+    const float2 *sF = c.tabF2 + P->tab_off, *sP = c.tabP2 + P->tab_off;
+    for (int k = threadIdx.x; k < np * T; k += blockDim.x) {
+      dF[k] = sF[k];
+      dP[k] = sP[k];
+    }
+    tv.tF2 = dF;
+    tv.tP2 = dP;
+  } else {
+    double *dF = (double *)(sm + off), *dP = dF + np * T;
+    const double *sF = c.tabF + P->tab_off, *sP = c.tabP + P->tab_off;
+    for (int k = threadIdx.x; k < np * T; k += blockDim.x) {
+      dF[k] = sF[k];
+      dP[k] = sP[k];
+    }
+    tv.tF = dF;
+    tv.tP = dP;
+  }
+}
+
+__device__ __forceinline__ void global_tables(const DevCtx &c, const SysParam *P, TabView &tv) {
+  tv.pm = c.pairmat + P->pm_off;
+  tv.rc2 = c.rc2 + P->pair_off;
+  tv.rc2f = c.rc2f + P->pair_off;
+  tv.vdr2 = c.vdr2 + P->pair_off;
+  tv.tF = c.tabF + P->tab_off;
+  tv.tP = c.tabP + P->tab_off;
+  tv.tF2 = c.tabF2 + P->tab_off;
+  tv.tP2 = c.tabP2 + P->tab_off;
+}
+
+// MODE 0: tables read from global memory; 1: staged in shared memory;
+// 2: staged, and every system has one type and one pair (no per-pair
+// type lookup, cutoff and table scale held in registers)
+template <int TPA, bool MIXED, bool FUSE, int MODE>
+__global__ __launch_bounds__(TILE * TPA) void k_pair(DevCtx c, int host_flags, int ntiles,
+                                                     unsigned long long next_h) {
+  constexpr bool STAB = MODE >= 1;
+  constexpr bool ONE = MODE == 2;
+  extern __shared__ __align__(16) unsigned char dsm[];
+  const int G = gridDim.x;
+  const int t0 = (int)((long long)blockIdx.x * ntiles / G);
+  const int t1 = (int)((long long)(blockIdx.x + 1) * ntiles / G);
+  int loaded = -1;
+  TabView tv;
+  __shared__ int last;
+  __shared__ double sm[8 * 32];
+
+  for (int tile = t0; tile < t1; ++tile) {
+    const int a0 = tile * TILE;
+    const int sys = c.chunk_sys[a0 / ATOM_ALIGN];
+    if (sys < 0) continue;
+    const SysParam *__restrict__ P = c.P + sys;
+    SysState *S = c.S + sys;
+    const int flags = FUSE ? S->flags : host_flags;
+    if (FUSE && !(flags & F_ACTIVE)) continue;
+    if (!FUSE && P->n == 0) continue;
+    if (sys != loaded) {
+      if (STAB) {
+        __syncthreads();  // no thread still reads the previous system's tables
+        stage_tables<MIXED>(c, P, dsm, tv);
+        __syncthreads();  // tables complete before the first pair
+      } else {
+        global_tables(c, P, tv);
+      }
+      loaded = sys;
+    }
+    // prefetch the next tile's neighbour list (one contiguous region of
+    // rows x TILE ints) into L2 while this tile computes
+    if (threadIdx.x == 0 && tile + 1 < t1) {
+      const int nt_ = tile + 1;
+      const int ns = c.chunk_sys[nt_ * TILE / ATOM_ALIGN];
+      if (ns >= 0) {
+        const SysParam *Pn = c.P + ns;
+        const int rows = min(c.tile_rows[nt_], Pn->maxnb);
+        const int *src = c.nbr + Pn->nbr_off + (long long)((nt_ * TILE - Pn->atom_off) / TILE) *
+                                                   Pn->maxnb * TILE;
+        if (rows > 0) {
+          asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(
+                           __cvta_generic_to_global(src)),
+                       "r"(rows * TILE * 4)
+                       : "memory");
+        }
+      }
+    }
+    const int g = threadIdx.x / TPA, la = threadIdx.x % TPA;
+    const int i = a0 + g;
+    const int local = i - P->atom_off;
+    const bool valid = local < P->n;
+    const bool cu = flags & F_CU, cv = flags & F_CV;
+    const int ntypes = P->ntypes, T = P->ptsize + 1, ptsize = P->ptsize;
+
+    double pe = 0.0, vir[6] = {0, 0, 0, 0, 0, 0};
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    long long qx = 0, qy = 0, qz = 0;  // mixed: 64-bit fixed-point force
+    int ti = 1;
+    if (valid) {
+      // blocked list: row k of this tile is TILE contiguous ints
+      const int *__restrict__ nb =
+          c.nbr + P->nbr_off + (long long)(local / TILE) * P->maxnb * TILE + g;
+      int cnt = c.nnb[i];
+      cnt = cnt < P->maxnb ? cnt : P->maxnb;
+      if (!MIXED) {
+        const double4 pi = c.pos[i];
+        ti = tw_type(tw_of(pi.w));
+        const int *pmr = tv.pm + (ti - 1);
+        const double b0 = S->box[0], b1 = S->box[1], b2 = S->box[2];
+        const double ptrmin = P->ptrmin;
+        for (int k0 = la; k0 < cnt; k0 += UNR_D * TPA) {
+          int qq[UNR_D];
+          double4 pj[UNR_D];
+#pragma unroll
+          for (int q = 0; q < UNR_D; ++q) {
+            const int k = k0 + q * TPA;
+            qq[q] = k < cnt ? __ldg(nb + k * TILE) : -1;
+          }
+#pragma unroll
+          for (int q = 0; q < UNR_D; ++q) pj[q] = c.pos[qq[q] >= 0 ? qq[q] : i];
+#pragma unroll
+          for (int q = 0; q < UNR_D; ++q) {
+            const int pt = ONE ? 1 : pmr[(tw_type(tw_of(pj[q].w)) - 1) * ntypes];
+            const int p1 = ONE ? 0 : (pt > 0 ? pt - 1 : 0);
+            double s0 = pi.x - pj[q].x, s1 = pi.y - pj[q].y, s2 = pi.z - pj[q].z;
+            s0 = s0 - round(s0);
+            s1 = s1 - round(s1);
+            s2 = s2 - round(s2);
+            const double r0 = b0 * s0, r1 = b1 * s1, r2 = b2 * s2;
+            double d2 = r0 * r0;
+            d2 = d2 + r1 * r1;
+            d2 = d2 + r2 * r2;
+            const bool ok = qq[q] >= 0 && pt > 0 && !(d2 > tv.rc2[p1]);
+            const float rk = (float)(d2 - ptrmin) * tv.vdr2[p1] + 1.0f;
+            int kk = (int)rk;
+            kk = kk < 1 ? 1 : (kk > ptsize ? ptsize : kk);
+            const double w = (double)rk - (double)kk;
+            const int base = p1 * T + kk - 1;
+            const double fk1 = tv.tF[base + 1], fk = tv.tF[base];
+            double df = w * fk1 + (1.0 - w) * fk;
+            df = ok ? df / d2 : 0.0;
+            fx = fx + r0 * df;
+            fy = fy + r1 * df;
+            fz = fz + r2 * df;
+            if (cu && ok) pe = pe + (w * tv.tP[base + 1] + (1.0 - w) * tv.tP[base]);
+            if (cv) {
+              vir[0] = vir[0] + r0 * r0 * df;
+              vir[1] = vir[1] + r1 * r1 * df;
+              vir[2] = vir[2] + r2 * r2 * df;
+              vir[3] = vir[3] + r0 * r1 * df;
+              vir[4] = vir[4] + r0 * r2 * df;
+              vir[5] = vir[5] + r1 * r2 * df;
+            }
+          }
+        }
+      } else {
+        const int4 pi = c.pfx[i];
+        ti = tw_type(pi.w);
+        const int *pmr = tv.pm + (ti - 1);
+        const float sb0 = (float)(S->box[0] * (1.0 / FX_ONE));
+        const float sb1 = (float)(S->box[1] * (1.0 / FX_ONE));
+        const float sb2 = (float)(S->box[2] * (1.0 / FX_ONE));
+        const float ptrmin = (float)P->ptrmin;
+        const float rc2f1 = tv.rc2f[0], vdr21 = tv.vdr2[0];
+        float ax = 0.f, ay = 0.f, az = 0.f, ape = 0.f;
+        float av0 = 0.f, av1 = 0.f, av2 = 0.f, av3 = 0.f, av4 = 0.f, av5 = 0.f;
+        int grp = 0;
+        int qn[UNR];  // list entries of the next group, loaded one group ahead
+#pragma unroll
+        for (int q = 0; q < UNR; ++q) {
+          const int k = la + q * TPA;
+          qn[q] = k < cnt ? __ldg(nb + k * TILE) : -1;
+        }
+        for (int k0 = la; k0 < cnt; k0 += UNR * TPA) {
+          int qq[UNR];
+          int4 pj[UNR];
+#pragma unroll
+          for (int q = 0; q < UNR; ++q) qq[q] = qn[q];
+#pragma unroll
+          for (int q = 0; q < UNR; ++q) {
+            const int k = k0 + (UNR + q) * TPA;
+            qn[q] = k < cnt ? __ldg(nb + k * TILE) : -1;
+          }
+#pragma unroll
+          for (int q = 0; q < UNR; ++q) pj[q] = c.pfx[qq[q] >= 0 ? qq[q] : i];
+#pragma unroll
+          for (int q = 0; q < UNR; ++q) {
+            const int pt = ONE ? 1 : pmr[(tw_type(pj[q].w) - 1) * ntypes];
+            const int p1 = ONE ? 0 : (pt > 0 ? pt - 1 : 0);
+            const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj[q].x) * sb0;
+            const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj[q].y) * sb1;
+            const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj[q].z) * sb2;
+            const float d2 = __fmaf_rn(r0, r0, __fmaf_rn(r1, r1, __fmul_rn(r2, r2)));
+            const bool ok = qq[q] >= 0 && pt > 0 && !(d2 > (ONE ? rc2f1 : tv.rc2f[p1]));
+            const float rk = __fmaf_rn(d2 - ptrmin, ONE ? vdr21 : tv.vdr2[p1], 1.0f);
+            int kk = (int)rk;
+            kk = kk < 1 ? 1 : (kk > ptsize ? ptsize : kk);
+            const float w = rk - (float)kk;
+            const int base = p1 * T + kk - 1;
+            const float2 F = tv.tF2[base];
+            const float df = ok ? __fdividef(__fmaf_rn(w, F.y - F.x, F.x), d2) : 0.f;
+            ax = __fmaf_rn(r0, df, ax);
+            ay = __fmaf_rn(r1, df, ay);
+            az = __fmaf_rn(r2, df, az);
+            if (cu && ok) {
+              const float2 Pp = tv.tP2[base];
+              ape += __fmaf_rn(w, Pp.y - Pp.x, Pp.x);
+            }
+            if (cv) {
+              const float r0d = r0 * df, r1d = r1 * df;
+              av0 = __fmaf_rn(r0d, r0, av0);
+              av1 = __fmaf_rn(r1d, r1, av1);
+              av2 = __fmaf_rn(r2 * df, r2, av2);
+              av3 = __fmaf_rn(r0d, r1, av3);
+              av4 = __fmaf_rn(r0d, r2, av4);
+              av5 = __fmaf_rn(r1d, r2, av5);
+            }
+          }
+          if (++grp == 2) {
+            // flush the FP32 partial sums (8 pairs) into the 64-bit fixed-point totals
+            qx += __float2ll_rn(ax * (float)FORCE_FX);
+            qy += __float2ll_rn(ay * (float)FORCE_FX);
+            qz += __float2ll_rn(az * (float)FORCE_FX);
+            ax = ay = az = 0.f;
+            grp = 0;
+          }
+        }
+        qx += __float2ll_rn(ax * (float)FORCE_FX);
+        qy += __float2ll_rn(ay * (float)FORCE_FX);
+        qz += __float2ll_rn(az * (float)FORCE_FX);
+        pe = (double)ape;
+        vir[0] = av0; vir[1] = av1; vir[2] = av2; vir[3] = av3; vir[4] = av4; vir[5] = av5;
+      }
+    }
+    if (!MIXED) {
+      // combine the TPA partial forces of an atom (fixed tree: deterministic)
+#pragma unroll
+      for (int o = TPA / 2; o > 0; o >>= 1) {
+        fx += __shfl_xor_sync(0xffffffffu, fx, o);
+        fy += __shfl_xor_sync(0xffffffffu, fy, o);
+        fz += __shfl_xor_sync(0xffffffffu, fz, o);
+      }
+    } else {
+      // fixed-point sums are exact, so any combination order gives one result
+#pragma unroll
+      for (int o = TPA / 2; o > 0; o >>= 1) {
+        qx += __shfl_xor_sync(0xffffffffu, qx, o);
+        qy += __shfl_xor_sync(0xffffffffu, qy, o);
+        qz += __shfl_xor_sync(0xffffffffu, qz, o);
+      }
+      fx = (double)qx * (1.0 / FORCE_FX);
+      fy = (double)qy * (1.0 / FORCE_FX);
+      fz = (double)qz * (1.0 / FORCE_FX);
+    }
+    double ke = 0.0;
+    if (valid && la == 0) {
+      if (FUSE) {
+        const double m = c.mass[P->type_off + ti - 1];
+        const double rmass = 1.0 / m;
+        const double dt = P->dt;
+        double *v = c.vel + 3 * (size_t)i;
+        double *a = c.acc + 3 * (size_t)i;
+        const double v0 = v[0] + 0.5 * dt * (fx * rmass + a[0]);
+        const double v1 = v[1] + 0.5 * dt * (fy * rmass + a[1]);
+        const double v2 = v[2] + 0.5 * dt * (fz * rmass + a[2]);
+        v[0] = v0; v[1] = v1; v[2] = v2;
+        a[0] = fx * rmass; a[1] = fy * rmass; a[2] = fz * rmass;
+        if (flags & F_CK) {
+          double kt = v0 * v0;
+          kt = kt + v1 * v1;
+          kt = kt + v2 * v2;
+          ke = kt * m;
+        }
+      } else {
+        double *f = c.force + 3 * (size_t)i;
+        f[0] = fx; f[1] = fy; f[2] = fz;
+      }
+    }
+    // per-tile partial sums (only what the step needs), then the last tile
+    // of the system runs the end-of-step epilogue
+    double red[8] = {pe, vir[0], vir[1], vir[2], vir[3], vir[4], vir[5], ke};
+    if (flags & (F_CU | F_CV)) {
+      block_sum<8>(red, sm);
+    } else if (flags & F_CK) {
+      double r1[1] = {ke};  // kinetic energy only (thermostat steps)
+      block_sum<1>(r1, sm);
+      red[7] = r1[0];
+    }
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) c.red[8 * (size_t)tile + k] = red[k];
+      __threadfence();
+      const unsigned nblk = (unsigned)(P->npad / TILE);
+      const unsigned t = atomicAdd(&S->ticket, 1u);
+      last = (t == nblk - 1);
+    }
     __syncthreads();
-    for (int il = ib + threadIdx.x; il < ie; il += NB_THREADS) {
-      const int cnt = ncnt[il - ib];
-      c.nnb[P->atom_off + il] = cnt;
-      if (cnt > maxnb) set_err(c, S, E_NEIMAX);
+    if (last) {
+      __threadfence();
+      finalize_system(c, sys, P->atom_off / TILE, P->npad / TILE, flags, FUSE, next_h);
+      if (threadIdx.x == 0) S->ticket = 0;
     }
     __syncthreads();
   }
@@ -911,27 +1225,67 @@ void launch_integrate1(const DevCtx &c, cudaStream_t st, int standalone, int mix
   k_integrate1<<<c.nchunks, BLOCK, 0, st>>>(c, standalone, mixed);
 }
 
+template <int TPA, bool MIXED, bool FUSE, int MODE>
+static void pair_go(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh) {
+  auto kern = k_pair<TPA, MIXED, FUSE, MODE>;
+  const int smem = MODE ? c.stab_smem : 0;
+  static int cfg_smem = -1, occ = 0;
+  if (smem != cfg_smem) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, TILE * TPA, smem);
+    if (occ < 1) occ = 1;
+    cfg_smem = smem;
+  }
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int ntiles = c.nchunks * (ATOM_ALIGN / TILE);
+  const int grid = ntiles < nsm * occ ? ntiles : nsm * occ;
+  kern<<<grid, TILE * TPA, smem, st>>>(c, hf, ntiles, nh);
+}
+
+template <int TPA, bool MIXED, bool FUSE>
+static void pair_mode(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh) {
+  if (c.stab_smem <= 0) pair_go<TPA, MIXED, FUSE, 0>(c, st, hf, nh);
+  else if (c.one_pair) pair_go<TPA, MIXED, FUSE, 2>(c, st, hf, nh);
+  else pair_go<TPA, MIXED, FUSE, 1>(c, st, hf, nh);
+}
+
 template <int TPA>
-static void pair_tpa(const DevCtx &c, cudaStream_t st, int mixed, int fuse, int hf) {
-  const int grid = c.nchunks * TPA;
+static void pair_tpa(const DevCtx &c, cudaStream_t st, int mixed, int fuse, int hf,
+                     unsigned long long nh) {
   if (mixed) {
-    if (fuse) k_pair<TPA, true, true><<<grid, BLOCK, 0, st>>>(c, hf);
-    else k_pair<TPA, true, false><<<grid, BLOCK, 0, st>>>(c, hf);
+    if (fuse) pair_mode<TPA, true, true>(c, st, hf, nh);
+    else pair_mode<TPA, true, false>(c, st, hf, nh);
   } else {
-    if (fuse) k_pair<TPA, false, true><<<grid, BLOCK, 0, st>>>(c, hf);
-    else k_pair<TPA, false, false><<<grid, BLOCK, 0, st>>>(c, hf);
+    if (fuse) pair_mode<TPA, false, true>(c, st, hf, nh);
+    else pair_mode<TPA, false, false>(c, st, hf, nh);
   }
 }
 
-void launch_pair(const DevCtx &c, cudaStream_t st, int tpa, int mixed, int fuse, int hf) {
+void launch_pair(const DevCtx &c, cudaStream_t st, int tpa, int mixed, int fuse, int hf,
+                 unsigned long long next_h) {
   switch (tpa) {
-    case 1: pair_tpa<1>(c, st, mixed, fuse, hf); break;
-    case 2: pair_tpa<2>(c, st, mixed, fuse, hf); break;
-    case 4: pair_tpa<4>(c, st, mixed, fuse, hf); break;
-    case 8: pair_tpa<8>(c, st, mixed, fuse, hf); break;
-    case 16: pair_tpa<16>(c, st, mixed, fuse, hf); break;
-    default: pair_tpa<32>(c, st, mixed, fuse, hf); break;
+    case 1: pair_tpa<1>(c, st, mixed, fuse, hf, next_h); break;
+    case 2: pair_tpa<2>(c, st, mixed, fuse, hf, next_h); break;
+    case 4: pair_tpa<4>(c, st, mixed, fuse, hf, next_h); break;
+    default: pair_tpa<8>(c, st, mixed, fuse, hf, next_h); break;
   }
+}
+
+// seed the first rebuild node of a captured step block from device state
+__global__ void k_decide(DevCtx c, unsigned long long h) {
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  for (int s = threadIdx.x; s < c.nsys_cap; s += blockDim.x)
+    if (c.P[s].n > 0 && (c.S[s].flags & F_ACTIVE) && c.S[s].rebuild) any = 1;
+  __syncthreads();
+  if (threadIdx.x == 0) cudaGraphSetConditional((cudaGraphConditionalHandle)h, any ? 1u : 0u);
+}
+
+void launch_decide(const DevCtx &c, cudaStream_t st, unsigned long long h) {
+  k_decide<<<1, 256, 0, st>>>(c, h);
 }
 
 void launch_integrate2(const DevCtx &c, cudaStream_t st, int ck) {
@@ -945,7 +1299,12 @@ void launch_rebuild(const DevCtx &c, cudaStream_t st, int force_all, int mixed) 
   k_order<<<(c.ncells + BLOCK / 32 - 1) / (BLOCK / 32), BLOCK, 0, st>>>(c, force_all);
   k_permute<<<c.nchunks, BLOCK, 0, st>>>(c, force_all);
   k_copyback<<<c.nchunks, BLOCK, 0, st>>>(c, force_all, mixed);
-  k_build<<<c.ncells, NB_THREADS, 0, st>>>(c, force_all);
+  static int cfg = -1;
+  if (c.nb_smem > cfg) {
+    cudaFuncSetAttribute(k_build, cudaFuncAttributeMaxDynamicSharedMemorySize, c.nb_smem);
+    cfg = c.nb_smem;
+  }
+  k_build<<<c.nchunks * (ATOM_ALIGN / TILE), NBT, c.nb_smem, st>>>(c, force_all);
 }
 
 void launch_begin_run(const DevCtx &c, cudaStream_t st, int nsys_cap, int nsteps, int cont) {

@@ -13,11 +13,18 @@ struct DevCtx {
   const int *chunk_sys;  // per ATOM_ALIGN-atom chunk: system id or -1
   const int *cell_sys;   // per global cell: system id or -1
   int nchunks, ncells, nsys_cap;
+  int stab_smem;  // shared-memory bytes of the staged pair tables, 0 = read from global
+  int nb_smem;  // neighbour build dynamic smem
   double4 *pos;
   int4 *pfx;
   double *vel, *acc, *disp, *force;
   int *gid;
-  int *nbr, *nnb;
+  int *nbr;  // blocked neighbour list (128-atom tiles), atom slots
+  int *nnb;
+  int *tile_nc, *tile_cell, *tile_coff;  // per 128-atom tile: cells staged by the build
+  int *tile_rows;  // per tile: rows of its list in use (L2 prefetch size)
+  int cand_cap;  // candidates a tile may stage in the pair kernel
+  int one_pair;  // every system has one type and one pair potential
   int *atom_cell, *atom_slot, *cell_count, *cell_start;
   int *perm, *tmp_src, *tmp_key;
   double4 *s_pos;
@@ -38,7 +45,11 @@ struct DevCtx {
 
 // launchers (stream-ordered; safe to capture in a CUDA graph)
 void launch_integrate1(const DevCtx &c, cudaStream_t st, int standalone, int mixed);
-void launch_pair(const DevCtx &c, cudaStream_t st, int tpa, int mixed, int fuse, int host_flags);
+// next_h: conditional-node handle of the next step's rebuild group (0 when
+// not launched inside a captured step block)
+void launch_pair(const DevCtx &c, cudaStream_t st, int tpa, int mixed, int fuse, int host_flags,
+                 unsigned long long next_h = 0);
+void launch_decide(const DevCtx &c, cudaStream_t st, unsigned long long h);
 void launch_integrate2(const DevCtx &c, cudaStream_t st, int ck);
 void launch_rebuild(const DevCtx &c, cudaStream_t st, int force_all, int mixed);
 void launch_begin_run(const DevCtx &c, cudaStream_t st, int nsys_cap, int nsteps, int cont);
@@ -46,6 +57,16 @@ void launch_flush(const DevCtx &c, cudaStream_t st, int nsys_cap);
 void launch_check(const DevCtx &c, cudaStream_t st, int nsys_cap);
 void launch_scale_vel(const DevCtx &c, cudaStream_t st, int sys, double lam);
 void launch_refresh_pfx(const DevCtx &c, cudaStream_t st);
+
+// bytes of shared memory a system's tables need in the staged layout of the
+// pair kernel: pair matrix, per-pair cutoffs/scales, then the F and P tables
+NDG_HD int stab_bytes(int ntypes, int npairs, int ptsize) {
+  int b = (ntypes * ntypes * 4 + 15) / 16 * 16;
+  b += npairs * 16;  // rc2 (double) + rc2f + vdr2
+  b = (b + 15) / 16 * 16;
+  b += npairs * (ptsize + 1) * 16;  // F and P: a double each, or a float2 each
+  return b;
+}
 
 // stencil of neighbour cells for a link-cell grid (shared host/device)
 NDG_HD int make_stencil(const int *mcell, int quirk, int *out) {

@@ -787,11 +787,20 @@ void ora_mk_iso_p(ora_sys *s) {
   box[2] = box[0] * lam[4] + box[1] * lam[3] + box[2] * lam[2];
 }
 
-/* dynamics main loop, src/nd.f90:137-180 */
+/* dynamics: prologue (lists) then the main loop */
 int ora_run(ora_sys *s, int nsteps, double dt, ora_thermo_cb cb, void *user) {
   s->c.dt = dt;
   int rc = ora_setup_lists(s);
   if (rc) return rc;
+  return ora_run_loop(s, nsteps, dt, cb, user);
+}
+
+/* dynamics main loop only, src/nd.f90:137-180 (the part the reference's
+ * 'Elapsed time for main dynamics' measures, :129,186) */
+int ora_run_loop(ora_sys *s, int nsteps, double dt, ora_thermo_cb cb, void *user) {
+  int rc;
+  s->c.dt = dt;
+  if (!s->lists_ready) return ORA_ERR_ARG;
   ora_control *c = &s->c;
   for (int tt = 1; tt <= nsteps; ++tt) {
     c->step = c->step + 1;

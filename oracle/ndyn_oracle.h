@@ -125,6 +125,8 @@ void ora_mk_iso_p(ora_sys *s);         /* src/nd.f90:1183-1213 */
 
 /* the whole dynamics loop for nsteps steps (src/nd.f90:60-199) */
 int ora_run(ora_sys *s, int nsteps, double dt, ora_thermo_cb cb, void *user);
+/* the loop alone, after ora_setup_lists (what the reference times) */
+int ora_run_loop(ora_sys *s, int nsteps, double dt, ora_thermo_cb cb, void *user);
 
 /* list inspection: cell (0-based ICELL-1) of each atom; neighbour pairs
  * (i<j, 0-based, one entry per occurrence in the half list) */

@@ -86,6 +86,7 @@ def lib():
         L.ora_integrate2.argtypes = [vp, i]
         L.ora_integrate2.restype = None
         L.ora_run.argtypes = [vp, i, d, THERMO_CB, vp]
+        L.ora_run_loop.argtypes = [vp, i, d, THERMO_CB, vp]
         L.ora_get_mcell.argtypes = [vp, vp]
         L.ora_get_cells.argtypes = [vp, vp]
         L.ora_get_neighbors.argtypes = [vp, vp, ctypes.c_long]
@@ -234,7 +235,8 @@ class Oracle:
     def check_list_update(self):
         return self.L.ora_check_list_update(self.s)
 
-    def run(self, nsteps, dt):
+    def run(self, nsteps, dt, loop_only=False):
+        """dynamics; loop_only skips the prologue (call setup_lists first)"""
         rows = []
 
         def cb(t, u):
@@ -243,7 +245,8 @@ class Oracle:
                              eerr=t.energy_error, press=t.pressure, vol=t.volume,
                              virial=list(t.virial), box=list(t.box)))
         c = THERMO_CB(cb)
-        rc = self.L.ora_run(self.s, int(nsteps), float(dt), c, None)
+        fn = self.L.ora_run_loop if loop_only else self.L.ora_run
+        rc = fn(self.s, int(nsteps), float(dt), c, None)
         return rc, rows
 
     def mcell(self):

@@ -244,3 +244,36 @@ def test_deterministic_repeat(specs):
     for a, b in zip(out[0][0], out[1][0]):
         assert np.array_equal(a, b)
     assert out[0][1] == out[1][1]
+
+
+@pytest.fixture(scope="module")
+def large_liquid():
+    # 78,732 atoms = 616 tiles of 128: every persistent CTA of the pair kernel
+    # works through several tiles (and table staging) per launch
+    return W.ar_liquid(27, 120.0, seed=31, quirk="fixed")
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("mixed", 1e-5)])
+def test_large_system_forces(large_liquid, prec, tol):
+    o = oracle_from_spec(large_liquid)
+    o.setup_lists()
+    o.compute0(1, 1)
+    fo, peo, viro, _ = o.forces()
+    with nd.Context(0, prec) as ctx:
+        sid = gpu_from_spec(ctx, large_liquid)
+        ctx.setup_lists()
+        ctx.compute0(True, True)
+        fg, peg, virg, _ = ctx.forces(sid)
+        assert np.array_equal(pair_multiset(ctx.neighbors(sid)), pair_multiset(o.neighbors()))
+    assert rel_l2(fg, fo) < tol
+    assert abs(peg - peo) <= max(tol, 1e-6) * abs(peo)
+
+
+def test_large_system_run_follows_oracle(large_liquid):
+    spec = dict(large_liquid)
+    spec["control"] = dict(spec["control"], out_steps=10)
+    o, ro, rg, _, nup = _run_both(spec, 40, precision="mixed")
+    assert nup == o.list_updates
+    for a, b in zip(rg, ro):
+        assert a["pe"] == pytest.approx(b["pe"], rel=1e-6)
+        assert a["ke"] == pytest.approx(b["ke"], rel=1e-5)
