@@ -198,6 +198,38 @@ int ndg_get_cells(ndg_ctx *ctx, int sys, int *cell);
 int ndg_get_neighbors(ndg_ctx *ctx, int sys, int *pairs, long long cap,
                       long long *npairs);
 
+/* ---- compute0 without device allocation ------------------------------- */
+/* No counterpart in the reference (which allocates nothing on a GPU).
+ *
+ * The same forces, potential energy and virial as ndg_compute (compute0,
+ * FP64) for one system, for callers that cannot allocate device memory:
+ * code that launches work while a CUDA stream is being captured into a
+ * graph (cudaMalloc is not allowed there), host applications that hand all
+ * of a GPU's memory to their own pool and only lend out buffers, and
+ * latency-bound loops that must not stall on the driver's allocator.
+ *
+ * The caller owns every buffer: pos_d (3*np, fractional, reference layout),
+ * typ_d (np), the tables fpair_d/ppair_d ((ptsize+1)*npairs, column-major)
+ * and the output force_d (3*np) are device pointers; pairmat (ntypes^2,
+ * column-major), rcpair (npairs) and box (3) are host arrays; skin and quirk
+ * select the link-cell grid as ndg_setup_lists does (skin >= 0).  potential
+ * and virial (6) are written on the host; the call returns when they are.
+ * stream is a cudaStream_t (NULL: the legacy default stream).
+ *
+ * Scratch lives in one static device array of about 0.8 MB that every GPU
+ * loading the library keeps until the process exits.  Limits: 32768 atoms,
+ * 32768 link cells, 8 types, 36 pairs; larger inputs return NDG_ERR_ARG
+ * with a message on stderr.  The first call on each device looks up the
+ * array's device address (cudaGetSymbolAddress), so make that first call
+ * before capturing a stream.  All calls share the array: calls that overlap
+ * on the GPU (other streams or threads) corrupt each other; order them. */
+int ndg_compute0_static(int np, int ntypes, int npairs, int ptsize, double ptrmin,
+                        const int *pairmat, const double *rcpair, double skin,
+                        int quirk, const double *box, const double *fpair_d,
+                        const double *ppair_d, const double *pos_d,
+                        const int *typ_d, double *force_d, double *potential,
+                        double *virial, void *stream);
+
 /* ---- tuning ------------------------------------------------------------ */
 /* threads per atom in the pair kernel (1,2,4,8,16,32; 0 = choose from the
  * mean neighbour count) and steps per CUDA-graph block */

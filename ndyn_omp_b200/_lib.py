@@ -53,6 +53,8 @@ SIGNATURES = [
     ("ndg_get_kernel_times", i, [vp, vp, vp, vp, vp]),
     ("ndg_get_stream", i, [vp, vp]),
     ("ndg_profile_run", i, [vp, i]),
+    ("ndg_compute0_static", i, [i, i, i, i, d, vp, vp, d, i, vp, vp, vp, vp, vp, vp, vp, vp,
+                                vp]),
 ]
 
 

@@ -27,7 +27,8 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC"
          "-Xcompiler", "-ffp-contract=off", "-ccbin", "/usr/bin/g++",
          "-I" + os.path.join(ROOT, "include")]
 
-LIB_SOURCES = ["ndg_kernels.cu", "ndg_context.cu", "ndg_tables.cpp", "ndg_server.cpp"]
+LIB_SOURCES = ["ndg_kernels.cu", "ndg_context.cu", "ndg_tables.cpp", "ndg_server.cpp",
+               "ndg_static.cu"]
 EXE_SOURCES = ["ndyn_main.cpp"]
 
 
