@@ -312,6 +312,7 @@ def main():
     nb_half = None
     if args.config != "c4":
         nb_half = len(ctx.neighbors(ids[0])) / len(specs[0]["typ"])
+    nup0 = sum(ctx.list_updates(i) for i in ids)
     s = torch.cuda.ExternalStream(ctx.stream_ptr)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier(ws)
@@ -323,6 +324,7 @@ def main():
         torch.cuda.synchronize()
     barrier(ws)
     ms = e0.elapsed_time(e1)
+    rebuilds = sum(ctx.list_updates(i) for i in ids) - nup0
     ms = allmax(ms, ws)
     value = N * args.steps * ws / (ms / 1e3)
     clocks = clk.summary()
@@ -397,6 +399,7 @@ def main():
                    "baseline_metric": "atom-steps/s at 1 GPU, batched mixed vs plain FP64 at "
                                       "stated force error; p50/p99"},
         "force_rel_err_vs_fp64": force_err,
+        "list_rebuilds_in_timed_region": rebuilds,
         "gpu_launches": 9 * args.steps + 3,
         "clocks": clocks,
         "roofline": roof,

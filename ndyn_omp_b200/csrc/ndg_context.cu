@@ -128,6 +128,7 @@ struct ndg_ctx {
   int tpa = 0, graph_steps = 100;
   int stab_smem = 0;  // staged-table bytes of the pair kernel (0: tables from global)
   int nb_smem = 0;  // neighbour-build dynamic smem
+  int nb_maxnb = 8, nb_vcap = 8192;
   int one_pair = 0;  // every system has one type and one pair (pair-kernel variant)
   std::map<int, cudaGraphExec_t> graphs;
   // per-kernel timing of the last profiled block
@@ -186,6 +187,8 @@ DevCtx devctx(ndg_ctx *c) {
   d.tile_coff = c->tile_coff;
   d.cand_cap = c->cand_cap;
   d.one_pair = c->one_pair;
+  d.nb_maxnb = c->nb_maxnb;
+  d.nb_vcap = c->nb_vcap;
   d.nnb = c->nnb;
   d.atom_cell = c->atom_cell;
   d.atom_slot = c->atom_slot;
@@ -416,14 +419,17 @@ int upload_params(ndg_ctx *c) {
     c->one_pair = one;
     drop_graphs(c);
   }
-  // neighbour build: 4096 staged candidates (16 B each) plus the 16-bit
-  // lists of the tile's 128 atoms
+  // neighbour build: 3072 staged candidates (16 B each), the 16-bit lists
+  // of the tile's 128 atoms, and the runs' flat candidate lists
   int mx = 8;
   for (auto &h : c->sys)
     if (h.alive) mx = std::max(mx, h.maxnb);
-  const int nbs = 4096 * 16 + 128 * mx * 2;
-  if (nbs != c->nb_smem) {
+  const int vcap = 8192;
+  const int nbs = 3072 * 16 + 128 * mx * 2 + vcap * 2;
+  if (nbs != c->nb_smem || mx != c->nb_maxnb) {
     c->nb_smem = nbs;
+    c->nb_maxnb = mx;
+    c->nb_vcap = vcap;
     drop_graphs(c);
   }
   int rc = 0;

@@ -601,7 +601,7 @@ constexpr int TILE = 128;      // atoms per tile
 constexpr int TC_MAX = 256;    // link cells a tile may stage
 constexpr int HSLOTS = 1024;   // shared hash slots for the tile's cell set
 constexpr float NB_MARGIN = 1e-5f;
-constexpr int BUILD_CAP = 4096;  // candidates the build stages per tile
+constexpr int BUILD_CAP = 3072;  // candidates the build stages per tile
 constexpr int NBT = 512;         // threads of the build CTA (16 warps)
 
 __device__ __forceinline__ int stencil_cell(int cl, int st, int M0, int M1, int M2) {
@@ -643,6 +643,8 @@ __global__ __launch_bounds__(NBT) void k_build(DevCtx c, int force_all) {
   const int maxnb = P->maxnb;
   int4 *cpf = (int4 *)dsm;                                   // BUILD_CAP candidates
   unsigned short *lst = (unsigned short *)(cpf + BUILD_CAP);  // TILE * maxnb
+  unsigned short *vlist = lst + TILE * c.nb_maxnb;             // flat per-run lists
+  const int vcap = c.nb_vcap;
   __shared__ int hset[HSLOTS];
   __shared__ int ucell[TC_MAX + 1], coff[TC_MAX + 1], ustart[TC_MAX];
   __shared__ int stc[MAX_STENCIL];
@@ -650,6 +652,8 @@ __global__ __launch_bounds__(NBT) void k_build(DevCtx c, int force_all) {
   __shared__ short run_of[TILE];               // own atom -> run of equal cells
   __shared__ int run_cell[TILE];
   __shared__ short ent_u[TILE * MAX_STENCIL];  // run x stencil entry -> staged cell
+  __shared__ short epre[TILE * MAX_STENCIL];   // run x entry -> offset in the run's list
+  __shared__ int vsize[TILE], vstart[TILE], run_t0[TILE + 1];
   __shared__ int nu, bad, nruns, rows_s;
   __shared__ int pm_s[16 * 16];
   __shared__ float rl2f_s[136];
@@ -774,11 +778,13 @@ __global__ __launch_bounds__(NBT) void k_build(DevCtx c, int force_all) {
       const int cl = c.atom_cell[a0 + t];
       if (cl != prev) {
         run_cell[++r] = cl;
+        run_t0[r] = t;
         prev = cl;
       }
       run_of[t] = (short)r;
     }
     nruns = r + 1;
+    run_t0[nruns] = nown;
   }
   __syncthreads();
   for (int idx = threadIdx.x; idx < nruns * ne; idx += NBT) {
@@ -787,30 +793,78 @@ __global__ __launch_bounds__(NBT) void k_build(DevCtx c, int force_all) {
         (short)find_cell(ucell, U, stencil_cell(run_cell[r], stc[e], M0, M1, M2));
   }
   __syncthreads();
-  // 3. one warp per own atom
-  for (int t = warp; t < nown; t += NBT / 32) {
-    const int i = a0 + t;
-    const double4 pid = c.pos[i];
-    const int4 pi = make_int4(fx32(pid.x), fx32(pid.y), fx32(pid.z), tw_of(pid.w));
-    const int ti = tw_type(pi.w);
-    const short *eu = ent_u + run_of[t] * MAX_STENCIL;
-    unsigned short *mylst = lst + t * maxnb;
-    int cnt = 0;
+  // each run's candidates as one flat list: its stencil entries' staged
+  // ranges back to back (entries repeat where the reference's half stencil
+  // reaches a cell twice), bit 15 marks the run's own cell (PTrMin test)
+  if (threadIdx.x < nruns) {
+    const int r = threadIdx.x;
+    int tot = 0;
     for (int e = 0; e < ne; ++e) {
-      const bool center = (stc[e] >> 12) & 1;
-      const int u = eu[e];
-      const int q0 = coff[u], q1 = coff[u + 1];
-      for (int qb = q0; qb < q1; qb += 32) {
-        const int q = qb + lane;
+      epre[r * MAX_STENCIL + e] = (short)tot;
+      const int u = ent_u[r * MAX_STENCIL + e];
+      tot += coff[u + 1] - coff[u];
+    }
+    vsize[r] = tot;
+  }
+  __syncthreads();
+  const int *__restrict__ pmg = pm;
+  const bool one = nt == 1 && npr == 1;
+  for (int rb = 0; rb < nruns;) {
+    // the runs whose lists fit the buffer together
+    __shared__ int re_s;
+    if (threadIdx.x == 0) {
+      int re = rb, tot = 0;
+      while (re < nruns && tot + vsize[re] <= vcap) {
+        vstart[re] = tot;
+        tot += vsize[re];
+        ++re;
+      }
+      re_s = re;
+      if (re == rb) bad = 1;  // one run alone exceeds the buffer
+    }
+    __syncthreads();
+    if (bad) break;
+    const int re = re_s;
+    for (int w = warp; w < (re - rb) * ne; w += NBT / 32) {
+      const int r = rb + w / ne, e = w % ne;
+      const int u = ent_u[r * MAX_STENCIL + e];
+      const int q0 = coff[u], len = coff[u + 1] - q0;
+      const unsigned short cflag = ((stc[e] >> 12) & 1) ? 0x8000u : 0u;
+      unsigned short *dst = vlist + vstart[r] + epre[r * MAX_STENCIL + e];
+      for (int k = lane; k < len; k += 32) dst[k] = (unsigned short)(q0 + k) | cflag;
+    }
+    __syncthreads();
+    // 3. one warp per own atom, 32 candidates of the flat list per pass
+    for (int t = run_t0[rb] + warp; t < run_t0[re]; t += NBT / 32) {
+      const int i = a0 + t;
+      const int r = run_of[t];
+      const double4 pid = c.pos[i];
+      const int4 pi = make_int4(fx32(pid.x), fx32(pid.y), fx32(pid.z), tw_of(pid.w));
+      const int ti = tw_type(pi.w);
+      // the atom's own slot among the staged candidates
+      const int uo = find_cell(ucell, U, run_cell[r]);
+      const int qi = coff[uo] + (i - (P->atom_off + ustart[uo]));
+      const unsigned short *vl = vlist + vstart[r];
+      const int V = vsize[r];
+      unsigned short *mylst = lst + t * maxnb;
+      int cnt = 0;
+      for (int vb = 0; vb < V; vb += 32) {
+        const int v = vb + lane;
         bool hit = false;
-        if (q < q1) {
-          const int j = P->atom_off + ustart[u] + (q - q0);
+        int q = 0;
+        if (v < V) {
+          const unsigned short raw = vl[v];
+          q = raw & 0x7fff;
+          const bool center = raw >> 15;
           const int4 pj = cpf[q];
-          const int tj = tw_type(pj.w);
-          const int a = pm[(ti - 1) + (tj - 1) * nt];
-          const int b = pm[(tj - 1) + (ti - 1) * nt];
-          const int mx = a > b ? a : b;
-          if (j != i && mx > 0) {
+          int mx = 1;
+          if (!one) {
+            const int tj = tw_type(pj.w);
+            const int a = pmg[(ti - 1) + (tj - 1) * nt];
+            const int b = pmg[(tj - 1) + (ti - 1) * nt];
+            mx = a > b ? a : b;
+          }
+          if (q != qi && mx > 0) {
             const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * sb0;
             const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * sb1;
             const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * sb2;
@@ -820,7 +874,8 @@ __global__ __launch_bounds__(NBT) void k_build(DevCtx c, int force_all) {
             const bool near_min = center && d2f >= ptrlo && d2f <= ptrhi;
             if (near_cut || near_min) {
               // the reference's FP64 test (src/nd.f90:1362-1377)
-              const double4 pjd = c.pos[j];
+              const int u = find_cell(coff + 1, U, q + 1);
+              const double4 pjd = c.pos[P->atom_off + ustart[u] + (q - coff[u])];
               double s0 = pid.x - pjd.x, s1 = pid.y - pjd.y, s2 = pid.z - pjd.z;
               s0 = s0 - round(s0);
               s1 = s1 - round(s1);
@@ -843,10 +898,20 @@ __global__ __launch_bounds__(NBT) void k_build(DevCtx c, int force_all) {
         }
         cnt += __popc(bal);
       }
+      if (lane == 0) ncnt[t] = cnt;
     }
-    if (lane == 0) ncnt[t] = cnt;
+    __syncthreads();
+    rb = re;
   }
-  __syncthreads();
+  if (bad) {
+    if (threadIdx.x == 0) {
+      c.tile_nc[tile] = 0;
+      c.tile_rows[tile] = 0;
+      set_err(c, S, E_NEIMAX);
+    }
+    if (threadIdx.x < nown) c.nnb[a0 + threadIdx.x] = 0;
+    return;
+  }
   // 4. write the tile's lists row by row (consecutive threads, consecutive atoms)
   if (threadIdx.x == 0) {
     int r = 0;
