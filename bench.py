@@ -1,15 +1,17 @@
 """Benchmark of the Ndyn MD timestep path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c2]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c4]
                     [--impl ours|reference] [--precision mixed|fp64]
 
 A step is one MD timestep (the dynamics loop body, src/nd.f90:138-178) of
-the configured system.  Default workload (c2): LJ argon liquid, 256,000
-atoms on a +-0.05 sigma jittered FCC lattice at reduced density 0.8442,
-Berendsen thermostat to 120 K (tau = 100 steps), dt = 0.1, mixed precision,
-fixed list-rebuild semantics.  Other workloads: c1 (Cu Morse crystal 4000
-atoms, FP64, NVE), c3 (rocksalt Buckingham 1,048,576 atoms, NPT), c4 (512
-replicas in one launch).
+every system of the workload.  Default workload (c4): 512 independent
+replicas (half Cu Morse crystals, half LJ argon liquids, 500-20,000 atoms
+each, own Berendsen thermostats) stepped together in mixed precision, with
+the plain single-system FP64 path timed on a sample of the same replicas
+one after another, and the mixed path's force error against FP64 on the
+thermalised replicas.  Other workloads: c1 (Cu Morse crystal 4000 atoms,
+FP64, NVE), c2 (LJ argon liquid 256,000 atoms, NVT, mixed), c3 (rocksalt
+Buckingham 1,048,576 atoms, NPT).
 
 Multi-GPU: the workload does not shard (one system per GPU, no exchange),
 so N ranks run N independent replicas ("replicas only"): value is the
@@ -39,7 +41,7 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=50)
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--config", default="c4", choices=["c1", "c2", "c3", "c4"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default=None, choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -179,6 +181,61 @@ def n_atoms(specs):
     return sum(len(s["typ"]) for s in specs)
 
 
+def rel_l2(a, b):
+    a, b = np.asarray(a, np.float64).ravel(), np.asarray(b, np.float64).ravel()
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def force_error(specs, states, local):
+    """Relative L2 force error of the mixed path against the FP64 path on the
+    given configurations: over all atoms of all systems, and the largest
+    per-system value."""
+    import ndyn_omp_b200 as nd
+    from ndyn_omp_b200 import workloads as W
+    fs = {}
+    for p in ("fp64", "mixed"):
+        with nd.Context(local, p) as cx:
+            ids = []
+            for sp, st in zip(specs, states):
+                q = dict(sp)
+                if st is not None:
+                    q.update(pos=st[0], vel=st[1], box=st[3])
+                ids.append(W.add_to_context(cx, q))
+            cx.setup_lists()
+            cx.compute0(True, True)
+            fs[p] = [cx.forces(i)[0] for i in ids]
+    per = [rel_l2(m, f) for m, f in zip(fs["mixed"], fs["fp64"])]
+    allv = rel_l2(np.concatenate([f.ravel() for f in fs["mixed"]]),
+                  np.concatenate([f.ravel() for f in fs["fp64"]]))
+    return allv, max(per)
+
+
+def plain_fp64_rate(specs, local, steps, stride):
+    """The plain path: each sampled replica alone in an FP64 context (its own
+    list build and graphs, untimed), `steps` steps timed with CUDA events on
+    the library's stream; returns summed atom-steps / summed time."""
+    import torch
+
+    import ndyn_omp_b200 as nd
+    from ndyn_omp_b200 import workloads as W
+    tot_as, tot_s, n = 0.0, 0.0, 0
+    for sp in specs[::stride]:
+        with nd.Context(local, "fp64") as cx:
+            sid = W.add_to_context(cx, sp)
+            cx.run(100)  # list build and the 100-step graph capture
+            st = torch.cuda.ExternalStream(cx.stream_ptr)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(st)
+            cx.run(steps, cont=True)
+            e1.record(st)
+            torch.cuda.synchronize()
+            tot_s += e0.elapsed_time(e1) / 1e3
+            tot_as += len(sp["typ"]) * steps
+            n += 1
+    return tot_as / tot_s, n
+
+
 # ---------------------------------------------------------------------------
 def dist_init():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
@@ -291,16 +348,8 @@ def main():
     # stated force error of this precision against the FP64 path (the FP64
     # path itself matches the CPU oracle to 1e-12, tests/test_gpu_parity.py)
     force_err = None
-    if prec == "mixed":
-        fs = {}
-        probe = specs[:1] if args.config != "c4" else specs[:8]
-        for p in ("fp64", "mixed"):
-            with nd.Context(local, p) as cx:
-                ids = [W.add_to_context(cx, s) for s in probe]
-                cx.setup_lists()
-                cx.compute0(True, True)
-                fs[p] = np.concatenate([cx.forces(i)[0].ravel() for i in ids])
-        force_err = float(np.linalg.norm(fs["mixed"] - fs["fp64"]) / np.linalg.norm(fs["fp64"]))
+    if prec == "mixed" and args.config != "c4":
+        force_err, _ = force_error(specs[:1], [None], local)
 
     ctx = nd.Context(local, prec)
     ids = [W.add_to_context(ctx, s) for s in specs]
@@ -309,9 +358,8 @@ def main():
         ctx.autotune(10)
     # warm-up (includes the dynamics prologue: cell + Verlet list build)
     ctx.run(max(args.warmup, 3))
-    nb_half = None
-    if args.config != "c4":
-        nb_half = len(ctx.neighbors(ids[0])) / len(specs[0]["typ"])
+    # half the full-list entries per atom (each pair once)
+    nb_half = sum(ctx.neighbor_count(i) for i in ids) / (2.0 * N)
     nup0 = sum(ctx.list_updates(i) for i in ids)
     s = torch.cuda.ExternalStream(ctx.stream_ptr)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -329,13 +377,29 @@ def main():
     value = N * args.steps * ws / (ms / 1e3)
     clocks = clk.summary()
 
+    extra = {}
+    if args.config == "c4":
+        # the mixed path's force error on the thermalised replicas, and the
+        # plain single-system FP64 path on every 8th replica in sequence
+        states = [ctx.state(i) for i in ids]
+        if prec == "mixed":
+            ea, em = force_error(specs, states, local)
+            force_err = ea
+            extra["force_rel_err_max_replica"] = em
+        prate, pn = plain_fp64_rate(specs, local, 200, 8)
+        extra["plain_fp64"] = {
+            "value": prate, "unit": "atom-steps/s",
+            "sample": f"{pn} of 512 replicas (every 8th), each alone in an FP64 context, "
+                      f"200 steps, CUDA-graph blocks of 100",
+            "batched_over_plain": (value / ws) / prate}
+
     # per-kernel mean launch time over the same kind of steps (eager launches
     # with CUDA events on the library's stream)
     prof = ctx.profile_run(min(200, max(20, args.steps // 10)))
     tpa, gsteps = ctx.tuning()
     peak, peak_kind = hbm_peak()
     roof = None
-    if nb_half is not None:
+    if nb_half:
         # algorithmic bytes of the fused pair kernel per atom: half-list
         # indices 4*n_half + own position/type 28 + neighbour positions 24
         # (each read once) + integrate2 state (read vel, acc; write vel, acc) 96
@@ -351,26 +415,30 @@ def main():
 
     # end to end through the C ABI with host buffers: load state, run, read
     # state back (what a caller of ndg_load_state/ndg_run/ndg_get_state pays)
-    e2e = None
-    if args.config != "c4":
-        sp = specs[0]
-        pos0, vel0, acc0, box0 = ctx.state(ids[0])
-        pin = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
-               for a in (pos0, vel0, acc0)]
-        barrier(ws)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        ctx.load_state(ids[0], pin[0], pin[1], pin[2], box0)
-        rows = ctx.run(args.steps)
-        out = ctx.state(ids[0])
-        torch.cuda.synchronize()
-        el = allmax(time.perf_counter() - t0, ws)
-        n = len(sp["typ"])
-        h2d = n * (32 + 24 * 3 + 4)            # pos(+type) double4, vel, acc, disp, gid
-        d2h = n * (36 + 4 + 32 + 24 * 2) + 120 * len(rows)  # types for load, gid, pos, vel, acc, thermo
-        e2e = {"value": n * args.steps * ws / el, "unit": "atom-steps/s",
-               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-               "what": "ndg_load_state + ndg_run(K) (incl. list build) + ndg_get_state"}
+    # end to end through the C ABI with host buffers: load every system's
+    # state from pinned host memory, run K steps (prologue list build
+    # included), read every state back
+    host = []
+    for i in ids:
+        pos0, vel0, acc0, box0 = ctx.state(i)
+        host.append([torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+                     for a in (pos0, vel0, acc0)] + [box0])
+    barrier(ws)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i, hs in zip(ids, host):
+        ctx.load_state(i, hs[0], hs[1], hs[2], hs[3])
+    rows = ctx.run(args.steps)
+    for i in ids:
+        ctx.state(i)
+    torch.cuda.synchronize()
+    el = allmax(time.perf_counter() - t0, ws)
+    h2d = N * (32 + 24 * 3 + 4)            # pos(+type) double4, vel, acc, disp, gid
+    d2h = N * (36 + 4 + 32 + 24 * 2) + 120 * len(rows)  # types for load, gid, pos, vel, acc, thermo
+    e2e = {"value": N * args.steps * ws / el, "unit": "atom-steps/s",
+           "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+           "what": "ndg_load_state + ndg_run(K) (incl. list build) + ndg_get_state, "
+                   "every system"}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -399,8 +467,12 @@ def main():
                    "baseline_metric": "atom-steps/s at 1 GPU, batched mixed vs plain FP64 at "
                                       "stated force error; p50/p99"},
         "force_rel_err_vs_fp64": force_err,
+        **extra,
         "list_rebuilds_in_timed_region": rebuilds,
-        "gpu_launches": 9 * args.steps + 3,
+        # per step integrate1 + pair; per graph block k_decide; the 7 rebuild
+        # kernels on steps whose conditional node fires (at most one per
+        # step, at most one per list update)
+        "gpu_launches": 2 * args.steps + -(-args.steps // gsteps) + 7 * min(args.steps, rebuilds),
         "clocks": clocks,
         "roofline": roof,
         "cpu_baseline": cpu,

@@ -197,6 +197,9 @@ int ndg_get_cells(ndg_ctx *ctx, int sys, int *cell);
  * pairs == NULL returns the count in *npairs. */
 int ndg_get_neighbors(ndg_ctx *ctx, int sys, int *pairs, long long cap,
                       long long *npairs);
+/* total entries of the system's full neighbour list (each pair counted
+ * from both atoms), the length the pair loop of compute0 walks */
+int ndg_get_neighbor_count(ndg_ctx *ctx, int sys, long long *entries);
 
 /* ---- compute0 without device allocation ------------------------------- */
 /* No counterpart in the reference (which allocates nothing on a GPU).
@@ -231,8 +234,8 @@ int ndg_compute0_static(int np, int ntypes, int npairs, int ptsize, double ptrmi
                         double *virial, void *stream);
 
 /* ---- tuning ------------------------------------------------------------ */
-/* threads per atom in the pair kernel (1,2,4,8,16,32; 0 = choose from the
- * mean neighbour count) and steps per CUDA-graph block */
+/* threads per atom in the pair kernel (1,2,4,8; 0 = choose from the atom
+ * count and mean neighbour count) and steps per CUDA-graph block */
 int ndg_set_tuning(ndg_ctx *ctx, int threads_per_atom, int graph_steps);
 int ndg_get_tuning(ndg_ctx *ctx, int *threads_per_atom, int *graph_steps);
 /* time candidate launch shapes on the current systems for a few steps and

@@ -45,6 +45,7 @@ SIGNATURES = [
     ("ndg_get_mcell", i, [vp, i, vp]),
     ("ndg_get_cells", i, [vp, i, vp]),
     ("ndg_get_neighbors", i, [vp, i, vp, ll, vp]),
+    ("ndg_get_neighbor_count", i, [vp, i, vp]),
     ("ndg_set_tuning", i, [vp, i, i]),
     ("ndg_get_tuning", i, [vp, vp, vp]),
     ("ndg_autotune", i, [vp, i]),

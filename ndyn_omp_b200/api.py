@@ -271,6 +271,12 @@ class Context:
         _ok(self.L.ndg_get_cells(self._c, sys, _p(c)), "get_cells")
         return c
 
+    def neighbor_count(self, sys=0):
+        """entries of the full neighbour list (each pair from both atoms)"""
+        n = ctypes.c_longlong()
+        _ok(self.L.ndg_get_neighbor_count(self._c, sys, ctypes.byref(n)), "get_neighbor_count")
+        return n.value
+
     def neighbors(self, sys=0):
         n = ctypes.c_longlong()
         _ok(self.L.ndg_get_neighbors(self._c, sys, None, 0, ctypes.byref(n)), "get_neighbors")

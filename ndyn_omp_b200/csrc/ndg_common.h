@@ -47,7 +47,9 @@ enum : int {
   F_KE_SCALE = 32, // mkIsoKE after this step
   F_P_SCALE = 64,  // mkIsoP after this step
   F_E_SCALE = 128, // mkIsoE after this step
-  F_FIRST = 256    // first step of a run (tt == 1): e0 is set
+  F_FIRST = 256,   // first step of a run (tt == 1): e0 is set
+  F_DONE = 512     // the pair kernel finished this step (set with the next
+                   // step's flags, cleared by the next integrate1)
 };
 
 // error bits (SysState::err)

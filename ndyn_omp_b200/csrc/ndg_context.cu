@@ -111,6 +111,7 @@ struct ndg_ctx {
   int *cell_count = nullptr, *cell_start = nullptr;
   int *nbr = nullptr;
   int *tile_rows = nullptr;
+  int *rb_list = nullptr;  // systems listed for a list rebuild
   int *tile_nc = nullptr, *tile_cell = nullptr, *tile_coff = nullptr;
   int cand_cap = 6144;  // candidates a tile stages in the pair kernel
   double *red = nullptr, *itop = nullptr, *ired = nullptr;
@@ -217,6 +218,7 @@ DevCtx devctx(ndg_ctx *c) {
   d.ired = c->ired;
   d.ring = c->ring;
   d.ring_count = c->ring_count;
+  d.rb_list = c->rb_list;
   d.ring_cap = c->ring_cap;
   d.stab_smem = c->stab_smem;
   d.nb_smem = c->nb_smem;
@@ -308,6 +310,7 @@ int grow_sys(ndg_ctx *c, int n) {
   int rc = 0;
   rc |= grow(c, c->dP, (size_t)c->nsys_cap, (size_t)n);
   rc |= grow(c, c->dS, (size_t)c->nsys_cap, (size_t)n);
+  rc |= grow(c, c->rb_list, 0, (size_t)n);
   if (rc) return NDG_ERR_NOMEM;
   std::vector<SysParam> z(n - c->nsys_cap);
   std::vector<SysState> zs(n - c->nsys_cap);
@@ -449,6 +452,10 @@ int upload_params(ndg_ctx *c) {
   return NDG_OK;
 }
 
+// upload the per-pair/per-type arrays once before the next launch that
+// needs them, so that adding many systems stays linear in their number
+int ensure_params(ndg_ctx *c) { return c->params_dirty ? upload_params(c) : NDG_OK; }
+
 void fill_control_params(HostSys &h) {
   SysParam &p = h.prm;
   const ndg_control &q = h.ctl;
@@ -534,6 +541,17 @@ int upload_atoms(ndg_ctx *c, int s, const int *typ, const double *pos, const dou
   return NDG_OK;
 }
 
+// put every live system on the rebuild list (the setup paths rebuild all)
+int list_all_systems(ndg_ctx *c) {
+  std::vector<int> ids;
+  for (size_t s = 0; s < c->sys.size(); ++s)
+    if (c->sys[s].alive) ids.push_back((int)s);
+  const int n = (int)ids.size();
+  if (n) CK(c, cudaMemcpy(c->rb_list, ids.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+  CK(c, cudaMemcpy(c->ring_count + 3, &n, sizeof(int), cudaMemcpyHostToDevice));
+  return NDG_OK;
+}
+
 // dynamics prologue for every system, src/nd.f90:73-108: skin default,
 // MCELL, neighbour capacity; then one rebuild of all lists.
 int setup_lists(ndg_ctx *c) {
@@ -611,10 +629,13 @@ int setup_lists(ndg_ctx *c) {
   int rc = upload_params(c);
   if (rc) return rc;
   CK(c, cudaMemset(c->ring_count, 0, 4 * sizeof(int)));
+  rc = list_all_systems(c);
+  if (rc) return rc;
   DevCtx d = devctx(c);
-  launch_rebuild(d, c->st, 1, c->precision == NDG_PREC_MIXED);
+  launch_rebuild(d, c->st, 0, c->precision == NDG_PREC_MIXED);
   CK(c, cudaGetLastError());
   CK(c, cudaStreamSynchronize(c->st));
+  CK(c, cudaMemset(c->ring_count + 3, 0, sizeof(int)));
   int words[4];
   CK(c, cudaMemcpy(words, c->ring_count, sizeof(words), cudaMemcpyDeviceToHost));
   if (words[1]) {
@@ -640,7 +661,7 @@ int choose_tpa(ndg_ctx *c) {
   nb /= atoms;
   // enough threads to fill the 148 SMs, and about 16+ neighbours per thread
   int t = 1;
-  while (t < 32 && ((double)atoms * t < 148.0 * 1024.0 || nb / t > 48.0)) t *= 2;
+  while (t < 8 && ((double)atoms * t < 148.0 * 1024.0 || nb / t > 48.0)) t *= 2;
   return t;
 }
 
@@ -649,7 +670,7 @@ void enqueue_steps(ndg_ctx *c, int nsteps) {
   const int mixed = c->precision == NDG_PREC_MIXED;
   const int tpa = choose_tpa(c);
   for (int k = 0; k < nsteps; ++k) {
-    launch_rebuild(d, c->st, 0, mixed);
+    launch_rebuild(d, c->st, 1, mixed);
     launch_integrate1(d, c->st, 0, mixed);
     launch_pair(d, c->st, tpa, mixed, 1, 0);
   }
@@ -688,7 +709,7 @@ int capture_block(ndg_ctx *c, int g, cudaGraphExec_t *out) {
   DevCtx d = devctx(c);
   const int mixed = c->precision == NDG_PREC_MIXED;
   const int tpa = choose_tpa(c);
-  if (!c->st2) CK(c, cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking));
+  if (!c->st2) CK(c, cudaStreamCreate(&c->st2));
   cudaGraph_t graph;
   CK(c, cudaGraphCreate(&graph, 0));
   std::vector<cudaGraphConditionalHandle> h(g);
@@ -714,7 +735,7 @@ int capture_block(ndg_ctx *c, int g, cudaGraphExec_t *out) {
     CK(c, cudaStreamUpdateCaptureDependencies(c->st, &cn, 1, cudaStreamSetCaptureDependencies));
     CK(c, cudaStreamBeginCaptureToGraph(c->st2, body, nullptr, nullptr, 0,
                                         cudaStreamCaptureModeThreadLocal));
-    launch_rebuild(d, c->st2, 0, mixed);
+    launch_rebuild(d, c->st2, 1, mixed);
     cudaGraph_t body_out;
     CK(c, cudaStreamEndCapture(c->st2, &body_out));
     launch_integrate1(d, c->st, 0, mixed);
@@ -776,7 +797,7 @@ ndg_ctx::~ndg_ctx() {
   drop_graphs(this);
   void *ptrs[] = {dP, dS, chunk_sys, cell_sys, pos, s_pos, pfx, vel, acc, disp, force, s_vel,
                   s_acc, gid, s_gid, s_cell, nnb, atom_cell, atom_slot, perm, tmp_src, tmp_key,
-                  cell_count, cell_start, nbr, tile_rows, tile_nc, tile_cell, tile_coff, red, itop, ired, pairmat, mass, rc2, rlist2,
+                  cell_count, cell_start, rb_list, nbr, tile_rows, tile_nc, tile_cell, tile_coff, red, itop, ired, pairmat, mass, rc2, rlist2,
                   vdr2, rc2f, tabF, tabP, tabF2, tabP2, ring, ring_count};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -836,7 +857,9 @@ int ndg_create(ndg_ctx **out, int device, int precision) {
   ndg_ctx *c = new ndg_ctx();
   c->device = device;
   c->precision = precision;
-  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
+  // a blocking stream: the host paths' plain cudaMemcpy/cudaMemset (legacy
+  // default stream) are ordered with the kernels launched on it
+  if (cudaStreamCreate(&c->st) != cudaSuccess) {
     delete c;
     return NDG_ERR_CUDA;
   }
@@ -871,6 +894,8 @@ int ndg_set_precision(ndg_ctx *c, int precision) {
     c->precision = precision;
     drop_graphs(c);
     if (precision == NDG_PREC_MIXED) {
+      int e = ensure_params(c);
+      if (e) return e;
       DevCtx d = devctx(c);
       launch_refresh_pfx(d, c->st);
       CK(c, cudaStreamSynchronize(c->st));
@@ -959,13 +984,9 @@ int ndg_add_system(ndg_ctx *c, int np, int ntypes, int npairs, int ptsize, doubl
   if (rc) return rc;
   rc = upload_atoms(c, s, typ, pos, vel, acc);
   if (rc) return rc;
-  rc = upload_params(c);
-  if (rc) return rc;
-  if (c->precision == NDG_PREC_MIXED) {
-    DevCtx d = devctx(c);
-    launch_refresh_pfx(d, c->st);
-    CK(c, cudaStreamSynchronize(c->st));
-  }
+  // per-pair/per-type arrays are uploaded once before the next launch; the
+  // fixed-point positions are written by the list build every run starts with
+  c->params_dirty = true;
   if (sys_out) *sys_out = s;
   return NDG_OK;
 }
@@ -989,7 +1010,8 @@ int ndg_remove_system(ndg_ctx *c, int s) {
   memset(&S, 0, sizeof(S));
   int rc = put_state_dev(c, s, S);
   if (rc) return rc;
-  return upload_params(c);
+  c->params_dirty = true;
+  return ensure_params(c);
 }
 
 int ndg_num_systems(const ndg_ctx *c) {
@@ -1003,7 +1025,9 @@ int ndg_load_state(ndg_ctx *c, int s, const double *pos, const double *vel, cons
                    const double *box) {
   if (!valid_sys(c, s) || !pos) return NDG_ERR_ARG;
   cudaSetDevice(c->device);
-  int rc = upload_atoms(c, s, nullptr, pos, vel, acc);
+  int rc = ensure_params(c);
+  if (rc) return rc;
+  rc = upload_atoms(c, s, nullptr, pos, vel, acc);
   if (rc) return rc;
   if (box) {
     SysState S;
@@ -1076,7 +1100,8 @@ int ndg_set_control(ndg_ctx *c, int s, const ndg_control *q) {
   S.step = q->step;
   rc = put_state_dev(c, s, S);
   if (rc) return rc;
-  return upload_params(c);
+  c->params_dirty = true;
+  return NDG_OK;
 }
 
 int ndg_get_control(ndg_ctx *c, int s, ndg_control *q) {
@@ -1097,13 +1122,20 @@ int ndg_setup_lists(ndg_ctx *c) {
 
 int ndg_build_cell_list(ndg_ctx *c) {
   if (!c) return NDG_ERR_ARG;
+  {
+    int e = ensure_params(c);
+    if (e) return e;
+  }
   for (auto &h : c->sys)
     if (h.alive && h.maxnb == 0) return setup_lists(c);
   DevCtx d = devctx(c);
   CK(c, cudaMemset(c->ring_count, 0, 4 * sizeof(int)));
-  launch_rebuild(d, c->st, 1, c->precision == NDG_PREC_MIXED);
+  int rc = list_all_systems(c);
+  if (rc) return rc;
+  launch_rebuild(d, c->st, 0, c->precision == NDG_PREC_MIXED);
   CK(c, cudaGetLastError());
-  int rc = status_from_words(c);
+  rc = status_from_words(c);
+  CK(c, cudaMemset(c->ring_count + 3, 0, sizeof(int)));
   if (!rc)
     for (auto &h : c->sys)
       if (h.alive) h.lists_valid = true;
@@ -1118,12 +1150,17 @@ static bool lists_ready(ndg_ctx *c) {
 
 int ndg_check_list_update(ndg_ctx *c, int *rebuilt) {
   if (!c || !lists_ready(c)) return NDG_ERR_ARG;
+  {
+    int e = ensure_params(c);
+    if (e) return e;
+  }
   DevCtx d = devctx(c);
   CK(c, cudaMemset(c->ring_count, 0, 4 * sizeof(int)));
-  launch_check(d, c->st, c->nsys_cap);
-  launch_rebuild(d, c->st, 0, c->precision == NDG_PREC_MIXED);
+  launch_check(d, c->st, c->nsys_cap);  // lists the systems to rebuild
+  launch_rebuild(d, c->st, 1, c->precision == NDG_PREC_MIXED);
   CK(c, cudaGetLastError());
   int rc = status_from_words(c);
+  CK(c, cudaMemset(c->ring_count + 3, 0, sizeof(int)));
   if (rc) return rc;
   if (rebuilt) {
     std::vector<SysState> S(c->nsys_cap);
@@ -1137,6 +1174,10 @@ int ndg_check_list_update(ndg_ctx *c, int *rebuilt) {
 
 int ndg_integrate1(ndg_ctx *c) {
   if (!c) return NDG_ERR_ARG;
+  {
+    int e = ensure_params(c);
+    if (e) return e;
+  }
   std::vector<SysState> S(c->nsys_cap);
   CK(c, cudaMemcpy(S.data(), c->dS, S.size() * sizeof(SysState), cudaMemcpyDeviceToHost));
   for (auto &x : S)
@@ -1151,6 +1192,10 @@ int ndg_integrate1(ndg_ctx *c) {
 
 int ndg_compute(ndg_ctx *c, int cv, int cu) {
   if (!c || !lists_ready(c)) return NDG_ERR_ARG;
+  {
+    int e = ensure_params(c);
+    if (e) return e;
+  }
   DevCtx d = devctx(c);
   const int flags = (cv ? F_CV : 0) | (cu ? F_CU : 0);
   launch_pair(d, c->st, choose_tpa(c), c->precision == NDG_PREC_MIXED, 0, flags);
@@ -1161,6 +1206,10 @@ int ndg_compute(ndg_ctx *c, int cv, int cu) {
 
 int ndg_integrate2(ndg_ctx *c, int ck) {
   if (!c) return NDG_ERR_ARG;
+  {
+    int e = ensure_params(c);
+    if (e) return e;
+  }
   DevCtx d = devctx(c);
   launch_integrate2(d, c->st, ck);
   CK(c, cudaGetLastError());
@@ -1170,6 +1219,10 @@ int ndg_integrate2(ndg_ctx *c, int ck) {
 
 int ndg_mk_iso_ke(ndg_ctx *c, int s) {
   if (!valid_sys(c, s)) return NDG_ERR_ARG;
+  {
+    int e = ensure_params(c);
+    if (e) return e;
+  }
   SysState S;
   int rc = get_state_dev(c, s, S);
   if (rc) return rc;
@@ -1183,6 +1236,10 @@ int ndg_mk_iso_ke(ndg_ctx *c, int s) {
 
 int ndg_mk_iso_e(ndg_ctx *c, int s) {
   if (!valid_sys(c, s)) return NDG_ERR_ARG;
+  {
+    int e = ensure_params(c);
+    if (e) return e;
+  }
   SysState S;
   int rc = get_state_dev(c, s, S);
   if (rc) return rc;
@@ -1239,9 +1296,6 @@ static int run_impl(ndg_ctx *c, int nsteps, ndg_thermo_cb cb, void *user, int co
     rc = setup_lists(c);
     if (rc) return rc;
     cont = 0;
-  } else if (c->params_dirty) {
-    rc = upload_params(c);
-    if (rc) return rc;
   }
   // controls may have changed between runs
   for (auto &h : c->sys)
@@ -1339,9 +1393,22 @@ int ndg_get_neighbors(ndg_ctx *c, int s, int *pairs, long long cap, long long *n
   return NDG_OK;
 }
 
+int ndg_get_neighbor_count(ndg_ctx *c, int s, long long *entries) {
+  if (!valid_sys(c, s) || !entries || !c->sys[s].lists_valid) return NDG_ERR_ARG;
+  HostSys &h = c->sys[s];
+  const size_t off = (size_t)h.atoms.off * ATOM_ALIGN;
+  std::vector<int> cnt(h.n);
+  CK(c, cudaStreamSynchronize(c->st));
+  CK(c, cudaMemcpy(cnt.data(), c->nnb + off, h.n * sizeof(int), cudaMemcpyDeviceToHost));
+  long long m = 0;
+  for (int x : cnt) m += std::min(x, h.maxnb);
+  *entries = m;
+  return NDG_OK;
+}
+
 int ndg_set_tuning(ndg_ctx *c, int tpa, int graph_steps) {
   if (!c) return NDG_ERR_ARG;
-  if (tpa != 0 && tpa != 1 && tpa != 2 && tpa != 4 && tpa != 8 && tpa != 16 && tpa != 32)
+  if (tpa != 0 && tpa != 1 && tpa != 2 && tpa != 4 && tpa != 8)
     return NDG_ERR_ARG;
   if (graph_steps < 1) return NDG_ERR_ARG;
   if (tpa != c->tpa || graph_steps != c->graph_steps) drop_graphs(c);
@@ -1390,9 +1457,86 @@ long long ndg_system_bytes(int np, int ntypes, int npairs, int ptsize, double de
          (long long)npairs * (ptsize + 1) * 32;
 }
 
+// Autotuner: every mutable device array is snapshotted, each candidate
+// launch shape (threads per atom) runs `steps` real graph steps on the
+// current systems, timed with CUDA events on the library's stream, the state
+// is restored after each trial, and the fastest shape is kept.
 int ndg_autotune(ndg_ctx *c, int steps) {
-  (void)steps;
-  return c ? NDG_OK : NDG_ERR_ARG;
+  if (!c || steps < 1) return NDG_ERR_ARG;
+  cudaSetDevice(c->device);
+  int rc = NDG_OK;
+  if (!lists_ready(c)) {
+    rc = setup_lists(c);
+    if (rc) return rc;
+  }
+  rc = ensure_params(c);
+  if (rc) return rc;
+  const size_t A = (size_t)c->atoms.cap * ATOM_ALIGN, T = 2 * (size_t)c->atoms.cap;
+  struct Buf {
+    void *p;
+    size_t bytes;
+  };
+  const std::vector<Buf> bufs = {
+      {c->pos, A * sizeof(double4)},       {c->pfx, A * sizeof(int4)},
+      {c->vel, 3 * A * sizeof(double)},    {c->acc, 3 * A * sizeof(double)},
+      {c->disp, 3 * A * sizeof(double)},   {c->gid, A * sizeof(int)},
+      {c->nnb, A * sizeof(int)},           {c->atom_cell, A * sizeof(int)},
+      {c->itop, 2 * (size_t)c->atoms.cap * sizeof(double)},
+      {c->tile_nc, T * sizeof(int)},       {c->tile_rows, T * sizeof(int)},
+      {c->tile_cell, T * 256 * sizeof(int)}, {c->tile_coff, T * 257 * sizeof(int)},
+      {c->cell_start, (size_t)c->cells.cap * sizeof(int)},
+      {c->nbr, (size_t)c->nbrs.cap * sizeof(int)},
+      {c->dS, (size_t)c->nsys_cap * sizeof(SysState)}};
+  size_t total = 0;
+  for (auto &b : bufs) total += b.bytes;
+  char *snap = dalloc<char>(total);
+  if (!snap) return NDG_ERR_NOMEM;
+  auto copy = [&](bool save) -> cudaError_t {
+    size_t off = 0;
+    for (auto &b : bufs) {
+      cudaError_t e = save ? cudaMemcpyAsync(snap + off, b.p, b.bytes, cudaMemcpyDeviceToDevice, c->st)
+                           : cudaMemcpyAsync(b.p, snap + off, b.bytes, cudaMemcpyDeviceToDevice, c->st);
+      if (e != cudaSuccess) return e;
+      off += b.bytes;
+    }
+    return cudaStreamSynchronize(c->st);
+  };
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int keep_tpa = c->tpa;
+  int best = 0;
+  float best_ms = 0.f;
+  cudaError_t ce = copy(true);
+  const int cand[4] = {1, 2, 4, 8};
+  for (int k = 0; k < 4 && ce == cudaSuccess && rc == NDG_OK; ++k) {
+    c->tpa = cand[k];
+    drop_graphs(c);
+    CK(c, cudaMemset(c->ring_count, 0, 4 * sizeof(int)));
+    DevCtx d = devctx(c);
+    launch_begin_run(d, c->st, c->nsys_cap, 2 * steps, 1);
+    rc = run_steps(c, steps, nullptr, nullptr);  // warm: capture + first launch
+    if (rc) break;
+    cudaEventRecord(e0, c->st);
+    rc = run_steps(c, steps, nullptr, nullptr);
+    cudaEventRecord(e1, c->st);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (!rc && (best == 0 || ms < best_ms)) {
+      best = cand[k];
+      best_ms = ms;
+    }
+    ce = copy(false);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(snap);
+  CK(c, cudaMemset(c->ring_count, 0, 4 * sizeof(int)));
+  c->tpa = best ? best : keep_tpa;
+  drop_graphs(c);
+  if (ce != cudaSuccess) return cuda_fail(c, ce, "autotune snapshot");
+  return rc;
 }
 
 int ndg_get_stream(ndg_ctx *c, void **stream) {
@@ -1415,7 +1559,7 @@ int ndg_profile_run(ndg_ctx *c, int nsteps) {
   for (auto &e : ev) CK(c, cudaEventCreate(&e));
   for (int k = 0; k < nsteps; ++k) {
     CK(c, cudaEventRecord(ev[4 * k], c->st));
-    launch_rebuild(d, c->st, 0, mixed);
+    launch_rebuild(d, c->st, 1, mixed);
     CK(c, cudaEventRecord(ev[4 * k + 1], c->st));
     launch_integrate1(d, c->st, 0, mixed);
     CK(c, cudaEventRecord(ev[4 * k + 2], c->st));

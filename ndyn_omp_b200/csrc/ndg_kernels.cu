@@ -16,6 +16,8 @@
 //                                           CheckListUpdate decision)
 #include <cstdio>
 
+#include <algorithm>
+
 #include "ndg_kernels.h"
 
 namespace ndg {
@@ -124,6 +126,12 @@ __global__ __launch_bounds__(BLOCK) void k_integrate1(DevCtx c, int standalone, 
       }
     }
   }
+  // this step's rebuild group is done with the rebuild list
+  if (!standalone && blockIdx.x == 0 && threadIdx.x == 0) c.ring_count[3] = 0;
+  // a new step: the system's pair kernel has not run yet (only the block of
+  // the system's first chunk writes; the others read flag bits this leaves)
+  if (!standalone && sys >= 0 && threadIdx.x == 0 && chunk == c.P[sys].atom_off / ATOM_ALIGN)
+    c.S[sys].flags &= ~F_DONE;
   warp_top2(t1, t2);
   __shared__ double s1[BLOCK / 32], s2[BLOCK / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -144,18 +152,64 @@ __global__ __launch_bounds__(BLOCK) void k_integrate1(DevCtx c, int standalone, 
 // End-of-step epilogue for one system, run by the last block of the pair
 // kernel to finish (dynamics, src/nd.f90:164-178 and the next step's head
 // :138-151).
+// The tiles' partials are summed in an order that depends only on the tile
+// index (the first FIN threads, whatever the block size): FP64 values by a
+// fixed tree in `fs` (shared, NR rows of FIN doubles: the 7 energy/virial
+// rows and the kinetic row in FP64, the kinetic row alone when mixed), the
+// mixed path's fixed-point energy and virial exactly.
+constexpr int FIN = 128;
+
+template <bool MIXED>
 __device__ void finalize_system(const DevCtx &c, int sys, int blk0, int nblk, int flags,
-                                int fuse, unsigned long long next_h) {
+                                int fuse, unsigned long long next_h, double (*fs)[FIN]) {
   const SysParam *__restrict__ P = c.P + sys;
   SysState *S = c.S + sys;
-  __shared__ double sm[8 * 32];
+  constexpr int NR = MIXED ? 1 : 8, KR = NR - 1;
+  __shared__ unsigned long long fq[7];
+  const bool ev = flags & (F_CU | F_CV);
+  if (threadIdx.x < 7) fq[threadIdx.x] = 0ull;
+  __syncthreads();
   double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
-    const double *r = c.red + 8 * (size_t)(blk0 + b);
+  if (threadIdx.x < FIN) {
+    long long q[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int b = threadIdx.x; b < nblk; b += FIN) {
+      const double *r = c.red + 8 * (size_t)(blk0 + b);
+      if (ev) {
 #pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] += __ldcg(r + k);
+        for (int k = 0; k < 7; ++k) {
+          if (MIXED) q[k] += __double_as_longlong(__ldcg(r + k));
+          else v[k] += __ldcg(r + k);
+        }
+      }
+      v[7] += __ldcg(r + 7);
+    }
+    if (!MIXED)
+#pragma unroll
+      for (int k = 0; k < 7; ++k) fs[k][threadIdx.x] = v[k];
+    fs[KR][threadIdx.x] = v[7];
+    if (MIXED && ev) {
+#pragma unroll
+      for (int k = 0; k < 7; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) q[k] += __shfl_xor_sync(0xffffffffu, q[k], o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&fq[k], (unsigned long long)q[k]);
+      }
+    }
   }
-  block_sum<8>(v, sm);
+  __syncthreads();
+#pragma unroll 1
+  for (int sft = FIN / 2; sft > 0; sft >>= 1) {
+    if ((int)threadIdx.x < sft)
+      for (int k = 0; k < NR; ++k) fs[k][threadIdx.x] += fs[k][threadIdx.x + sft];
+    __syncthreads();
+  }
+  if (!MIXED)
+#pragma unroll
+    for (int k = 0; k < 7; ++k) v[k] = fs[k][0];
+  v[7] = fs[KR][0];
+  if (MIXED && ev)
+#pragma unroll
+    for (int k = 0; k < 7; ++k) v[k] = (double)(long long)fq[k] * (1.0 / FORCE_FX);
   // two largest displacement measures of this system (integrate1 partials)
   double t1 = 0.0, t2 = 0.0;
   if (fuse) {
@@ -206,7 +260,9 @@ __device__ void finalize_system(const DevCtx &c, int sys, int blk0, int nblk, in
   if (S->steps_left > 0) {
     S->step += 1;
     S->tt += 1;
-    S->flags = step_flags(*P, S->step, S->tt) | F_ACTIVE;
+    // F_DONE keeps the step's second pair kernel (the other energy/virial
+    // variant) from taking this system again under the next step's flags
+    S->flags = step_flags(*P, S->step, S->tt) | F_ACTIVE | F_DONE;
     int rb = 0;
     if (P->renei && S->step % P->renei_freq == 0) {
       rb = list_check(*P, *S, t1, t2);
@@ -227,6 +283,7 @@ __device__ void finalize_system(const DevCtx &c, int sys, int blk0, int nblk, in
       S->ncell = nc;
     }
     S->rebuild = rb;
+    if (rb) c.rb_list[atomicAdd(c.ring_count + 3, 1)] = sys;
     // inside a captured step block: switch on the next step's rebuild node
     if (rb && next_h) cudaGraphSetConditional((cudaGraphConditionalHandle)next_h, 1u);
   } else {
@@ -311,6 +368,7 @@ __global__ void k_begin_run(DevCtx c, int nsys_cap, int nsteps, int cont) {
     }
   }
   S.rebuild = rb;
+  if (rb) c.rb_list[atomicAdd(c.ring_count + 3, 1)] = s;
   S.ticket = 0;
   S.ticket_i = 0;
 }
@@ -403,21 +461,57 @@ __global__ void k_check(DevCtx c, int nsys_cap) {
     S->ncell = nc;
   }
   S->rebuild = rb;
+  if (rb) c.rb_list[atomicAdd(c.ring_count + 3, 1)] = s;
 }
 
 // ---------------------------------------------------------------------------
 // List rebuild: buildCellList + buildVerletList (src/nd.f90:1214-1446).
+//
+// Only the systems on the rebuild list are touched.  The per-system epilogue
+// (or k_check / k_begin_run) appends a system when its CheckListUpdate
+// fires, and the setup paths list every system.  Each rebuild kernel runs a
+// small persistent grid: the listed systems' units (256-atom chunks,
+// 128-atom tiles, groups of cells) form one sequence dealt round-robin to
+// the blocks, so a step in which a few of many replicas rebuild costs a few
+// replicas' worth of work.  k_integrate1 empties the list afterwards.
 
-__device__ __forceinline__ bool rebuilding(const DevCtx &c, int sys, int force_all) {
-  return force_all || c.S[sys].rebuild;
+constexpr int LIST_STAGE = 256;  // listed systems whose ranges a block stages at once
+
+template <class Range, class Body>
+__device__ __forceinline__ void for_listed(const DevCtx &c, Range range, Body body) {
+  // the listed systems' unit ranges, loaded in parallel into shared memory
+  __shared__ int l_sys[LIST_STAGE], l_first[LIST_STAGE], l_cnt[LIST_STAGE];
+  const int n = c.ring_count[3];
+  const int G = gridDim.x, b = blockIdx.x;
+  long long base = 0;
+  for (int k0 = 0; k0 < n; k0 += LIST_STAGE) {
+    const int m = min(LIST_STAGE, n - k0);
+    __syncthreads();  // the previous group's entries are no longer read
+    for (int t = threadIdx.x; t < m; t += blockDim.x) {
+      const int sys = c.rb_list[k0 + t];
+      int first = 0, cnt = 0;
+      range(sys, first, cnt);
+      l_sys[t] = sys;
+      l_first[t] = first;
+      l_cnt[t] = cnt;
+    }
+    __syncthreads();
+    for (int k = 0; k < m; ++k) {
+      const int sys = l_sys[k], first = l_first[k], cnt = l_cnt[k];
+      for (int q = (int)(((long long)b - base % G + G) % G); q < cnt; q += G) body(sys, first + q);
+      base += cnt;
+    }
+  }
+}
+
+__device__ __forceinline__ void chunk_range(const DevCtx &c, int sys, int &first, int &cnt) {
+  first = c.P[sys].atom_off / ATOM_ALIGN;
+  cnt = c.P[sys].npad / ATOM_ALIGN;
 }
 
 // link cell of each atom, src/nd.f90:1237-1248, counted with warp-aggregated
 // atomics (lanes with the same cell elect one atomicAdd)
-__global__ __launch_bounds__(BLOCK) void k_bin(DevCtx c, int force_all) {
-  const int chunk = blockIdx.x;
-  const int sys = c.chunk_sys[chunk];
-  if (sys < 0 || !rebuilding(c, sys, force_all)) return;
+__device__ void bin_chunk(const DevCtx &c, int sys, int chunk) {
   const SysParam *__restrict__ P = c.P + sys;
   SysState *S = c.S + sys;
   const int i = chunk * ATOM_ALIGN + threadIdx.x;
@@ -454,13 +548,17 @@ __global__ __launch_bounds__(BLOCK) void k_bin(DevCtx c, int force_all) {
   if (local < P->n) c.atom_slot[i] = cell >= 0 ? base + rank : 0;
 }
 
-// exclusive scan of the cell counts of one system (one block per system)
-__global__ __launch_bounds__(1024) void k_scan(DevCtx c, int nsys_cap, int force_all) {
-  const int s = blockIdx.x;
-  if (s >= nsys_cap) return;
+__global__ __launch_bounds__(BLOCK) void k_bin(DevCtx c) {
+  for_listed(c, [&](int s, int &f, int &n) { chunk_range(c, s, f, n); },
+             [&](int s, int u) { bin_chunk(c, s, u); });
+}
+
+// exclusive scan of the cell counts of one listed system per block
+__global__ __launch_bounds__(1024) void k_scan(DevCtx c, int counting) {
+  if ((int)blockIdx.x >= c.ring_count[3]) return;
+  const int s = c.rb_list[blockIdx.x];
   const SysParam *__restrict__ P = c.P + s;
   SysState *S = c.S + s;
-  if (P->n == 0 || !(force_all || S->rebuild)) return;
   __shared__ int wsum[32];
   __shared__ int carry;
   if (threadIdx.x == 0) carry = 0;
@@ -501,14 +599,11 @@ __global__ __launch_bounds__(1024) void k_scan(DevCtx c, int nsys_cap, int force
     start[ncell] = carry;
     S->nstencil = make_stencil(S->mcell, P->quirk, S->stencil);
     for (int d = 0; d < 3; ++d) S->box_build[d] = S->box[d];
-    if (!force_all) S->nlist_updates += 1;
+    if (counting) S->nlist_updates += 1;  // NlistUpdates, src/nd.f90:1495
   }
 }
 
-__global__ __launch_bounds__(BLOCK) void k_scatter(DevCtx c, int force_all) {
-  const int chunk = blockIdx.x;
-  const int sys = c.chunk_sys[chunk];
-  if (sys < 0 || !rebuilding(c, sys, force_all)) return;
+__device__ void scatter_chunk(const DevCtx &c, int sys, int chunk) {
   const SysParam *__restrict__ P = c.P + sys;
   const int i = chunk * ATOM_ALIGN + threadIdx.x;
   if (i - P->atom_off >= P->n) return;
@@ -517,15 +612,15 @@ __global__ __launch_bounds__(BLOCK) void k_scatter(DevCtx c, int force_all) {
   c.tmp_key[P->atom_off + dest] = c.gid[i];
 }
 
+__global__ __launch_bounds__(BLOCK) void k_scatter(DevCtx c) {
+  for_listed(c, [&](int s, int &f, int &n) { chunk_range(c, s, f, n); },
+             [&](int s, int u) { scatter_chunk(c, s, u); });
+}
+
 // order the atoms of each cell by original id (one warp per cell) so the
 // layout, and the neighbour order, do not depend on atomic timing
-__global__ __launch_bounds__(BLOCK) void k_order(DevCtx c, int force_all) {
-  const int gc = blockIdx.x * (BLOCK / 32) + (threadIdx.x >> 5);
-  if (gc >= c.ncells) return;
-  const int sys = c.cell_sys[gc];
-  if (sys < 0 || !rebuilding(c, sys, force_all)) return;
+__device__ void order_cell(const DevCtx &c, int sys, int cl) {
   const SysParam *__restrict__ P = c.P + sys;
-  const int cl = gc - P->cell_off;
   if (cl >= c.S[sys].ncell) return;
   const int s0 = c.cell_start[P->cell_off + cl], s1 = c.cell_start[P->cell_off + cl + 1];
   const int *key = c.tmp_key + P->atom_off + s0;
@@ -539,10 +634,17 @@ __global__ __launch_bounds__(BLOCK) void k_order(DevCtx c, int force_all) {
   }
 }
 
-__global__ __launch_bounds__(BLOCK) void k_permute(DevCtx c, int force_all) {
-  const int chunk = blockIdx.x;
-  const int sys = c.chunk_sys[chunk];
-  if (sys < 0 || !rebuilding(c, sys, force_all)) return;
+__global__ __launch_bounds__(BLOCK) void k_order(DevCtx c) {
+  constexpr int W = BLOCK / 32;
+  for_listed(c,
+             [&](int s, int &f, int &n) {
+               f = 0;
+               n = (c.S[s].ncell + W - 1) / W;
+             },
+             [&](int s, int u) { order_cell(c, s, u * W + (threadIdx.x >> 5)); });
+}
+
+__device__ void permute_chunk(const DevCtx &c, int sys, int chunk) {
   const SysParam *__restrict__ P = c.P + sys;
   const int i = chunk * ATOM_ALIGN + threadIdx.x;
   if (i - P->atom_off >= P->n) return;
@@ -560,10 +662,12 @@ __global__ __launch_bounds__(BLOCK) void k_permute(DevCtx c, int force_all) {
   c.s_cell[i] = c.atom_cell[s];
 }
 
-__global__ __launch_bounds__(BLOCK) void k_copyback(DevCtx c, int force_all, int mixed) {
-  const int chunk = blockIdx.x;
-  const int sys = c.chunk_sys[chunk];
-  if (sys < 0 || !rebuilding(c, sys, force_all)) return;
+__global__ __launch_bounds__(BLOCK) void k_permute(DevCtx c) {
+  for_listed(c, [&](int s, int &f, int &n) { chunk_range(c, s, f, n); },
+             [&](int s, int u) { permute_chunk(c, s, u); });
+}
+
+__device__ void copyback_chunk(const DevCtx &c, int sys, int chunk, int mixed) {
   const SysParam *__restrict__ P = c.P + sys;
   if (threadIdx.x == 0) {
     c.itop[2 * chunk] = 0.0;  // dispList was reset: the displacement measure is 0
@@ -581,6 +685,11 @@ __global__ __launch_bounds__(BLOCK) void k_copyback(DevCtx c, int force_all, int
   }
   c.gid[i] = c.s_gid[i];
   c.atom_cell[i] = c.s_cell[i];
+}
+
+__global__ __launch_bounds__(BLOCK) void k_copyback(DevCtx c, int mixed) {
+  for_listed(c, [&](int s, int &f, int &n) { chunk_range(c, s, f, n); },
+             [&](int s, int u) { copyback_chunk(c, s, u, mixed); });
 }
 
 // Neighbour build, one CTA per 128-atom tile (atoms are sorted by link cell,
@@ -611,6 +720,25 @@ __device__ __forceinline__ int stencil_cell(int cl, int st, int M0, int M1, int 
   return nx + ny * M0 + nz * M0 * M1;
 }
 
+// exclusive prefix sum of one int per thread over the whole block, in
+// thread order (wsum: one int per warp of shared scratch)
+__device__ __forceinline__ int block_excl_scan(int v, int *wsum) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  __syncthreads();  // wsum free for reuse
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  int before = 0;
+  for (int w = 0; w < warp; ++w) before += wsum[w];
+  (void)nw;
+  return before + incl - v;
+}
+
 __device__ __forceinline__ int find_cell(const int *ucell, int nu, int cell) {
   int lo = 0, hi = nu - 1;
   while (lo < hi) {
@@ -621,12 +749,10 @@ __device__ __forceinline__ int find_cell(const int *ucell, int nu, int cell) {
   return lo;
 }
 
-__global__ __launch_bounds__(NBT) void k_build(DevCtx c, int force_all) {
+__device__ void build_tile(const DevCtx &c, int sys, int tile) {
   extern __shared__ __align__(16) unsigned char dsm[];
-  const int tile = blockIdx.x;
+  __syncthreads();  // the block's previous tile is done with shared memory
   const int a0 = tile * TILE;
-  const int sys = c.chunk_sys[a0 / ATOM_ALIGN];
-  if (sys < 0 || !rebuilding(c, sys, force_all)) return;
   const SysParam *__restrict__ P = c.P + sys;
   SysState *S = c.S + sys;
   const int local0 = a0 - P->atom_off;
@@ -656,6 +782,7 @@ __global__ __launch_bounds__(NBT) void k_build(DevCtx c, int force_all) {
   __shared__ int vsize[TILE], vstart[TILE], run_t0[TILE + 1];
   __shared__ int nu, bad, nruns, rows_s;
   __shared__ int pm_s[16 * 16];
+  __shared__ int scan_w[NBT / 32];
   __shared__ float rl2f_s[136];
   __shared__ double rl2_s[136];
   const int nt = P->ntypes, npr = P->npairs;
@@ -724,16 +851,17 @@ __global__ __launch_bounds__(NBT) void k_build(DevCtx c, int force_all) {
         }
         __syncthreads();
       }
-    if (threadIdx.x == 0) {
-      int tot = 0;
-      for (int u = 0; u < nu; ++u) {
-        coff[u] = tot;
-        ustart[u] = cst[ucell[u]];
-        tot += cst[ucell[u] + 1] - cst[ucell[u]];
-      }
-      coff[nu] = tot;
-      if (tot > BUILD_CAP) bad = 1;
+    // each staged cell's first atom and length, read in parallel; an
+    // exclusive scan of the lengths gives the candidate offsets
+    int len = 0;
+    if (threadIdx.x < nu) {
+      const int s0 = cst[ucell[threadIdx.x]];
+      ustart[threadIdx.x] = s0;
+      len = cst[ucell[threadIdx.x] + 1] - s0;
     }
+    const int pre = block_excl_scan(len, scan_w);
+    if ((int)threadIdx.x <= nu) coff[threadIdx.x] = pre;  // coff[nu] = all candidates
+    if ((int)threadIdx.x == nu && pre > BUILD_CAP) bad = 1;
   }
   __syncthreads();
   if (bad) {
@@ -771,20 +899,27 @@ __global__ __launch_bounds__(NBT) void k_build(DevCtx c, int force_all) {
   const double ptrmin = P->ptrmin;
   const float ptrlo = (float)ptrmin * (1.f - NB_MARGIN), ptrhi = (float)ptrmin * (1.f + NB_MARGIN);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  // the stencil cells of each run of equal own cells, resolved once per run
-  if (threadIdx.x == 0) {
-    int r = -1, prev = -1;
-    for (int t = 0; t < nown; ++t) {
-      const int cl = c.atom_cell[a0 + t];
-      if (cl != prev) {
-        run_cell[++r] = cl;
-        run_t0[r] = t;
-        prev = cl;
-      }
-      run_of[t] = (short)r;
+  // runs of equal own cells (the atoms are sorted by cell): a run starts
+  // where the cell changes; its index is the number of starts before it
+  {
+    const int t = threadIdx.x;
+    int cl = -1, head = 0;
+    if (t < nown) {
+      cl = c.atom_cell[a0 + t];
+      head = t == 0 || cl != c.atom_cell[a0 + t - 1];
     }
-    nruns = r + 1;
-    run_t0[nruns] = nown;
+    const int pre = block_excl_scan(head, scan_w);
+    if (t < nown) {
+      if (head) {
+        run_cell[pre] = cl;
+        run_t0[pre] = t;
+      }
+      run_of[t] = (short)(pre + head - 1);
+    }
+    if (t == nown) {
+      nruns = pre;
+      run_t0[pre] = nown;
+    }
   }
   __syncthreads();
   for (int idx = threadIdx.x; idx < nruns * ne; idx += NBT) {
@@ -913,10 +1048,11 @@ __global__ __launch_bounds__(NBT) void k_build(DevCtx c, int force_all) {
     return;
   }
   // 4. write the tile's lists row by row (consecutive threads, consecutive atoms)
-  if (threadIdx.x == 0) {
-    int r = 0;
-    for (int t = 0; t < nown; ++t) r = max(r, min(ncnt[t], maxnb));
-    rows_s = r;
+  if (threadIdx.x == 0) rows_s = 0;
+  __syncthreads();
+  if (threadIdx.x < TILE) {
+    const int r = __reduce_max_sync(0xffffffffu, (int)threadIdx.x < nown ? min(ncnt[threadIdx.x], maxnb) : 0);
+    if ((threadIdx.x & 31) == 0) atomicMax(&rows_s, r);
   }
   __syncthreads();
   const int rows = rows_s;
@@ -937,20 +1073,28 @@ __global__ __launch_bounds__(NBT) void k_build(DevCtx c, int force_all) {
   }
 }
 
+__global__ __launch_bounds__(NBT) void k_build(DevCtx c) {
+  for_listed(c,
+             [&](int s, int &f, int &n) {
+               f = c.P[s].atom_off / TILE;
+               n = c.P[s].npad / TILE;
+             },
+             [&](int s, int u) { build_tile(c, s, u); });
+}
+
 // ---------------------------------------------------------------------------
 // Pair loop: compute0 (src/nd.f90:273-333) over the full neighbour list,
 // TPA threads per atom, and with FUSE the integrate2 update
 // (src/nd.f90:1094-1116) of each atom as soon as its force is complete.
 //
 // One CTA (TILE*TPA threads) works on one 128-atom tile at a time; CTAs are
-// persistent and own contiguous tile ranges.  Per tile it stages the
-// positions of the tile's candidate atoms (the cells recorded by k_build)
-// in shared memory, so every neighbour gather of the pair loop is a
-// shared-memory load addressed by the 16-bit tile-local index of the list;
-// the pair matrix, cutoffs and interpolation tables of the system are
-// staged once per system change.
-constexpr int UNR = 4;    // mixed: pairs in flight per thread
-constexpr int UNR_D = 2;  // FP64
+// persistent and own contiguous tile ranges.  The tile's list rows are one
+// contiguous region, bulk-prefetched into L2 one tile ahead; neighbour
+// positions are gathered from global memory (the atoms are sorted by link
+// cell, so a tile's neighbours are a compact set that stays in L1/L2); the
+// pair matrix, cutoffs and interpolation tables of the system are staged in
+// shared memory once per system change.
+constexpr int UNR_D = 2;  // FP64: pairs in flight per thread
 
 struct TabView {
   const int *pm;
@@ -1013,8 +1157,22 @@ __device__ __forceinline__ void global_tables(const DevCtx &c, const SysParam *P
 
 // MODE 0: tables read from global memory; 1: staged in shared memory;
 // 2: staged, and every system has one type and one pair (no per-pair
-// type lookup, cutoff and table scale held in registers)
-template <int TPA, bool MIXED, bool FUSE, int MODE>
+// type lookup, cutoff and table scale held in registers).
+// EV: the kernel of steps that need the potential energy or the virial
+// (calcPot / calcVirial); the kernel of the other steps carries no energy
+// or virial accumulators, so its pair loop holds fewer registers.
+//
+// Mixed precision: each thread sums whole chunks of CHUNK consecutive list
+// entries in FP32, in list order, and adds every chunk's sum to 64-bit
+// fixed-point totals (force, and with EV potential energy and virial).
+// Chunks are dealt to the TPA threads of an atom round-robin, so every
+// launch shape forms the same chunks and the integer totals, which do not
+// depend on the order of addition, are the same bits for any TPA, grid or
+// batch composition.
+constexpr int CHUNK = 8;   // mixed: list entries per FP32 partial sum
+constexpr int GATHER = 4;  // mixed: neighbour gathers in flight per thread
+
+template <int TPA, bool MIXED, bool FUSE, int MODE, bool EV>
 __global__ __launch_bounds__(TILE * TPA) void k_pair(DevCtx c, int host_flags, int ntiles,
                                                      unsigned long long next_h) {
   constexpr bool STAB = MODE >= 1;
@@ -1026,7 +1184,11 @@ __global__ __launch_bounds__(TILE * TPA) void k_pair(DevCtx c, int host_flags, i
   int loaded = -1;
   TabView tv;
   __shared__ int last;
-  __shared__ double sm[8 * 32];
+  constexpr int NR = MIXED ? 1 : 8, KR = NR - 1;  // rows: FP64 energy/virial 0-6, kinetic KR
+  __shared__ double s_red[NR][TILE];          // per-atom values, reduced by atom index
+  __shared__ unsigned long long s_q[7];       // mixed: tile's fixed-point PE and virial
+  if (threadIdx.x < 7) s_q[threadIdx.x] = 0ull;
+  __syncthreads();
 
   for (int tile = t0; tile < t1; ++tile) {
     const int a0 = tile * TILE;
@@ -1035,7 +1197,8 @@ __global__ __launch_bounds__(TILE * TPA) void k_pair(DevCtx c, int host_flags, i
     const SysParam *__restrict__ P = c.P + sys;
     SysState *S = c.S + sys;
     const int flags = FUSE ? S->flags : host_flags;
-    if (FUSE && !(flags & F_ACTIVE)) continue;
+    if (FUSE && (flags & (F_ACTIVE | F_DONE)) != F_ACTIVE) continue;
+    if (FUSE && (((flags & (F_CU | F_CV)) != 0) != EV)) continue;  // the other kernel's tile
     if (!FUSE && P->n == 0) continue;
     if (sys != loaded) {
       if (STAB) {
@@ -1069,10 +1232,11 @@ __global__ __launch_bounds__(TILE * TPA) void k_pair(DevCtx c, int host_flags, i
     const int i = a0 + g;
     const int local = i - P->atom_off;
     const bool valid = local < P->n;
-    const bool cu = flags & F_CU, cv = flags & F_CV;
+    const bool cu = EV && (flags & F_CU), cv = EV && (flags & F_CV);
     const int ntypes = P->ntypes, T = P->ptsize + 1, ptsize = P->ptsize;
 
-    double pe = 0.0, vir[6] = {0, 0, 0, 0, 0, 0};
+    double pe = 0.0, vir[6] = {0, 0, 0, 0, 0, 0};       // FP64 path
+    long long qpe = 0, qv[6] = {0, 0, 0, 0, 0, 0};      // mixed path, fixed point
     double fx = 0.0, fy = 0.0, fz = 0.0;
     long long qx = 0, qy = 0, qz = 0;  // mixed: 64-bit fixed-point force
     int ti = 1;
@@ -1142,74 +1306,68 @@ __global__ __launch_bounds__(TILE * TPA) void k_pair(DevCtx c, int host_flags, i
         const float sb2 = (float)(S->box[2] * (1.0 / FX_ONE));
         const float ptrmin = (float)P->ptrmin;
         const float rc2f1 = tv.rc2f[0], vdr21 = tv.vdr2[0];
-        float ax = 0.f, ay = 0.f, az = 0.f, ape = 0.f;
-        float av0 = 0.f, av1 = 0.f, av2 = 0.f, av3 = 0.f, av4 = 0.f, av5 = 0.f;
-        int grp = 0;
-        int qn[UNR];  // list entries of the next group, loaded one group ahead
+        const int nch = (cnt + CHUNK - 1) / CHUNK;
+        for (int m = la; m < nch; m += TPA) {
+          const int kb = m * CHUNK;
+          int qq[CHUNK];
 #pragma unroll
-        for (int q = 0; q < UNR; ++q) {
-          const int k = la + q * TPA;
-          qn[q] = k < cnt ? __ldg(nb + k * TILE) : -1;
-        }
-        for (int k0 = la; k0 < cnt; k0 += UNR * TPA) {
-          int qq[UNR];
-          int4 pj[UNR];
+          for (int q = 0; q < CHUNK; ++q) qq[q] = kb + q < cnt ? __ldg(nb + (kb + q) * TILE) : -1;
+          float ax = 0.f, ay = 0.f, az = 0.f, ape = 0.f;
+          float av0 = 0.f, av1 = 0.f, av2 = 0.f, av3 = 0.f, av4 = 0.f, av5 = 0.f;
 #pragma unroll
-          for (int q = 0; q < UNR; ++q) qq[q] = qn[q];
+          for (int h = 0; h < CHUNK; h += GATHER) {
+            int4 pj[GATHER];
 #pragma unroll
-          for (int q = 0; q < UNR; ++q) {
-            const int k = k0 + (UNR + q) * TPA;
-            qn[q] = k < cnt ? __ldg(nb + k * TILE) : -1;
-          }
+            for (int q = 0; q < GATHER; ++q) pj[q] = c.pfx[qq[h + q] >= 0 ? qq[h + q] : i];
 #pragma unroll
-          for (int q = 0; q < UNR; ++q) pj[q] = c.pfx[qq[q] >= 0 ? qq[q] : i];
-#pragma unroll
-          for (int q = 0; q < UNR; ++q) {
-            const int pt = ONE ? 1 : pmr[(tw_type(pj[q].w) - 1) * ntypes];
-            const int p1 = ONE ? 0 : (pt > 0 ? pt - 1 : 0);
-            const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj[q].x) * sb0;
-            const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj[q].y) * sb1;
-            const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj[q].z) * sb2;
-            const float d2 = __fmaf_rn(r0, r0, __fmaf_rn(r1, r1, __fmul_rn(r2, r2)));
-            const bool ok = qq[q] >= 0 && pt > 0 && !(d2 > (ONE ? rc2f1 : tv.rc2f[p1]));
-            const float rk = __fmaf_rn(d2 - ptrmin, ONE ? vdr21 : tv.vdr2[p1], 1.0f);
-            int kk = (int)rk;
-            kk = kk < 1 ? 1 : (kk > ptsize ? ptsize : kk);
-            const float w = rk - (float)kk;
-            const int base = p1 * T + kk - 1;
-            const float2 F = tv.tF2[base];
-            const float df = ok ? __fdividef(__fmaf_rn(w, F.y - F.x, F.x), d2) : 0.f;
-            ax = __fmaf_rn(r0, df, ax);
-            ay = __fmaf_rn(r1, df, ay);
-            az = __fmaf_rn(r2, df, az);
-            if (cu && ok) {
-              const float2 Pp = tv.tP2[base];
-              ape += __fmaf_rn(w, Pp.y - Pp.x, Pp.x);
-            }
-            if (cv) {
-              const float r0d = r0 * df, r1d = r1 * df;
-              av0 = __fmaf_rn(r0d, r0, av0);
-              av1 = __fmaf_rn(r1d, r1, av1);
-              av2 = __fmaf_rn(r2 * df, r2, av2);
-              av3 = __fmaf_rn(r0d, r1, av3);
-              av4 = __fmaf_rn(r0d, r2, av4);
-              av5 = __fmaf_rn(r1d, r2, av5);
+            for (int q = 0; q < GATHER; ++q) {
+              const int pt = ONE ? 1 : pmr[(tw_type(pj[q].w) - 1) * ntypes];
+              const int p1 = ONE ? 0 : (pt > 0 ? pt - 1 : 0);
+              // minimum image by 32-bit wrap-around of the fixed-point difference
+              const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj[q].x) * sb0;
+              const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj[q].y) * sb1;
+              const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj[q].z) * sb2;
+              const float d2 = __fmaf_rn(r0, r0, __fmaf_rn(r1, r1, __fmul_rn(r2, r2)));
+              const bool ok = qq[h + q] >= 0 && pt > 0 && !(d2 > (ONE ? rc2f1 : tv.rc2f[p1]));
+              // branch-free: every lane evaluates the pair, excluded ones add 0
+              const float rk = __fmaf_rn(d2 - ptrmin, ONE ? vdr21 : tv.vdr2[p1], 1.0f);
+              int kk = (int)rk;
+              kk = kk < 1 ? 1 : (kk > ptsize ? ptsize : kk);
+              const float w = rk - (float)kk;
+              const int base = p1 * T + kk - 1;
+              const float2 F = tv.tF2[base];
+              const float df = ok ? __fdividef(__fmaf_rn(w, F.y - F.x, F.x), d2) : 0.f;
+              ax = __fmaf_rn(r0, df, ax);
+              ay = __fmaf_rn(r1, df, ay);
+              az = __fmaf_rn(r2, df, az);
+              if (cu && ok) {
+                const float2 Pp = tv.tP2[base];
+                ape += __fmaf_rn(w, Pp.y - Pp.x, Pp.x);
+              }
+              if (cv) {
+                const float r0d = r0 * df, r1d = r1 * df;
+                av0 = __fmaf_rn(r0d, r0, av0);
+                av1 = __fmaf_rn(r1d, r1, av1);
+                av2 = __fmaf_rn(r2 * df, r2, av2);
+                av3 = __fmaf_rn(r0d, r1, av3);
+                av4 = __fmaf_rn(r0d, r2, av4);
+                av5 = __fmaf_rn(r1d, r2, av5);
+              }
             }
           }
-          if (++grp == 2) {
-            // flush the FP32 partial sums (8 pairs) into the 64-bit fixed-point totals
-            qx += __float2ll_rn(ax * (float)FORCE_FX);
-            qy += __float2ll_rn(ay * (float)FORCE_FX);
-            qz += __float2ll_rn(az * (float)FORCE_FX);
-            ax = ay = az = 0.f;
-            grp = 0;
+          qx += __float2ll_rn(ax * (float)FORCE_FX);
+          qy += __float2ll_rn(ay * (float)FORCE_FX);
+          qz += __float2ll_rn(az * (float)FORCE_FX);
+          if (EV) {
+            qpe += __float2ll_rn(ape * (float)FORCE_FX);
+            qv[0] += __float2ll_rn(av0 * (float)FORCE_FX);
+            qv[1] += __float2ll_rn(av1 * (float)FORCE_FX);
+            qv[2] += __float2ll_rn(av2 * (float)FORCE_FX);
+            qv[3] += __float2ll_rn(av3 * (float)FORCE_FX);
+            qv[4] += __float2ll_rn(av4 * (float)FORCE_FX);
+            qv[5] += __float2ll_rn(av5 * (float)FORCE_FX);
           }
         }
-        qx += __float2ll_rn(ax * (float)FORCE_FX);
-        qy += __float2ll_rn(ay * (float)FORCE_FX);
-        qz += __float2ll_rn(az * (float)FORCE_FX);
-        pe = (double)ape;
-        vir[0] = av0; vir[1] = av1; vir[2] = av2; vir[3] = av3; vir[4] = av4; vir[5] = av5;
       }
     }
     if (!MIXED) {
@@ -1219,6 +1377,11 @@ __global__ __launch_bounds__(TILE * TPA) void k_pair(DevCtx c, int host_flags, i
         fx += __shfl_xor_sync(0xffffffffu, fx, o);
         fy += __shfl_xor_sync(0xffffffffu, fy, o);
         fz += __shfl_xor_sync(0xffffffffu, fz, o);
+        if (EV) {
+          pe += __shfl_xor_sync(0xffffffffu, pe, o);
+#pragma unroll
+          for (int k = 0; k < 6; ++k) vir[k] += __shfl_xor_sync(0xffffffffu, vir[k], o);
+        }
       }
     } else {
       // fixed-point sums are exact, so any combination order gives one result
@@ -1256,19 +1419,53 @@ __global__ __launch_bounds__(TILE * TPA) void k_pair(DevCtx c, int host_flags, i
         f[0] = fx; f[1] = fy; f[2] = fz;
       }
     }
-    // per-tile partial sums (only what the step needs), then the last tile
-    // of the system runs the end-of-step epilogue
-    double red[8] = {pe, vir[0], vir[1], vir[2], vir[3], vir[4], vir[5], ke};
-    if (flags & (F_CU | F_CV)) {
-      block_sum<8>(red, sm);
-    } else if (flags & F_CK) {
-      double r1[1] = {ke};  // kinetic energy only (thermostat steps)
-      block_sum<1>(r1, sm);
-      red[7] = r1[0];
+    // per-tile partial sums (only what the step needs), reduced in an order
+    // fixed by the atom index, then the last tile of the system runs the
+    // end-of-step epilogue
+    const bool ck = FUSE && (flags & F_CK);
+    if (EV && MIXED) {
+      // exact integer sums: warp butterfly, then one shared atomic per warp
+      long long v7[7] = {qpe, qv[0], qv[1], qv[2], qv[3], qv[4], qv[5]};
+#pragma unroll
+      for (int k = 0; k < 7; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v7[k] += __shfl_xor_sync(0xffffffffu, v7[k], o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&s_q[k], (unsigned long long)v7[k]);
+      }
+    }
+    if (la == 0) {
+      if (EV && !MIXED) {
+        s_red[0][g] = pe;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) s_red[(1 + k) % NR][g] = vir[k];
+      }
+      if (ck) s_red[KR][g] = ke;
+    }
+    __syncthreads();
+    const int r0 = (EV && !MIXED) ? 0 : KR, r1 = ck ? NR : KR;
+    if (r1 > r0) {
+#pragma unroll 1
+      for (int sft = TILE / 2; sft > 0; sft >>= 1) {
+        if ((int)threadIdx.x < sft)
+          for (int r = r0; r < r1; ++r) s_red[r][threadIdx.x] += s_red[r][threadIdx.x + sft];
+        __syncthreads();
+      }
     }
     if (threadIdx.x == 0) {
+      double *red = c.red + 8 * (size_t)tile;
+      if (EV) {
+        if (MIXED) {
 #pragma unroll
-      for (int k = 0; k < 8; ++k) c.red[8 * (size_t)tile + k] = red[k];
+          for (int k = 0; k < 7; ++k) {
+            red[k] = __longlong_as_double((long long)s_q[k]);  // bits of the integer sum
+            s_q[k] = 0ull;
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < 7; ++k) red[k] = s_red[k % NR][0];
+        }
+      }
+      red[7] = ck ? s_red[KR][0] : 0.0;
       __threadfence();
       const unsigned nblk = (unsigned)(P->npad / TILE);
       const unsigned t = atomicAdd(&S->ticket, 1u);
@@ -1277,11 +1474,23 @@ __global__ __launch_bounds__(TILE * TPA) void k_pair(DevCtx c, int host_flags, i
     __syncthreads();
     if (last) {
       __threadfence();
-      finalize_system(c, sys, P->atom_off / TILE, P->npad / TILE, flags, FUSE, next_h);
+      finalize_system<MIXED>(c, sys, P->atom_off / TILE, P->npad / TILE, flags, FUSE, next_h,
+                             s_red);
       if (threadIdx.x == 0) S->ticket = 0;
     }
     __syncthreads();
   }
+}
+
+static int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n < 1) n = 148;
+  }
+  return n;
 }
 
 // ---------------------------------------------------------------------------
@@ -1290,9 +1499,9 @@ void launch_integrate1(const DevCtx &c, cudaStream_t st, int standalone, int mix
   k_integrate1<<<c.nchunks, BLOCK, 0, st>>>(c, standalone, mixed);
 }
 
-template <int TPA, bool MIXED, bool FUSE, int MODE>
+template <int TPA, bool MIXED, bool FUSE, int MODE, bool EV>
 static void pair_go(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh) {
-  auto kern = k_pair<TPA, MIXED, FUSE, MODE>;
+  auto kern = k_pair<TPA, MIXED, FUSE, MODE, EV>;
   const int smem = MODE ? c.stab_smem : 0;
   static int cfg_smem = -1, occ = 0;
   if (smem != cfg_smem) {
@@ -1301,19 +1510,32 @@ static void pair_go(const DevCtx &c, cudaStream_t st, int hf, unsigned long long
     if (occ < 1) occ = 1;
     cfg_smem = smem;
   }
-  int dev = 0, nsm = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int nsm = sm_count();
   const int ntiles = c.nchunks * (ATOM_ALIGN / TILE);
   const int grid = ntiles < nsm * occ ? ntiles : nsm * occ;
   kern<<<grid, TILE * TPA, smem, st>>>(c, hf, ntiles, nh);
 }
 
+// FUSE (a dynamics step): the kernel without energy/virial takes the
+// systems whose step needs neither, then the EV kernel the others; each
+// skips the other's tiles.  Standalone compute0: the host flags choose.
+template <int TPA, bool MIXED, bool FUSE, int MODE>
+static void pair_ev(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh) {
+  if (FUSE) {
+    pair_go<TPA, MIXED, FUSE, MODE, false>(c, st, hf, nh);
+    pair_go<TPA, MIXED, FUSE, MODE, true>(c, st, hf, nh);
+  } else if (hf & (F_CU | F_CV)) {
+    pair_go<TPA, MIXED, FUSE, MODE, true>(c, st, hf, nh);
+  } else {
+    pair_go<TPA, MIXED, FUSE, MODE, false>(c, st, hf, nh);
+  }
+}
+
 template <int TPA, bool MIXED, bool FUSE>
 static void pair_mode(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh) {
-  if (c.stab_smem <= 0) pair_go<TPA, MIXED, FUSE, 0>(c, st, hf, nh);
-  else if (c.one_pair) pair_go<TPA, MIXED, FUSE, 2>(c, st, hf, nh);
-  else pair_go<TPA, MIXED, FUSE, 1>(c, st, hf, nh);
+  if (c.stab_smem <= 0) pair_ev<TPA, MIXED, FUSE, 0>(c, st, hf, nh);
+  else if (c.one_pair) pair_ev<TPA, MIXED, FUSE, 2>(c, st, hf, nh);
+  else pair_ev<TPA, MIXED, FUSE, 1>(c, st, hf, nh);
 }
 
 template <int TPA>
@@ -1338,7 +1560,6 @@ void launch_pair(const DevCtx &c, cudaStream_t st, int tpa, int mixed, int fuse,
   }
 }
 
-// seed the first rebuild node of a captured step block from device state
 __global__ void k_decide(DevCtx c, unsigned long long h) {
   __shared__ int any;
   if (threadIdx.x == 0) any = 0;
@@ -1357,19 +1578,26 @@ void launch_integrate2(const DevCtx &c, cudaStream_t st, int ck) {
   k_integrate2<<<c.nchunks, BLOCK, 0, st>>>(c, ck);
 }
 
-void launch_rebuild(const DevCtx &c, cudaStream_t st, int force_all, int mixed) {
-  k_bin<<<c.nchunks, BLOCK, 0, st>>>(c, force_all);
-  k_scan<<<c.nsys_cap, 1024, 0, st>>>(c, c.nsys_cap, force_all);
-  k_scatter<<<c.nchunks, BLOCK, 0, st>>>(c, force_all);
-  k_order<<<(c.ncells + BLOCK / 32 - 1) / (BLOCK / 32), BLOCK, 0, st>>>(c, force_all);
-  k_permute<<<c.nchunks, BLOCK, 0, st>>>(c, force_all);
-  k_copyback<<<c.nchunks, BLOCK, 0, st>>>(c, force_all, mixed);
+
+// the rebuild group over the systems on the rebuild list; `counting` adds
+// the rebuild to each system's NlistUpdates (not for the setup builds)
+void launch_rebuild(const DevCtx &c, cudaStream_t st, int counting, int mixed) {
+  const int nsm = sm_count();
+  const int gchunk = std::min(c.nchunks, nsm * 8);
+  const int gcell = std::min((c.ncells + BLOCK / 32 - 1) / (BLOCK / 32), nsm * 8);
+  const int gtile = std::min(c.nchunks * (ATOM_ALIGN / TILE), nsm * 2);
+  k_bin<<<gchunk, BLOCK, 0, st>>>(c);
+  k_scan<<<c.nsys_cap, 1024, 0, st>>>(c, counting);
+  k_scatter<<<gchunk, BLOCK, 0, st>>>(c);
+  k_order<<<gcell, BLOCK, 0, st>>>(c);
+  k_permute<<<gchunk, BLOCK, 0, st>>>(c);
+  k_copyback<<<gchunk, BLOCK, 0, st>>>(c, mixed);
   static int cfg = -1;
   if (c.nb_smem > cfg) {
     cudaFuncSetAttribute(k_build, cudaFuncAttributeMaxDynamicSharedMemorySize, c.nb_smem);
     cfg = c.nb_smem;
   }
-  k_build<<<c.nchunks * (ATOM_ALIGN / TILE), NBT, c.nb_smem, st>>>(c, force_all);
+  k_build<<<gtile, NBT, c.nb_smem, st>>>(c);
 }
 
 void launch_begin_run(const DevCtx &c, cudaStream_t st, int nsys_cap, int nsteps, int cont) {

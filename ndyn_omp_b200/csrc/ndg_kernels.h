@@ -40,7 +40,9 @@ struct DevCtx {
   double *itop;  // integrate1 chunk partials, 2 per chunk
   double *ired;  // integrate2 (standalone) chunk partials
   ThermoRec *ring;
-  int *ring_count;  // [0] records written, [1] error bits of any system
+  int *ring_count;  // [0] records written, [1] error bits of any system,
+                    // [2] largest tile candidate count, [3] systems on rb_list
+  int *rb_list;     // systems whose lists the next rebuild group rebuilds
   int ring_cap;
 };
 
@@ -52,7 +54,7 @@ void launch_pair(const DevCtx &c, cudaStream_t st, int tpa, int mixed, int fuse,
                  unsigned long long next_h = 0);
 void launch_decide(const DevCtx &c, cudaStream_t st, unsigned long long h);
 void launch_integrate2(const DevCtx &c, cudaStream_t st, int ck);
-void launch_rebuild(const DevCtx &c, cudaStream_t st, int force_all, int mixed);
+void launch_rebuild(const DevCtx &c, cudaStream_t st, int counting, int mixed);
 void launch_begin_run(const DevCtx &c, cudaStream_t st, int nsys_cap, int nsteps, int cont);
 void launch_flush(const DevCtx &c, cudaStream_t st, int nsys_cap);
 void launch_check(const DevCtx &c, cudaStream_t st, int nsys_cap);

@@ -277,3 +277,29 @@ def test_large_system_run_follows_oracle(large_liquid):
     for a, b in zip(rg, ro):
         assert a["pe"] == pytest.approx(b["pe"], rel=1e-6)
         assert a["ke"] == pytest.approx(b["ke"], rel=1e-5)
+
+
+def test_autotune_restores_state(specs):
+    """The autotuner's trial steps leave no trace: the state after tuning
+    equals the state before it, and a continued run equals one without
+    tuning (mixed precision: fixed-point sums make every launch shape give
+    the same bits)."""
+    spec = specs["ar_fixed"]
+    res = []
+    for tune in (False, True):
+        with nd.Context(0, "mixed") as ctx:
+            sid = gpu_from_spec(ctx, spec)
+            ctx.run(20)
+            before = ctx.state(sid)
+            nup = ctx.list_updates(sid)
+            if tune:
+                ctx.autotune(10)
+                for a, b in zip(before, ctx.state(sid)):
+                    assert np.array_equal(a, b)
+                assert ctx.list_updates(sid) == nup
+            rows = ctx.run(30, cont=True)
+            res.append((ctx.state(sid), rows, ctx.list_updates(sid)))
+    for a, b in zip(res[0][0], res[1][0]):
+        assert np.array_equal(a, b)
+    assert res[0][1] == res[1][1]
+    assert res[0][2] == res[1][2]
