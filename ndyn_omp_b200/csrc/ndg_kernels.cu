@@ -1171,6 +1171,13 @@ __device__ __forceinline__ void global_tables(const DevCtx &c, const SysParam *P
 // batch composition.
 constexpr int CHUNK = 8;   // mixed: list entries per FP32 partial sum
 constexpr int GATHER = 4;  // mixed: neighbour gathers in flight per thread
+// Mixed precision: a pair whose FP32 squared distance lies within NEAR_CUT
+// (relative) of the squared cutoff takes compute0's FP64 cutoff test, so
+// the two precisions sum the same set of pairs (the tabulated force at the
+// cutoff is not zero).  The FP32 distance from 32-bit fixed-point
+// positions is within 1e-6 relative of the FP64 one for boxes up to
+// 1e3 cutoffs wide, so 1e-5 leaves a tenfold margin.
+constexpr float NEAR_CUT = 1e-5f;
 
 template <int TPA, bool MIXED, bool FUSE, int MODE, bool EV>
 __global__ __launch_bounds__(TILE * TPA) void k_pair(DevCtx c, int host_flags, int ntiles,
@@ -1306,6 +1313,7 @@ __global__ __launch_bounds__(TILE * TPA) void k_pair(DevCtx c, int host_flags, i
         const float sb2 = (float)(S->box[2] * (1.0 / FX_ONE));
         const float ptrmin = (float)P->ptrmin;
         const float rc2f1 = tv.rc2f[0], vdr21 = tv.vdr2[0];
+        const float rlo1 = rc2f1 * (1.f - NEAR_CUT), rhi1 = rc2f1 * (1.f + NEAR_CUT);
         const int nch = (cnt + CHUNK - 1) / CHUNK;
         for (int m = la; m < nch; m += TPA) {
           const int kb = m * CHUNK;
@@ -1314,6 +1322,7 @@ __global__ __launch_bounds__(TILE * TPA) void k_pair(DevCtx c, int host_flags, i
           for (int q = 0; q < CHUNK; ++q) qq[q] = kb + q < cnt ? __ldg(nb + (kb + q) * TILE) : -1;
           float ax = 0.f, ay = 0.f, az = 0.f, ape = 0.f;
           float av0 = 0.f, av1 = 0.f, av2 = 0.f, av3 = 0.f, av4 = 0.f, av5 = 0.f;
+          unsigned nm = 0;  // entries of this chunk within FP32 rounding of the cutoff
 #pragma unroll
           for (int h = 0; h < CHUNK; h += GATHER) {
             int4 pj[GATHER];
@@ -1328,7 +1337,11 @@ __global__ __launch_bounds__(TILE * TPA) void k_pair(DevCtx c, int host_flags, i
               const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj[q].y) * sb1;
               const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj[q].z) * sb2;
               const float d2 = __fmaf_rn(r0, r0, __fmaf_rn(r1, r1, __fmul_rn(r2, r2)));
-              const bool ok = qq[h + q] >= 0 && pt > 0 && !(d2 > (ONE ? rc2f1 : tv.rc2f[p1]));
+              const bool live = qq[h + q] >= 0 && pt > 0;
+              const float rlo = ONE ? rlo1 : tv.rc2f[p1] * (1.f - NEAR_CUT);
+              const float rhi = ONE ? rhi1 : tv.rc2f[p1] * (1.f + NEAR_CUT);
+              const bool ok = live && d2 <= rlo;
+              nm |= (live && d2 > rlo && d2 <= rhi) ? (1u << (h + q)) : 0u;
               // branch-free: every lane evaluates the pair, excluded ones add 0
               const float rk = __fmaf_rn(d2 - ptrmin, ONE ? vdr21 : tv.vdr2[p1], 1.0f);
               int kk = (int)rk;
@@ -1341,6 +1354,57 @@ __global__ __launch_bounds__(TILE * TPA) void k_pair(DevCtx c, int host_flags, i
               ay = __fmaf_rn(r1, df, ay);
               az = __fmaf_rn(r2, df, az);
               if (cu && ok) {
+                const float2 Pp = tv.tP2[base];
+                ape += __fmaf_rn(w, Pp.y - Pp.x, Pp.x);
+              }
+              if (cv) {
+                const float r0d = r0 * df, r1d = r1 * df;
+                av0 = __fmaf_rn(r0d, r0, av0);
+                av1 = __fmaf_rn(r1d, r1, av1);
+                av2 = __fmaf_rn(r2 * df, r2, av2);
+                av3 = __fmaf_rn(r0d, r1, av3);
+                av4 = __fmaf_rn(r0d, r2, av4);
+                av5 = __fmaf_rn(r1d, r2, av5);
+              }
+            }
+          }
+          if (nm) {
+            // the chunk's entries near the cutoff: compute0's FP64 test
+            // decides (src/nd.f90:283-296), then the same FP32 evaluation
+            const double4 pid = c.pos[i];
+            const double b0 = S->box[0], b1 = S->box[1], b2 = S->box[2];
+#pragma unroll 1
+            while (nm) {
+              const int q = __ffs(nm) - 1;
+              nm &= nm - 1;
+              const int j = __ldg(nb + (kb + q) * TILE);
+              const int4 pj = c.pfx[j];
+              const int p1 = ONE ? 0 : pmr[(tw_type(pj.w) - 1) * ntypes] - 1;
+              const double4 pjd = c.pos[j];
+              double s0 = pid.x - pjd.x, s1 = pid.y - pjd.y, s2 = pid.z - pjd.z;
+              s0 = s0 - round(s0);
+              s1 = s1 - round(s1);
+              s2 = s2 - round(s2);
+              const double x0 = b0 * s0, x1 = b1 * s1, x2 = b2 * s2;
+              double dd = x0 * x0;
+              dd = dd + x1 * x1;
+              dd = dd + x2 * x2;
+              if (dd > tv.rc2[p1]) continue;
+              const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * sb0;
+              const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * sb1;
+              const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * sb2;
+              const float d2 = __fmaf_rn(r0, r0, __fmaf_rn(r1, r1, __fmul_rn(r2, r2)));
+              const float rk = __fmaf_rn(d2 - ptrmin, ONE ? vdr21 : tv.vdr2[p1], 1.0f);
+              int kk = (int)rk;
+              kk = kk < 1 ? 1 : (kk > ptsize ? ptsize : kk);
+              const float w = rk - (float)kk;
+              const int base = p1 * T + kk - 1;
+              const float2 F = tv.tF2[base];
+              const float df = __fdividef(__fmaf_rn(w, F.y - F.x, F.x), d2);
+              ax = __fmaf_rn(r0, df, ax);
+              ay = __fmaf_rn(r1, df, ay);
+              az = __fmaf_rn(r2, df, az);
+              if (cu) {
                 const float2 Pp = tv.tP2[base];
                 ape += __fmaf_rn(w, Pp.y - Pp.x, Pp.x);
               }
