@@ -41,7 +41,11 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=50)
-    ap.add_argument("--config", default="c4", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--config", default="c4", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--requests", type=int, default=128, help="c5: requests in the stream")
+    ap.add_argument("--rate", type=float, default=200.0, help="c5: Poisson arrivals per s")
+    ap.add_argument("--steps-scale", type=float, default=0.05,
+                    help="c5: factor on every request's step count")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default=None, choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -53,6 +57,8 @@ def parse():
 
 def workload(cfg, scale_cells=None):
     from ndyn_omp_b200 import workloads as W
+    if cfg == "c5":
+        return [], "mixed"
     if cfg == "c1":
         return [W.cu_crystal(scale_cells or 10, 300.0, seed=1, quirk="ref")], "fp64"
     if cfg == "c2":
@@ -72,6 +78,9 @@ WORKLOAD_TEXT = {
           "skin 1.6, thermostat 600 K + barostat P=0 (Pparm 10)",
     "c4": "512 replicas (half Cu Morse crystals, half LJ Ar liquids), N log-uniform "
           "[500,20000] in whole FCC cells, T uniform [100,1500] K, own thermostats",
+    "c5": "serving: Poisson stream of MD requests (Morse/LJ/Buckingham, N log-uniform "
+          "[1e3,2e5], steps log-uniform [1e3,5e4] x steps-scale, T uniform [100,1500] K, "
+          "NVE/NVT/NPT), 150 GB HBM budget, graph blocks of 100 steps",
 }
 
 
@@ -186,12 +195,19 @@ def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
-def force_error(specs, states, local):
+def force_error(specs, states, local, warm=0):
     """Relative L2 force error of the mixed path against the FP64 path on the
     given configurations: over all atoms of all systems, and the largest
-    per-system value."""
+    per-system value.  warm > 0: the configurations are first thermalised
+    by that many FP64 steps (a perfect lattice has zero net forces, against
+    which no relative error is meaningful)."""
     import ndyn_omp_b200 as nd
     from ndyn_omp_b200 import workloads as W
+    if warm:
+        with nd.Context(local, "fp64") as cx:
+            ids = [W.add_to_context(cx, sp) for sp in specs]
+            cx.run(warm)
+            states = [cx.state(i) for i in ids]
     fs = {}
     for p in ("fp64", "mixed"):
         with nd.Context(local, p) as cx:
@@ -296,10 +312,15 @@ def run_reference(args, ws, rank):
         n = int(min(64, max(6, round((want_atoms / 8) ** (1 / 3)))))
         sample = workload("c3", (n, n, n))[0][0]
         sample_txt = f"{len(sample['typ'])} atoms ({n}^3 rocksalt cells)"
-    else:
+    elif args.config == "c4":
         # c4: replicas run one after another (the plain path in sequence)
         sample = specs[1]
         sample_txt = f"replica 1 of 512 ({len(sample['typ'])} atoms)"
+    else:
+        # c5: the stream's first request system
+        from ndyn_omp_b200 import workloads as W
+        sample = W.build_request(W.serving_requests(1, args.rate, seed=5)[0])
+        sample_txt = f"request 0 of the stream ({len(sample['typ'])} atoms)"
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from helpers import oracle_from_spec
     o = oracle_from_spec(sample, threads=threads)
@@ -327,9 +348,101 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_serving(args, ws, rank, local):
+    """c5: the request loop.  Requests arrive on a seeded Poisson clock (wall
+    time); between blocks every arrived request is submitted, and each
+    server step admits what fits the HBM budget and advances every resident
+    run by one block.  Latency = completion - arrival, wall clock; value =
+    all atom-steps / (last completion - first arrival)."""
+    import torch
+
+    import ndyn_omp_b200 as nd
+    from ndyn_omp_b200 import workloads as W
+    torch.cuda.set_device(local)
+    reqs = W.serving_requests(args.requests, args.rate, seed=5 + rank)
+    specs = []
+    for r in reqs:
+        sp = W.build_request(r)
+        sp["steps"] = max(1, int(round(sp["steps"] * args.steps_scale)))
+        specs.append(sp)
+    total = float(sum(len(sp["typ"]) * sp["steps"] for sp in specs))
+    # the stated force error: mixed vs FP64 on the first requests' systems
+    probe = [sp for sp in specs[:8] if len(sp["typ"]) <= 60000][:4] or specs[:1]
+    ea, em = force_error(probe, [None] * len(probe), local, warm=100)
+    srv = nd.Server(local, "mixed", hbm_budget=150e9, block_steps=100)
+    arrival, lat, which, failed = {}, {}, {}, []
+    barrier(ws)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        k = 0
+        while len(lat) < len(specs):
+            now = time.perf_counter() - t0
+            while k < len(specs) and reqs[k]["arrival"] <= now:
+                t = W.submit_to_server(srv, specs[k])
+                arrival[t] = reqs[k]["arrival"]
+                which[t] = k
+                k += 1
+            st = srv.stats()
+            if st["resident"] + st["queued"] == 0:
+                if k < len(specs):
+                    time.sleep(max(0.0, min(0.01, reqs[k]["arrival"] - now)))
+                continue
+            srv.step()
+            tn = time.perf_counter() - t0
+            for t in srv.poll():
+                lat[t] = tn - arrival[t]
+                if srv.status(t) == 2:
+                    srv.result(t)
+                else:
+                    r = reqs[which[t]]
+                    failed.append({"request": which[t], "status": srv.status(t),
+                                   "pot": r["pot"], "atoms": len(specs[which[t]]["typ"]),
+                                   "ensemble": r["ensemble"], "T": round(r["T"], 1),
+                                   "steps": specs[which[t]]["steps"]})
+        t_end = max(arrival[t] + lat[t] for t in lat)
+    makespan = allmax(t_end - reqs[0]["arrival"], ws)
+    st = srv.stats()
+    srv.close()
+    lv = np.array(sorted(lat.values())) * 1e3
+    # each rank serves its own stream: aggregate work over the slowest rank
+    value_all = total * ws / makespan
+    line = {
+        "metric": "atom-steps/s", "value": value_all, "unit": "atom-steps/s", "n_gpus": ws,
+        "steps": len(specs), "warmup": 0, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 pair math + i64 fixed-point sums + f64 integrator",
+        "data": "synthetic (seeded Poisson request stream, seeded lattices and velocities)",
+        "config": {"workload": WORKLOAD_TEXT["c5"], "requests": len(specs),
+                   "rate_per_s": args.rate, "steps_scale": args.steps_scale,
+                   "atom_steps": total, "hbm_budget_gb": 150, "block_steps": 100,
+                   "parallelism": f"replicas x{ws} (one server per GPU)" if ws > 1 else "1 GPU"},
+        "latency_ms": {"p50": float(np.percentile(lv, 50)), "p99": float(np.percentile(lv, 99)),
+                       "max": float(lv[-1])},
+        "makespan_s": makespan, "failed": st["failed"], "failed_requests": failed[:20],
+        "server": {k: st[k] for k in ("t_admit", "t_setup", "t_block", "t_retire",
+                                      "graph_captures", "blocks")},
+        "force_rel_err_vs_fp64": ea, "force_rel_err_max_system": em,
+        "clocks": clk.summary(),
+        "e2e": {"value": value_all, "unit": "atom-steps/s",
+                "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                "what": "wall clock from the first arrival to the last completion: submit "
+                        "(host copies), admission, list builds, blocks, result copies"},
+        "roofline": None, "cpu_baseline": None, "gpu_launches": None,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_init()
+    if args.config == "c5" and args.impl != "reference":
+        run_serving(args, ws, rank, local)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.impl == "reference":
         run_reference(args, ws, rank)
         if ws > 1:

@@ -256,6 +256,69 @@ int ndg_profile_run(ndg_ctx *ctx, int nsteps);
 int ndg_get_kernel_times(ndg_ctx *ctx, double *integrate_ms, double *pair_ms,
                          double *rebuild_ms, int *launches);
 
+/* ---- serving loop: continuous batching of MD runs ----------------------
+ * No counterpart in the reference (one run per process).  A server owns a
+ * context and keeps every admitted run's state on the device until the run
+ * completes.  Requests queue on submit; each ndg_server_step admits queued
+ * requests in submission order while their estimated device bytes
+ * (ndg_system_bytes) fit the HBM budget (a request that does not fit waits,
+ * later smaller ones may pass it), builds the new runs' lists, and advances
+ * every resident run by one block of block_steps steps in one graph launch.
+ * A run's trajectory does not depend on the runs it shares the device with:
+ * in mixed precision it is the same bits as the run alone.  Not thread-safe
+ * per server. */
+typedef struct ndg_server ndg_server;
+
+typedef struct ndg_request {
+  int np, ntypes, npairs, ptsize; /* as ndg_add_system */
+  double ptrmin;
+  const double *mass;
+  const int *pairmat;
+  const double *rcpair, *ppair, *fpair;
+  const int *typ;
+  const double *pos, *vel; /* vel may be NULL (zero) */
+  const double *box;
+  ndg_control control; /* dt, skin, ensembles, OutSteps, quirk, ... */
+  int nsteps;          /* steps of the run (one Run directive) */
+} ndg_request;
+
+typedef struct ndg_server_stats {
+  int queued, resident, completed, failed;
+  long long bytes_in_use, budget;
+  double atom_steps; /* atom-steps advanced so far */
+  /* host wall seconds spent so far in admission (adding systems), run
+   * prologues (list builds), blocks (graph launch to completion, including
+   * graph captures) and retiring runs (state copies) */
+  double t_admit, t_setup, t_block, t_retire;
+  int graph_captures; /* step-block graphs captured by the context */
+  int blocks;         /* blocks run */
+} ndg_server_stats;
+
+int ndg_server_create(ndg_server **srv, int device, int precision, long long hbm_budget_bytes,
+                      int block_steps);
+int ndg_server_destroy(ndg_server *srv);
+/* copy the request's arrays and queue it; *ticket identifies it */
+int ndg_server_submit(ndg_server *srv, const ndg_request *req, long long *ticket);
+/* admit what fits, then one block for every resident run; *completed =
+ * runs that finished in this call (their results wait for ndg_server_result) */
+int ndg_server_step(ndg_server *srv, int *completed);
+/* tickets finished (or failed) since the last poll, up to cap */
+int ndg_server_poll(ndg_server *srv, long long *tickets, int cap, int *n);
+/* status of a ticket: 0 queued, 1 resident, 2 done, a negative NDG_ERR_*
+ * if the run failed */
+int ndg_server_status(ndg_server *srv, long long ticket, int *status);
+/* copy a finished run's final state (caller's atom order) and up to cap
+ * write_thermo rows, then forget the request */
+int ndg_server_result(ndg_server *srv, long long ticket, double *pos, double *vel, double *acc,
+                      double *box, ndg_thermo *rows, int cap, int *nrows);
+int ndg_server_stats_get(ndg_server *srv, ndg_server_stats *st);
+/* the server's context (stream, tuning, kernel timings) */
+int ndg_server_context(ndg_server *srv, ndg_ctx **ctx);
+/* The admission rule alone (host only): walk the queue in order and admit
+ * each request whose bytes fit what remains of the budget; admit[k] = 1 for
+ * admitted ones.  Returns the number admitted. */
+int ndg_admit_plan(const long long *bytes, int n, long long budget, long long in_use, int *admit);
+
 #ifdef __cplusplus
 }
 #endif

@@ -54,6 +54,16 @@ SIGNATURES = [
     ("ndg_get_kernel_times", i, [vp, vp, vp, vp, vp]),
     ("ndg_get_stream", i, [vp, vp]),
     ("ndg_profile_run", i, [vp, i]),
+    ("ndg_server_create", i, [vp, i, i, ll, i]),
+    ("ndg_server_destroy", i, [vp]),
+    ("ndg_server_submit", i, [vp, vp, vp]),
+    ("ndg_server_step", i, [vp, vp]),
+    ("ndg_server_poll", i, [vp, vp, i, vp]),
+    ("ndg_server_status", i, [vp, ll, vp]),
+    ("ndg_server_result", i, [vp, ll, vp, vp, vp, vp, vp, i, vp]),
+    ("ndg_server_stats_get", i, [vp, vp]),
+    ("ndg_server_context", i, [vp, vp]),
+    ("ndg_admit_plan", i, [vp, i, ll, ll, vp]),
     ("ndg_compute0_static", i, [i, i, i, i, d, vp, vp, d, i, vp, vp, vp, vp, vp, vp, vp, vp,
                                 vp]),
 ]

@@ -14,6 +14,9 @@ with the reference's names and flag arguments:
     ctx.mk_iso_ke/e/p(sys)     mkIsoKE/mkIsoE/mkIsoP src/nd.f90:1122-1213
     ctx.run(nsteps)            the dynamics loop     src/nd.f90:137-180
 
+`Server` is the serving loop (continuous batching of independent runs, no
+counterpart in the reference): submit(), step(), poll(), result().
+
 Errors the reference reports with STOP raise NdgError with the library's
 status code.  Everything runs in the CUDA library; there is no CPU path.
 """
@@ -319,3 +322,150 @@ class Context:
 
     def set_precision(self, precision):
         _ok(self.L.ndg_set_precision(self._c, PREC[precision]), "set_precision")
+
+
+# ---------------------------------------------------------------------------
+class Request(ctypes.Structure):
+    _fields_ = [("np", ctypes.c_int), ("ntypes", ctypes.c_int), ("npairs", ctypes.c_int),
+                ("ptsize", ctypes.c_int), ("ptrmin", ctypes.c_double),
+                ("mass", ctypes.c_void_p), ("pairmat", ctypes.c_void_p),
+                ("rcpair", ctypes.c_void_p), ("ppair", ctypes.c_void_p),
+                ("fpair", ctypes.c_void_p), ("typ", ctypes.c_void_p), ("pos", ctypes.c_void_p),
+                ("vel", ctypes.c_void_p), ("box", ctypes.c_void_p), ("control", Control),
+                ("nsteps", ctypes.c_int)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("queued", ctypes.c_int), ("resident", ctypes.c_int),
+                ("completed", ctypes.c_int), ("failed", ctypes.c_int),
+                ("bytes_in_use", ctypes.c_longlong), ("budget", ctypes.c_longlong),
+                ("atom_steps", ctypes.c_double), ("t_admit", ctypes.c_double),
+                ("t_setup", ctypes.c_double), ("t_block", ctypes.c_double),
+                ("t_retire", ctypes.c_double), ("graph_captures", ctypes.c_int),
+                ("blocks", ctypes.c_int)]
+
+
+def make_control(**kw):
+    """An ndg_control with the reference's defaults, then the given fields."""
+    c = Control()
+    L.lib().ndg_default_control(ctypes.byref(c))
+    for k, v in kw.items():
+        if k == "quirk" and isinstance(v, str):
+            v = QUIRK[v]
+        if k in ("p_target", "box_vel"):
+            for q in range(3):
+                getattr(c, k)[q] = v[q]
+        else:
+            setattr(c, k, v)
+    return c
+
+
+def admit_plan(nbytes, budget, in_use=0):
+    """The server's admission rule on its own (host only): which queued
+    requests, in order, fit what is left of the budget."""
+    b = np.ascontiguousarray(nbytes, np.int64)
+    out = np.zeros(len(b), np.int32)
+    k = L.lib().ndg_admit_plan(_p(b), len(b), int(budget), int(in_use), _p(out))
+    if k < 0:
+        raise NdgError(k, "admit_plan")
+    return out.astype(bool)
+
+
+class Server:
+    """Continuous batching of independent MD runs on one GPU.
+
+    submit() queues a run (its arrays are copied); each step() admits queued
+    runs that fit the HBM budget, builds their lists, and advances every
+    resident run by one block of block_steps steps; finished runs are
+    retired and their final state waits for result()."""
+
+    def __init__(self, device=0, precision="mixed", hbm_budget=150e9, block_steps=100):
+        self.L = L.lib()
+        self._s = ctypes.c_void_p()
+        _ok(self.L.ndg_server_create(ctypes.byref(self._s), int(device), PREC[precision],
+                                     int(hbm_budget), int(block_steps)), "server_create")
+        self.natoms = {}
+
+    def close(self):
+        if self._s:
+            self.L.ndg_server_destroy(self._s)
+            self._s = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def submit(self, masses, pairs, typ, pos, box, nsteps, vel=None, ptsize=1000, ptrmin=0.25,
+               **control):
+        masses = np.ascontiguousarray(masses, np.float64)
+        nt = len(masses)
+        pp, fp, _, _ = build_pair_tables(pairs, ptsize, ptrmin)
+        pm = pair_matrix(pairs, nt)
+        rcp = np.array([p[4][0] for p in pairs], np.float64)
+        typ = np.ascontiguousarray(typ, np.int32)
+        pos = np.ascontiguousarray(pos, np.float64).reshape(-1)
+        vel = None if vel is None else np.ascontiguousarray(vel, np.float64).reshape(-1)
+        box = np.ascontiguousarray(box, np.float64)
+        r = Request(np=len(typ), ntypes=nt, npairs=len(pairs), ptsize=int(ptsize),
+                    ptrmin=float(ptrmin), mass=_p(masses), pairmat=_p(pm), rcpair=_p(rcp),
+                    ppair=_p(pp), fpair=_p(fp), typ=_p(typ), pos=_p(pos), vel=_p(vel),
+                    box=_p(box), control=make_control(**control), nsteps=int(nsteps))
+        t = ctypes.c_longlong()
+        _ok(self.L.ndg_server_submit(self._s, ctypes.byref(r), ctypes.byref(t)), "server_submit")
+        # write_thermo rows: every OutSteps-th step and the run's first
+        self.natoms[t.value] = (len(typ), int(nsteps) // max(r.control.out_steps, 1) + 2)
+        return t.value
+
+    def step(self):
+        """admit what fits, one block for every resident run; returns the
+        number of runs that finished in this call"""
+        n = ctypes.c_int()
+        _ok(self.L.ndg_server_step(self._s, ctypes.byref(n)), "server_step")
+        return n.value
+
+    def poll(self):
+        out = []
+        buf = (ctypes.c_longlong * 256)()
+        while True:
+            n = ctypes.c_int()
+            _ok(self.L.ndg_server_poll(self._s, buf, 256, ctypes.byref(n)), "server_poll")
+            out.extend(buf[k] for k in range(n.value))
+            if n.value < 256:
+                return out
+
+    def status(self, ticket):
+        st = ctypes.c_int()
+        _ok(self.L.ndg_server_status(self._s, int(ticket), ctypes.byref(st)), "server_status")
+        return st.value
+
+    def result(self, ticket):
+        """(pos, vel, acc, box, thermo rows) of a finished run"""
+        n, cap = self.natoms.pop(ticket)
+        pos, vel, acc, box = np.zeros(3 * n), np.zeros(3 * n), np.zeros(3 * n), np.zeros(3)
+        rows = (Thermo * cap)()
+        nrows = ctypes.c_int()
+        _ok(self.L.ndg_server_result(self._s, int(ticket), _p(pos), _p(vel), _p(acc), _p(box),
+                                     rows, cap, ctypes.byref(nrows)), "server_result")
+        out = [rows[k].as_dict() for k in range(min(cap, nrows.value))]
+        return pos.reshape(n, 3), vel.reshape(n, 3), acc.reshape(n, 3), box, out
+
+    def stats(self):
+        st = ServerStats()
+        _ok(self.L.ndg_server_stats_get(self._s, ctypes.byref(st)), "server_stats")
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    @property
+    def stream_ptr(self):
+        c = ctypes.c_void_p()
+        _ok(self.L.ndg_server_context(self._s, ctypes.byref(c)), "server_context")
+        p = ctypes.c_void_p()
+        _ok(self.L.ndg_get_stream(c, ctypes.byref(p)), "get_stream")
+        return p.value

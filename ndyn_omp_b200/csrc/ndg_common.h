@@ -94,8 +94,13 @@ struct SysState {
   int err;
   unsigned int ticket;   // last-block election of the pair kernel
   unsigned int ticket_i; // last-block election of integrate2 (standalone)
-  int pad_[2];
+  int run_left;          // steps of the current run not yet given to a block
+  int start;             // how the next block begins: START_* (0 = continue)
 };
+
+// SysState::start: a block continues the run, or starts a new one (tt = 1)
+// with its lists just built (no list check on its first step) or without
+enum : int { START_CONTINUE = 0, START_BUILT = 1, START_NEW = 2 };
 
 // Device copy of one write_thermo record; layout equals ndg_thermo.
 struct ThermoRec {

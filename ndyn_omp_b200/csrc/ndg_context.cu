@@ -19,6 +19,7 @@
 
 #include "../../include/ndyn_gpu.h"
 #include "ndg_common.h"
+#include "ndg_internal.h"
 #include "ndg_kernels.h"
 
 using namespace ndg;
@@ -112,8 +113,6 @@ struct ndg_ctx {
   int *nbr = nullptr;
   int *tile_rows = nullptr;
   int *rb_list = nullptr;  // systems listed for a list rebuild
-  int *tile_nc = nullptr, *tile_cell = nullptr, *tile_coff = nullptr;
-  int cand_cap = 6144;  // candidates a tile stages in the pair kernel
   double *red = nullptr, *itop = nullptr, *ired = nullptr;
   int *pairmat = nullptr;
   double *mass = nullptr, *rc2 = nullptr, *rlist2 = nullptr;
@@ -130,8 +129,8 @@ struct ndg_ctx {
   int stab_smem = 0;  // staged-table bytes of the pair kernel (0: tables from global)
   int nb_smem = 0;  // neighbour-build dynamic smem
   int nb_maxnb = 8, nb_vcap = 8192;
-  int one_pair = 0;  // every system has one type and one pair (pair-kernel variant)
   std::map<int, cudaGraphExec_t> graphs;
+  int captures = 0;  // graphs captured (a changed arena or layout drops them)
   // per-kernel timing of the last profiled block
   double t_int = 0, t_pair = 0, t_reb = 0;
   int t_launches = 0;
@@ -183,11 +182,6 @@ DevCtx devctx(ndg_ctx *c) {
   d.gid = c->gid;
   d.nbr = c->nbr;
   d.tile_rows = c->tile_rows;
-  d.tile_nc = c->tile_nc;
-  d.tile_cell = c->tile_cell;
-  d.tile_coff = c->tile_coff;
-  d.cand_cap = c->cand_cap;
-  d.one_pair = c->one_pair;
   d.nb_maxnb = c->nb_maxnb;
   d.nb_vcap = c->nb_vcap;
   d.nnb = c->nnb;
@@ -269,11 +263,8 @@ int grow_atoms(ndg_ctx *c, long long new_chunks) {
   rc |= grow(c, c->chunk_sys, (size_t)c->atoms.cap, (size_t)new_chunks);
   {
     const size_t t_old = 2 * (size_t)c->atoms.cap, t_new = 2 * (size_t)new_chunks;
-    rc |= grow(c, c->tile_nc, t_old, t_new);
     rc |= grow(c, c->tile_rows, t_old, t_new);
     if (!rc) cudaMemset(c->tile_rows + t_old, 0, (t_new - t_old) * sizeof(int));
-    rc |= grow(c, c->tile_cell, t_old * 256, t_new * 256);
-    rc |= grow(c, c->tile_coff, t_old * 257, t_new * 257);
   }
   if (rc) return NDG_ERR_NOMEM;
   c->chunk_sys_h.resize(new_chunks, -1);
@@ -413,20 +404,12 @@ int upload_params(ndg_ctx *c) {
     c->stab_smem = stab;
     drop_graphs(c);
   }
-  // the single-pair pair-kernel variant applies only while every system has
-  // one type and one pair potential
-  int one = 1;
-  for (auto &h : c->sys)
-    if (h.alive && (h.ntypes != 1 || h.npairs != 1)) one = 0;
-  if (one != c->one_pair) {
-    c->one_pair = one;
-    drop_graphs(c);
-  }
   // neighbour build: 3072 staged candidates (16 B each), the 16-bit lists
   // of the tile's 128 atoms, and the runs' flat candidate lists
   int mx = 8;
   for (auto &h : c->sys)
     if (h.alive) mx = std::max(mx, h.maxnb);
+  mx = std::min(mx, 512);  // systems with longer lists build directly
   const int vcap = 8192;
   const int nbs = 3072 * 16 + 128 * mx * 2 + vcap * 2;
   if (nbs != c->nb_smem || mx != c->nb_maxnb) {
@@ -541,21 +524,28 @@ int upload_atoms(ndg_ctx *c, int s, const int *typ, const double *pos, const dou
   return NDG_OK;
 }
 
-// put every live system on the rebuild list (the setup paths rebuild all)
-int list_all_systems(ndg_ctx *c) {
+std::vector<int> live_systems(ndg_ctx *c) {
   std::vector<int> ids;
   for (size_t s = 0; s < c->sys.size(); ++s)
     if (c->sys[s].alive) ids.push_back((int)s);
+  return ids;
+}
+
+// put the given systems on the rebuild list
+int list_systems(ndg_ctx *c, const std::vector<int> &ids) {
   const int n = (int)ids.size();
   if (n) CK(c, cudaMemcpy(c->rb_list, ids.data(), n * sizeof(int), cudaMemcpyHostToDevice));
   CK(c, cudaMemcpy(c->ring_count + 3, &n, sizeof(int), cudaMemcpyHostToDevice));
   return NDG_OK;
 }
 
-// dynamics prologue for every system, src/nd.f90:73-108: skin default,
-// MCELL, neighbour capacity; then one rebuild of all lists.
-int setup_lists(ndg_ctx *c) {
-  for (size_t s = 0; s < c->sys.size(); ++s) {
+int list_all_systems(ndg_ctx *c) { return list_systems(c, live_systems(c)); }
+
+// dynamics prologue, src/nd.f90:73-108, for the given systems: skin default,
+// MCELL, neighbour capacity; then one rebuild of their lists (the other
+// systems are left as they are)
+int setup_lists(ndg_ctx *c, const std::vector<int> &which) {
+  for (int s : which) {
     HostSys &h = c->sys[s];
     if (!h.alive) continue;
     if (h.ctl.skin < 0) h.ctl.skin = 0.2 * h.rcut;  // persists, as in the reference
@@ -585,9 +575,9 @@ int setup_lists(ndg_ctx *c) {
     int maxnb = (int)(est * 1.2) + 16;
     if (h.ctl.neimax > 0) maxnb = std::max(maxnb, 2 * h.ctl.neimax);
     maxnb = std::min((maxnb + 7) / 8 * 8, std::max(h.n - 1, 8) * (h.ctl.quirk == 0 ? 2 : 1) + 8);
-    // the build keeps a tile's 128 lists in shared memory: 512 entries each
-    // at most (a denser neighbourhood reports NDG_ERR_NEIMAX)
-    maxnb = std::min(maxnb, 512);
+    // list capacity: a tile's lists up to 512 entries each are assembled in
+    // shared memory, longer ones by the build's direct path
+    maxnb = std::min(maxnb, 4096);
     const long long npad = (long long)h.atoms.len * ATOM_ALIGN;
     if (maxnb > h.maxnb) {
       if (h.nbr.off >= 0) c->nbrs.give(h.nbr.off);
@@ -629,7 +619,7 @@ int setup_lists(ndg_ctx *c) {
   int rc = upload_params(c);
   if (rc) return rc;
   CK(c, cudaMemset(c->ring_count, 0, 4 * sizeof(int)));
-  rc = list_all_systems(c);
+  rc = list_systems(c, which);
   if (rc) return rc;
   DevCtx d = devctx(c);
   launch_rebuild(d, c->st, 0, c->precision == NDG_PREC_MIXED);
@@ -643,10 +633,12 @@ int setup_lists(ndg_ctx *c) {
     if (words[1] & E_OUT_OF_BOX) return NDG_ERR_OUT_OF_BOX;
     return NDG_ERR_CELLS;
   }
-  for (auto &h : c->sys)
-    if (h.alive) h.lists_valid = true;
+  for (int s : which)
+    if (c->sys[s].alive) c->sys[s].lists_valid = true;
   return NDG_OK;
 }
+
+int setup_lists(ndg_ctx *c) { return setup_lists(c, live_systems(c)); }
 
 int choose_tpa(ndg_ctx *c) {
   if (c->tpa > 0) return c->tpa;
@@ -659,9 +651,11 @@ int choose_tpa(ndg_ctx *c) {
     }
   if (!atoms) return 1;
   nb /= atoms;
-  // enough threads to fill the 148 SMs, and about 16+ neighbours per thread
+  // more threads per atom only while there are too few atoms to fill the
+  // 148 SMs: with enough atoms one thread per atom gathers best
+  (void)nb;
   int t = 1;
-  while (t < 8 && ((double)atoms * t < 148.0 * 1024.0 || nb / t > 48.0)) t *= 2;
+  while (t < 8 && (double)atoms * t < 148.0 * 1024.0) t *= 2;
   return t;
 }
 
@@ -749,10 +743,17 @@ int capture_block(ndg_ctx *c, int g, cudaGraphExec_t *out) {
   return NDG_OK;
 }
 
-int run_steps(ndg_ctx *c, int nsteps, ndg_thermo_cb cb, void *user) {
+// Run nsteps as blocks of up to graph_steps: each block's head gives every
+// armed system its share of the block (k_begin_block), then the block runs
+// as one captured graph (or as eager launches when graph_steps is 1).
+int run_blocks(ndg_ctx *c, int nsteps, ndg_thermo_cb cb, void *user) {
   int left = nsteps;
   while (left > 0) {
     const int g = std::min(left, std::max(c->graph_steps, 1));
+    {
+      DevCtx d = devctx(c);
+      launch_begin_block(d, c->st, c->nsys_cap, g);
+    }
     cudaGraphExec_t exec = nullptr;
     auto it = c->graphs.find(g);
     if (it != c->graphs.end()) {
@@ -761,6 +762,7 @@ int run_steps(ndg_ctx *c, int nsteps, ndg_thermo_cb cb, void *user) {
       int rc = capture_block(c, g, &exec);
       if (rc) return rc;
       c->graphs[g] = exec;
+      c->captures += 1;
     }
     if (exec) {
       CK(c, cudaGraphLaunch(exec, c->st));
@@ -778,9 +780,9 @@ int run_steps(ndg_ctx *c, int nsteps, ndg_thermo_cb cb, void *user) {
   return NDG_OK;
 }
 
-int flush_pending(ndg_ctx *c) {
+int flush_pending(ndg_ctx *c, int sys = -1) {
   DevCtx d = devctx(c);
-  launch_flush(d, c->st, c->nsys_cap);
+  launch_flush(d, c->st, c->nsys_cap, sys);
   CK(c, cudaGetLastError());
   CK(c, cudaStreamSynchronize(c->st));
   return NDG_OK;
@@ -797,13 +799,61 @@ ndg_ctx::~ndg_ctx() {
   drop_graphs(this);
   void *ptrs[] = {dP, dS, chunk_sys, cell_sys, pos, s_pos, pfx, vel, acc, disp, force, s_vel,
                   s_acc, gid, s_gid, s_cell, nnb, atom_cell, atom_slot, perm, tmp_src, tmp_key,
-                  cell_count, cell_start, rb_list, nbr, tile_rows, tile_nc, tile_cell, tile_coff, red, itop, ired, pairmat, mass, rc2, rlist2,
+                  cell_count, cell_start, rb_list, nbr, tile_rows, red, itop, ired, pairmat, mass, rc2, rlist2,
                   vdr2, rc2f, tabF, tabP, tabF2, tabP2, ring, ring_count};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (st) cudaStreamDestroy(st);
   if (st2) cudaStreamDestroy(st2);
 }
+
+// ---------------------------------------------------------------------------
+namespace ndg_internal {
+
+int setup_systems(ndg_ctx *c, const std::vector<int> &ids) {
+  if (!c) return NDG_ERR_ARG;
+  cudaSetDevice(c->device);
+  return setup_lists(c, ids);
+}
+
+int arm_built(ndg_ctx *c, int sys, int nsteps) {
+  if (!valid_sys(c, sys)) return NDG_ERR_ARG;
+  DevCtx d = devctx(c);
+  launch_arm(d, c->st, c->nsys_cap, sys, nsteps, START_BUILT);
+  CK(c, cudaGetLastError());
+  return NDG_OK;
+}
+
+int run_block(ndg_ctx *c, int K, ndg_thermo_cb cb, void *user) {
+  if (!c || K < 1) return NDG_ERR_ARG;
+  cudaSetDevice(c->device);
+  int rc = ensure_params(c);
+  if (rc) return rc;
+  CK(c, cudaMemset(c->ring_count, 0, 2 * sizeof(int)));
+  return run_blocks(c, K, cb, user);
+}
+
+int flush_system(ndg_ctx *c, int sys) {
+  if (!valid_sys(c, sys)) return NDG_ERR_ARG;
+  return flush_pending(c, sys);
+}
+
+int graph_captures(ndg_ctx *c) { return c ? c->captures : 0; }
+
+int take_system_error(ndg_ctx *c, int sys, int *err) {
+  if (!valid_sys(c, sys) || !err) return NDG_ERR_ARG;
+  SysState S;
+  int rc = get_state_dev(c, sys, S);
+  if (rc) return rc;
+  *err = S.err;
+  if (S.err) {
+    S.err = 0;
+    rc = put_state_dev(c, sys, S);
+  }
+  return rc;
+}
+
+}  // namespace ndg_internal
 
 // ===========================================================================
 // C ABI
@@ -1304,9 +1354,9 @@ static int run_impl(ndg_ctx *c, int nsteps, ndg_thermo_cb cb, void *user, int co
   if (rc) return rc;
   CK(c, cudaMemset(c->ring_count, 0, 4 * sizeof(int)));
   DevCtx d = devctx(c);
-  launch_begin_run(d, c->st, c->nsys_cap, nsteps, cont);
+  launch_arm(d, c->st, c->nsys_cap, -1, nsteps, cont ? START_NEW : START_BUILT);
   CK(c, cudaGetLastError());
-  rc = run_steps(c, nsteps, cb, user);
+  rc = run_blocks(c, nsteps, cb, user);
   int rf = flush_pending(c);
   return rc ? rc : rf;
 }
@@ -1482,8 +1532,7 @@ int ndg_autotune(ndg_ctx *c, int steps) {
       {c->disp, 3 * A * sizeof(double)},   {c->gid, A * sizeof(int)},
       {c->nnb, A * sizeof(int)},           {c->atom_cell, A * sizeof(int)},
       {c->itop, 2 * (size_t)c->atoms.cap * sizeof(double)},
-      {c->tile_nc, T * sizeof(int)},       {c->tile_rows, T * sizeof(int)},
-      {c->tile_cell, T * 256 * sizeof(int)}, {c->tile_coff, T * 257 * sizeof(int)},
+      {c->tile_rows, T * sizeof(int)},
       {c->cell_start, (size_t)c->cells.cap * sizeof(int)},
       {c->nbr, (size_t)c->nbrs.cap * sizeof(int)},
       {c->dS, (size_t)c->nsys_cap * sizeof(SysState)}};
@@ -1514,11 +1563,11 @@ int ndg_autotune(ndg_ctx *c, int steps) {
     drop_graphs(c);
     CK(c, cudaMemset(c->ring_count, 0, 4 * sizeof(int)));
     DevCtx d = devctx(c);
-    launch_begin_run(d, c->st, c->nsys_cap, 2 * steps, 1);
-    rc = run_steps(c, steps, nullptr, nullptr);  // warm: capture + first launch
+    launch_arm(d, c->st, c->nsys_cap, -1, 2 * steps, START_NEW);
+    rc = run_blocks(c, steps, nullptr, nullptr);  // warm: capture + first launch
     if (rc) break;
     cudaEventRecord(e0, c->st);
-    rc = run_steps(c, steps, nullptr, nullptr);
+    rc = run_blocks(c, steps, nullptr, nullptr);
     cudaEventRecord(e1, c->st);
     cudaEventSynchronize(e1);
     float ms = 0.f;
@@ -1554,7 +1603,8 @@ int ndg_profile_run(ndg_ctx *c, int nsteps) {
   DevCtx d = devctx(c);
   const int mixed = c->precision == NDG_PREC_MIXED;
   const int tpa = choose_tpa(c);
-  launch_begin_run(d, c->st, c->nsys_cap, nsteps, 1);
+  launch_arm(d, c->st, c->nsys_cap, -1, nsteps, START_NEW);
+  launch_begin_block(d, c->st, c->nsys_cap, nsteps);
   std::vector<cudaEvent_t> ev(4 * (size_t)nsteps);
   for (auto &e : ev) CK(c, cudaEventCreate(&e));
   for (int k = 0; k < nsteps; ++k) {

@@ -17,6 +17,7 @@
 #include <cstdio>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "ndg_kernels.h"
 
@@ -152,6 +153,37 @@ __global__ __launch_bounds__(BLOCK) void k_integrate1(DevCtx c, int standalone, 
 // End-of-step epilogue for one system, run by the last block of the pair
 // kernel to finish (dynamics, src/nd.f90:164-178 and the next step's head
 // :138-151).
+// The next step's list decision for a system (dynamics, src/nd.f90:138-151):
+// CheckListUpdate every ReNeiFreq steps on the two largest displacement
+// measures; in fixed semantics a rebuild also resizes the cell grid to stay
+// at least rcut+skin wide.  A rebuilding system goes on the rebuild list
+// and, inside a captured step block, switches on the next step's rebuild
+// node.
+__device__ void decide_rebuild(const DevCtx &c, int sys, const SysParam *P, SysState *S,
+                               double t1, double t2, unsigned long long next_h) {
+  int rb = 0;
+  if (P->renei && S->step % P->renei_freq == 0) {
+    rb = list_check(*P, *S, t1, t2);
+    if (rb < 0) {
+      set_err(c, S, E_OUT_OF_BOX);
+      rb = 0;
+    }
+  }
+  if (rb && P->quirk != 0) {
+    int nc = 1;
+    for (int d = 0; d < 3; ++d) {
+      const int m = (int)(S->box[d] / P->rlist);
+      S->mcell[d] = m < P->mcell0[d] ? m : P->mcell0[d];
+      if (S->mcell[d] < 2) set_err(c, S, E_CELLS);
+      nc *= S->mcell[d];
+    }
+    S->ncell = nc;
+  }
+  S->rebuild = rb;
+  if (rb) c.rb_list[atomicAdd(c.ring_count + 3, 1)] = sys;
+  if (rb && next_h) cudaGraphSetConditional((cudaGraphConditionalHandle)next_h, 1u);
+}
+
 // The tiles' partials are summed in an order that depends only on the tile
 // index (the first FIN threads, whatever the block size): FP64 values by a
 // fixed tree in `fs` (shared, NR rows of FIN doubles: the 7 energy/virial
@@ -263,29 +295,7 @@ __device__ void finalize_system(const DevCtx &c, int sys, int blk0, int nblk, in
     // F_DONE keeps the step's second pair kernel (the other energy/virial
     // variant) from taking this system again under the next step's flags
     S->flags = step_flags(*P, S->step, S->tt) | F_ACTIVE | F_DONE;
-    int rb = 0;
-    if (P->renei && S->step % P->renei_freq == 0) {
-      rb = list_check(*P, *S, t1, t2);
-      if (rb < 0) {
-        set_err(c, S, E_OUT_OF_BOX);
-        rb = 0;
-      }
-    }
-    if (rb && P->quirk != 0) {
-      // fixed semantics: cells must stay at least rcut+skin wide
-      int nc = 1;
-      for (int d = 0; d < 3; ++d) {
-        int m = (int)(S->box[d] / P->rlist);
-        S->mcell[d] = m < P->mcell0[d] ? m : P->mcell0[d];
-        if (S->mcell[d] < 2) set_err(c, S, E_CELLS);
-        nc *= S->mcell[d];
-      }
-      S->ncell = nc;
-    }
-    S->rebuild = rb;
-    if (rb) c.rb_list[atomicAdd(c.ring_count + 3, 1)] = sys;
-    // inside a captured step block: switch on the next step's rebuild node
-    if (rb && next_h) cudaGraphSetConditional((cudaGraphConditionalHandle)next_h, 1u);
+    decide_rebuild(c, sys, P, S, t1, t2, next_h);
   } else {
     S->flags = 0;
     S->rebuild = 0;
@@ -345,39 +355,51 @@ __global__ __launch_bounds__(BLOCK) void k_integrate2(DevCtx c, int ck) {
 
 // ---------------------------------------------------------------------------
 // run bookkeeping
-__global__ void k_begin_run(DevCtx c, int nsys_cap, int nsteps, int cont) {
+// give every system (sys < 0) or one system a run of nsteps starting as
+// `start` (START_*)
+__global__ void k_arm(DevCtx c, int nsys_cap, int sys, int nsteps, int start) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsys_cap || (sys >= 0 && s != sys) || c.P[s].n == 0) return;
+  c.S[s].run_left = nsteps;
+  c.S[s].start = start;
+}
+
+// Head of a block of up to K steps: each system with steps left in its run
+// takes min(K, left) of them.  A new run starts at tt = 1 (write_thermo and
+// e0 on its first step, src/nd.f90:139-148,167); a continued run takes the
+// step the previous block's last epilogue left off, with the same list
+// decision (dynamics, src/nd.f90:138-151).
+__global__ void k_begin_block(DevCtx c, int nsys_cap, int K) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsys_cap) return;
   const SysParam &P = c.P[s];
   SysState &S = c.S[s];
-  if (P.n == 0) {
-    S.flags = 0;
-    return;
-  }
-  S.steps_left = nsteps;
-  S.tt = 1;
-  S.step = S.step + 1;
-  S.flags = step_flags(P, S.step, 1) | F_ACTIVE;
-  for (int d = 0; d < 3; ++d) S.li[d] = 1.0 / S.box[d];
-  int rb = 0;
-  if (cont && P.renei && S.step % P.renei_freq == 0) {
-    rb = list_check(P, S, S.dtop[0], S.dtop[1]);
-    if (rb < 0) {
-      set_err(c, &S, E_OUT_OF_BOX);
-      rb = 0;
-    }
-  }
-  S.rebuild = rb;
-  if (rb) c.rb_list[atomicAdd(c.ring_count + 3, 1)] = s;
   S.ticket = 0;
   S.ticket_i = 0;
+  if (P.n == 0 || S.run_left <= 0) {
+    S.flags = 0;
+    S.steps_left = 0;
+    S.rebuild = 0;
+    return;
+  }
+  const int k = S.run_left < K ? S.run_left : K;
+  S.run_left -= k;
+  S.steps_left = k;
+  const int start = S.start;
+  S.start = START_CONTINUE;
+  S.tt = start == START_CONTINUE ? S.tt + 1 : 1;
+  S.step = S.step + 1;
+  S.flags = step_flags(P, S.step, S.tt) | F_ACTIVE;
+  for (int d = 0; d < 3; ++d) S.li[d] = 1.0 / S.box[d];
+  if (start == START_BUILT) S.rebuild = 0;
+  else decide_rebuild(c, s, &P, &S, S.dtop[0], S.dtop[1], 0ull);
 }
 
 // apply pending mkIsoKE/mkIsoE velocity scales at the end of a run
-__global__ __launch_bounds__(BLOCK) void k_flush(DevCtx c) {
+__global__ __launch_bounds__(BLOCK) void k_flush(DevCtx c, int only) {
   const int chunk = blockIdx.x;
   const int sys = c.chunk_sys[chunk];
-  if (sys < 0) return;
+  if (sys < 0 || (only >= 0 && sys != only)) return;
   const SysParam *__restrict__ P = c.P + sys;
   const SysState *S = c.S + sys;
   const int pend = S->pend;
@@ -393,9 +415,9 @@ __global__ __launch_bounds__(BLOCK) void k_flush(DevCtx c) {
   }
 }
 
-__global__ void k_clear_pend(DevCtx c, int nsys_cap) {
+__global__ void k_clear_pend(DevCtx c, int nsys_cap, int sys) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s < nsys_cap) c.S[s].pend = 0;
+  if (s < nsys_cap && (sys < 0 || s == sys)) c.S[s].pend = 0;
 }
 
 __global__ __launch_bounds__(BLOCK) void k_scale_vel(DevCtx c, int sys, double lam) {
@@ -695,17 +717,19 @@ __global__ __launch_bounds__(BLOCK) void k_copyback(DevCtx c, int mixed) {
 // Neighbour build, one CTA per 128-atom tile (atoms are sorted by link cell,
 // so a tile covers a short run of cells).
 //   1. The cells its atoms' stencils reach are collected in a shared-memory
-//      hash set, sorted, and recorded with their candidate offsets
-//      (tile_cell / tile_coff); the pair kernel stages exactly these atoms.
-//   2. The candidates are staged as 32-bit fixed-point positions; a warp
-//      takes one own atom and tests the candidates of each stencil entry, 32
-//      per pass.  An FP32 distance decides every pair farther than a 1e-5
+//      hash set, sorted, and given candidate offsets by a block scan.
+//   2. The candidates are staged as 32-bit fixed-point positions; each run
+//      of own atoms in one cell gets one flat list of its stencil entries'
+//      candidates; a warp takes one own atom and tests 32 candidates per
+//      pass.  An FP32 distance decides every pair farther than a 1e-5
 //      relative margin from the cutoff (and from PTrMin); pairs inside the
 //      margin take the reference's exact FP64 test, so membership is
 //      bit-identical to buildVerletList (src/nd.f90:1356-1383 for the cell
 //      itself, :1403-1426 for the neighbour cells).
 //   3. Hits are compacted with __ballot_sync/__popc into 16-bit tile-local
 //      candidate indices and written to the blocked list row by row.
+// A tile whose cells or candidates do not fit the shared buffers takes
+// build_tile_direct (same test, same list order, no staging).
 constexpr int TILE = 128;      // atoms per tile
 constexpr int TC_MAX = 256;    // link cells a tile may stage
 constexpr int HSLOTS = 1024;   // shared hash slots for the tile's cell set
@@ -749,6 +773,103 @@ __device__ __forceinline__ int find_cell(const int *ucell, int nu, int cell) {
   return lo;
 }
 
+// The candidate test of the neighbour build for own atom i (double position
+// pid, fixed-point pi, type ti) and candidate j: FP32 distance on the
+// fixed-point positions, the reference's FP64 test within NB_MARGIN of the
+// list radius (or of PTrMin in the same cell), src/nd.f90:1356-1383,1403-1426.
+__device__ __forceinline__ bool nb_hit(const DevCtx &c, const SysParam *P, const int *pm,
+                                       const double4 &pid, const int4 &pi, int ti, int j,
+                                       bool center, float sb0, float sb1, float sb2, double b0,
+                                       double b1, double b2) {
+  const double4 pjd = c.pos[j];
+  const int4 pj = make_int4(fx32(pjd.x), fx32(pjd.y), fx32(pjd.z), tw_of(pjd.w));
+  const int nt = P->ntypes, tj = tw_type(pj.w);
+  const int a = pm[(ti - 1) + (tj - 1) * nt], b = pm[(tj - 1) + (ti - 1) * nt];
+  const int mx = a > b ? a : b;
+  if (mx <= 0) return false;
+  const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * sb0;
+  const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * sb1;
+  const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * sb2;
+  const float d2f = r0 * r0 + r1 * r1 + r2 * r2;
+  const double rl = c.rlist2[P->pair_off + mx - 1];
+  const float rlf = (float)rl;
+  const double ptrmin = P->ptrmin;
+  const float ptrlo = (float)ptrmin * (1.f - NB_MARGIN), ptrhi = (float)ptrmin * (1.f + NB_MARGIN);
+  const bool near_cut = fabsf(d2f - rlf) <= NB_MARGIN * rlf;
+  const bool near_min = center && d2f >= ptrlo && d2f <= ptrhi;
+  if (!(near_cut || near_min)) return !(center && d2f < ptrlo) && d2f < rlf;
+  double s0 = pid.x - pjd.x, s1 = pid.y - pjd.y, s2 = pid.z - pjd.z;
+  s0 = s0 - round(s0);
+  s1 = s1 - round(s1);
+  s2 = s2 - round(s2);
+  const double x0 = b0 * s0, x1 = b1 * s1, x2 = b2 * s2;
+  double d2 = x0 * x0;
+  d2 = d2 + x1 * x1;
+  d2 = d2 + x2 * x2;
+  return !(center && d2 < ptrmin) && !(d2 > rl);
+}
+
+// Neighbour build of one tile without shared staging, for tiles whose cells
+// or candidates exceed the staged path's buffers (coarse cell grids, dense
+// or shrunk boxes): one warp per own atom walks its stencil cells in order,
+// reading candidates from global memory, with the same test and the same
+// list order (stencil entry, then cell order) as the staged path.
+__device__ __noinline__ void build_tile_direct(const DevCtx &c, int sys, int tile, const int *stc,
+                                               int ne, int *ncnt, int *rows_s) {
+  const SysParam *__restrict__ P = c.P + sys;
+  SysState *S = c.S + sys;
+  const int a0 = tile * TILE, local0 = a0 - P->atom_off;
+  const int nown = min(TILE, P->n - local0);
+  const int M0 = S->mcell[0], M1 = S->mcell[1], M2 = S->mcell[2];
+  const int maxnb = P->maxnb;
+  const int *cst = c.cell_start + P->cell_off;
+  const int *pm = c.pairmat + P->pm_off;
+  const double b0 = S->box[0], b1 = S->box[1], b2 = S->box[2];
+  const float sb0 = (float)(b0 * (1.0 / FX_ONE)), sb1 = (float)(b1 * (1.0 / FX_ONE)),
+              sb2 = (float)(b2 * (1.0 / FX_ONE));
+  int *dst = c.nbr + P->nbr_off + (long long)(local0 / TILE) * maxnb * TILE;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int t = warp; t < nown; t += NBT / 32) {
+    const int i = a0 + t;
+    const int cl = c.atom_cell[i];
+    const double4 pid = c.pos[i];
+    const int4 pi = make_int4(fx32(pid.x), fx32(pid.y), fx32(pid.z), tw_of(pid.w));
+    const int ti = tw_type(pi.w);
+    int cnt = 0;
+    for (int e = 0; e < ne; ++e) {
+      const int nc = stencil_cell(cl, stc[e], M0, M1, M2);
+      const bool center = (stc[e] >> 12) & 1;
+      const int s0 = cst[nc], s1 = cst[nc + 1];
+      for (int vb = s0; vb < s1; vb += 32) {
+        const int v = vb + lane;
+        const int j = P->atom_off + v;
+        const bool hit = v < s1 && j != i &&
+                         nb_hit(c, P, pm, pid, pi, ti, j, center, sb0, sb1, sb2, b0, b1, b2);
+        const unsigned bal = __ballot_sync(0xffffffffu, hit);
+        if (hit) {
+          const int k = cnt + __popc(bal & ((1u << lane) - 1u));
+          if (k < maxnb) dst[k * TILE + t] = j;
+        }
+        cnt += __popc(bal);
+      }
+    }
+    if (lane == 0) ncnt[t] = cnt;
+  }
+  if (threadIdx.x == 0) *rows_s = 0;
+  __syncthreads();
+  if (threadIdx.x < TILE) {
+    const int r = __reduce_max_sync(0xffffffffu,
+                                    (int)threadIdx.x < nown ? min(ncnt[threadIdx.x], maxnb) : 0);
+    if ((threadIdx.x & 31) == 0) atomicMax(rows_s, r);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) c.tile_rows[tile] = *rows_s;
+  if (threadIdx.x < nown) {
+    c.nnb[a0 + threadIdx.x] = ncnt[threadIdx.x];
+    if (ncnt[threadIdx.x] > maxnb) set_err(c, S, E_NEIMAX);
+  }
+}
+
 __device__ void build_tile(const DevCtx &c, int sys, int tile) {
   extern __shared__ __align__(16) unsigned char dsm[];
   __syncthreads();  // the block's previous tile is done with shared memory
@@ -758,10 +879,7 @@ __device__ void build_tile(const DevCtx &c, int sys, int tile) {
   const int local0 = a0 - P->atom_off;
   const int nown = min(TILE, P->n - local0);
   if (nown <= 0) {
-    if (threadIdx.x == 0) {
-      c.tile_nc[tile] = 0;
-      c.tile_rows[tile] = 0;
-    }
+    if (threadIdx.x == 0) c.tile_rows[tile] = 0;
     return;
   }
   const int M0 = S->mcell[0], M1 = S->mcell[1], M2 = S->mcell[2];
@@ -783,6 +901,13 @@ __device__ void build_tile(const DevCtx &c, int sys, int tile) {
   __shared__ int nu, bad, nruns, rows_s;
   __shared__ int pm_s[16 * 16];
   __shared__ int scan_w[NBT / 32];
+  if (maxnb > c.nb_maxnb) {
+    // lists longer than the shared list buffer holds
+    if (threadIdx.x < ne) stc[threadIdx.x] = S->stencil[threadIdx.x];
+    __syncthreads();
+    build_tile_direct(c, sys, tile, stc, ne, ncnt, &rows_s);
+    return;
+  }
   __shared__ float rl2f_s[136];
   __shared__ double rl2_s[136];
   const int nt = P->ntypes, npr = P->npairs;
@@ -865,23 +990,12 @@ __device__ void build_tile(const DevCtx &c, int sys, int tile) {
   }
   __syncthreads();
   if (bad) {
-    if (threadIdx.x == 0) {
-      c.tile_nc[tile] = 0;
-      c.tile_rows[tile] = 0;
-      set_err(c, S, E_NEIMAX);
-    }
-    if (threadIdx.x < nown) c.nnb[a0 + threadIdx.x] = 0;
+    // more cells or candidates than the shared buffers hold
+    build_tile_direct(c, sys, tile, stc, ne, ncnt, &rows_s);
     return;
   }
   const int U = nu, C = coff[nu];
-  if (threadIdx.x == 0) {
-    atomicMax(c.ring_count + 2, C);
-    c.tile_nc[tile] = U;
-  }
-  for (int u = threadIdx.x; u <= U; u += NBT) {
-    if (u < U) c.tile_cell[(size_t)tile * TC_MAX + u] = ucell[u];
-    c.tile_coff[(size_t)tile * (TC_MAX + 1) + u] = coff[u];
-  }
+  if (threadIdx.x == 0) atomicMax(c.ring_count + 2, C);
   // 2. stage the candidates
   for (int u = threadIdx.x >> 5; u < U; u += NBT / 32) {
     const int q0 = coff[u], len = coff[u + 1] - q0;
@@ -1039,12 +1153,8 @@ __device__ void build_tile(const DevCtx &c, int sys, int tile) {
     rb = re;
   }
   if (bad) {
-    if (threadIdx.x == 0) {
-      c.tile_nc[tile] = 0;
-      c.tile_rows[tile] = 0;
-      set_err(c, S, E_NEIMAX);
-    }
-    if (threadIdx.x < nown) c.nnb[a0 + threadIdx.x] = 0;
+    // a run's candidate list is longer than the flat buffer
+    build_tile_direct(c, sys, tile, stc, ne, ncnt, &rows_s);
     return;
   }
   // 4. write the tile's lists row by row (consecutive threads, consecutive atoms)
@@ -1096,39 +1206,51 @@ __global__ __launch_bounds__(NBT) void k_build(DevCtx c) {
 // shared memory once per system change.
 constexpr int UNR_D = 2;  // FP64: pairs in flight per thread
 
+// Mixed precision: a pair whose FP32 squared distance lies within NEAR_CUT
+// (relative) of the squared cutoff takes compute0's FP64 cutoff test, so
+// the two precisions sum the same set of pairs (the tabulated force at the
+// cutoff is not zero).  The FP32 distance from 32-bit fixed-point
+// positions is within 1e-6 relative of the FP64 one for boxes up to
+// 1e3 cutoffs wide, so 1e-5 leaves a tenfold margin.
+constexpr float NEAR_CUT = 1e-5f;
+
 struct TabView {
   const int *pm;
   const double *rc2;
   const float *rc2f, *vdr2;
+  const float4 *pp;         // staged: per pair {rc2f(1-NEAR_CUT), rc2f(1+NEAR_CUT), vdr2, rc2f}
   const double *tF, *tP;    // FP64 tables
   const float2 *tF2, *tP2;  // FP32 (k, k+1) pairs
 };
 
-template <bool MIXED>
+// Staged layout (stab_bytes): pair matrix | rc2 (double) | packed per-pair
+// float4 | F table | P table.  The kernel without energy skips the P table.
+template <bool MIXED, bool EV>
 __device__ void stage_tables(const DevCtx &c, const SysParam *P, unsigned char *sm, TabView &tv) {
   const int nt = P->ntypes, np = P->npairs, T = P->ptsize + 1;
   int *pm = (int *)sm;
   int off = (nt * nt * 4 + 15) / 16 * 16;
   double *rc2 = (double *)(sm + off);
-  float *rc2f = (float *)(sm + off + np * 8);
-  float *vdr2 = (float *)(sm + off + np * 12);
-  off = (off + np * 16 + 15) / 16 * 16;
+  off = (off + np * 8 + 15) / 16 * 16;
+  float4 *pp = (float4 *)(sm + off);
+  off += np * 16;
   for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) pm[k] = c.pairmat[P->pm_off + k];
   for (int k = threadIdx.x; k < np; k += blockDim.x) {
     rc2[k] = c.rc2[P->pair_off + k];
-    rc2f[k] = c.rc2f[P->pair_off + k];
-    vdr2[k] = c.vdr2[P->pair_off + k];
+    const float r = c.rc2f[P->pair_off + k];
+    pp[k] = make_float4(r * (1.f - NEAR_CUT), r * (1.f + NEAR_CUT), c.vdr2[P->pair_off + k], r);
   }
   tv.pm = pm;
   tv.rc2 = rc2;
-  tv.rc2f = rc2f;
-  tv.vdr2 = vdr2;
+  tv.pp = pp;
+  tv.rc2f = c.rc2f + P->pair_off;
+  tv.vdr2 = c.vdr2 + P->pair_off;
   if (MIXED) {
     float2 *dF = (float2 *)(sm + off), *dP = dF + np * T;
     const float2 *sF = c.tabF2 + P->tab_off, *sP = c.tabP2 + P->tab_off;
     for (int k = threadIdx.x; k < np * T; k += blockDim.x) {
       dF[k] = sF[k];
-      dP[k] = sP[k];
+      if (EV) dP[k] = sP[k];
     }
     tv.tF2 = dF;
     tv.tP2 = dP;
@@ -1137,7 +1259,7 @@ __device__ void stage_tables(const DevCtx &c, const SysParam *P, unsigned char *
     const double *sF = c.tabF + P->tab_off, *sP = c.tabP + P->tab_off;
     for (int k = threadIdx.x; k < np * T; k += blockDim.x) {
       dF[k] = sF[k];
-      dP[k] = sP[k];
+      if (EV) dP[k] = sP[k];
     }
     tv.tF = dF;
     tv.tP = dP;
@@ -1149,42 +1271,55 @@ __device__ __forceinline__ void global_tables(const DevCtx &c, const SysParam *P
   tv.rc2 = c.rc2 + P->pair_off;
   tv.rc2f = c.rc2f + P->pair_off;
   tv.vdr2 = c.vdr2 + P->pair_off;
+  tv.pp = nullptr;
   tv.tF = c.tabF + P->tab_off;
   tv.tP = c.tabP + P->tab_off;
   tv.tF2 = c.tabF2 + P->tab_off;
   tv.tP2 = c.tabP2 + P->tab_off;
 }
 
-// MODE 0: tables read from global memory; 1: staged in shared memory;
-// 2: staged, and every system has one type and one pair (no per-pair
-// type lookup, cutoff and table scale held in registers).
+// per-pair cutoff band and table scale of the mixed loop
+template <bool STAB>
+__device__ __forceinline__ float4 pair_params(const TabView &tv, int p1) {
+  if (STAB) return tv.pp[p1];
+  const float r = tv.rc2f[p1];
+  return make_float4(r * (1.f - NEAR_CUT), r * (1.f + NEAR_CUT), tv.vdr2[p1], r);
+}
+
+// STAB: tables staged in shared memory (else read from global memory).
 // EV: the kernel of steps that need the potential energy or the virial
 // (calcPot / calcVirial); the kernel of the other steps carries no energy
-// or virial accumulators, so its pair loop holds fewer registers.
+// or virial state, so its pair loop holds fewer registers.  Per tile, a
+// system with one type and one pair potential takes the loop with the pair
+// parameters in registers, others look them up per pair.
 //
 // Mixed precision: each thread sums whole chunks of CHUNK consecutive list
 // entries in FP32, in list order, and adds every chunk's sum to 64-bit
-// fixed-point totals (force, and with EV potential energy and virial).
-// Chunks are dealt to the TPA threads of an atom round-robin, so every
-// launch shape forms the same chunks and the integer totals, which do not
-// depend on the order of addition, are the same bits for any TPA, grid or
-// batch composition.
+// fixed-point totals (the force in registers; with EV, the potential energy
+// and virial in per-thread shared-memory slots).  Chunks are dealt to the
+// TPA threads of an atom round-robin, so every launch shape forms the same
+// chunks and the integer totals, which do not depend on the order of
+// addition, are the same bits for any TPA, grid or batch composition.
 constexpr int CHUNK = 8;   // mixed: list entries per FP32 partial sum
 constexpr int GATHER = 4;  // mixed: neighbour gathers in flight per thread
-// Mixed precision: a pair whose FP32 squared distance lies within NEAR_CUT
-// (relative) of the squared cutoff takes compute0's FP64 cutoff test, so
-// the two precisions sum the same set of pairs (the tabulated force at the
-// cutoff is not zero).  The FP32 distance from 32-bit fixed-point
-// positions is within 1e-6 relative of the FP64 one for boxes up to
-// 1e3 cutoffs wide, so 1e-5 leaves a tenfold margin.
-constexpr float NEAR_CUT = 1e-5f;
 
-template <int TPA, bool MIXED, bool FUSE, int MODE, bool EV>
-__global__ __launch_bounds__(TILE * TPA) void k_pair(DevCtx c, int host_flags, int ntiles,
+// resident 128-thread CTAs per SM each variant is compiled for (register
+// budget 65536 / (128 * n)): the mixed lean loop fits 72 registers, its
+// energy/virial form about 100, the FP64 ones 100 and 128
+template <bool MIXED, bool EV>
+constexpr int pair_ctas() {
+  return MIXED ? (EV ? 5 : 7) : (EV ? 4 : 5);
+}
+
+template <int TPA, bool MIXED, bool FUSE, bool STAB, bool EV>
+__global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV>() * 128 / (TILE * TPA)) > 0
+                                             ? pair_ctas<MIXED, EV>() * 128 / (TILE * TPA)
+                                             : 1) void k_pair(DevCtx c, int host_flags, int ntiles,
                                                      unsigned long long next_h) {
-  constexpr bool STAB = MODE >= 1;
-  constexpr bool ONE = MODE == 2;
+  constexpr int NT = TILE * TPA;
   extern __shared__ __align__(16) unsigned char dsm[];
+  // mixed EV: 7 fixed-point slots (energy, virial) per thread, after the tables
+  unsigned long long *evq = (unsigned long long *)(dsm + (STAB ? c.stab_smem : 0));
   const int G = gridDim.x;
   const int t0 = (int)((long long)blockIdx.x * ntiles / G);
   const int t1 = (int)((long long)(blockIdx.x + 1) * ntiles / G);
@@ -1195,6 +1330,8 @@ __global__ __launch_bounds__(TILE * TPA) void k_pair(DevCtx c, int host_flags, i
   __shared__ double s_red[NR][TILE];          // per-atom values, reduced by atom index
   __shared__ unsigned long long s_q[7];       // mixed: tile's fixed-point PE and virial
   if (threadIdx.x < 7) s_q[threadIdx.x] = 0ull;
+  if (MIXED && EV)
+    for (int k = 0; k < 7; ++k) evq[k * NT + threadIdx.x] = 0ull;
   __syncthreads();
 
   for (int tile = t0; tile < t1; ++tile) {
@@ -1210,7 +1347,7 @@ __global__ __launch_bounds__(TILE * TPA) void k_pair(DevCtx c, int host_flags, i
     if (sys != loaded) {
       if (STAB) {
         __syncthreads();  // no thread still reads the previous system's tables
-        stage_tables<MIXED>(c, P, dsm, tv);
+        stage_tables<MIXED, EV>(c, P, dsm, tv);
         __syncthreads();  // tables complete before the first pair
       } else {
         global_tables(c, P, tv);
@@ -1241,9 +1378,9 @@ __global__ __launch_bounds__(TILE * TPA) void k_pair(DevCtx c, int host_flags, i
     const bool valid = local < P->n;
     const bool cu = EV && (flags & F_CU), cv = EV && (flags & F_CV);
     const int ntypes = P->ntypes, T = P->ptsize + 1, ptsize = P->ptsize;
+    const bool one = ntypes == 1 && P->npairs == 1 && tv.pm[0] == 1;
 
-    double pe = 0.0, vir[6] = {0, 0, 0, 0, 0, 0};       // FP64 path
-    long long qpe = 0, qv[6] = {0, 0, 0, 0, 0, 0};      // mixed path, fixed point
+    double pe = 0.0, vir[6] = {0, 0, 0, 0, 0, 0};  // FP64 path
     double fx = 0.0, fy = 0.0, fz = 0.0;
     long long qx = 0, qy = 0, qz = 0;  // mixed: 64-bit fixed-point force
     int ti = 1;
@@ -1259,51 +1396,56 @@ __global__ __launch_bounds__(TILE * TPA) void k_pair(DevCtx c, int host_flags, i
         const int *pmr = tv.pm + (ti - 1);
         const double b0 = S->box[0], b1 = S->box[1], b2 = S->box[2];
         const double ptrmin = P->ptrmin;
-        for (int k0 = la; k0 < cnt; k0 += UNR_D * TPA) {
-          int qq[UNR_D];
-          double4 pj[UNR_D];
+        auto loop = [&](auto one_t) {
+          constexpr bool ONE = decltype(one_t)::value;
+          for (int k0 = la; k0 < cnt; k0 += UNR_D * TPA) {
+            int qq[UNR_D];
+            double4 pj[UNR_D];
 #pragma unroll
-          for (int q = 0; q < UNR_D; ++q) {
-            const int k = k0 + q * TPA;
-            qq[q] = k < cnt ? __ldg(nb + k * TILE) : -1;
-          }
+            for (int q = 0; q < UNR_D; ++q) {
+              const int k = k0 + q * TPA;
+              qq[q] = k < cnt ? __ldg(nb + k * TILE) : -1;
+            }
 #pragma unroll
-          for (int q = 0; q < UNR_D; ++q) pj[q] = c.pos[qq[q] >= 0 ? qq[q] : i];
+            for (int q = 0; q < UNR_D; ++q) pj[q] = c.pos[qq[q] >= 0 ? qq[q] : i];
 #pragma unroll
-          for (int q = 0; q < UNR_D; ++q) {
-            const int pt = ONE ? 1 : pmr[(tw_type(tw_of(pj[q].w)) - 1) * ntypes];
-            const int p1 = ONE ? 0 : (pt > 0 ? pt - 1 : 0);
-            double s0 = pi.x - pj[q].x, s1 = pi.y - pj[q].y, s2 = pi.z - pj[q].z;
-            s0 = s0 - round(s0);
-            s1 = s1 - round(s1);
-            s2 = s2 - round(s2);
-            const double r0 = b0 * s0, r1 = b1 * s1, r2 = b2 * s2;
-            double d2 = r0 * r0;
-            d2 = d2 + r1 * r1;
-            d2 = d2 + r2 * r2;
-            const bool ok = qq[q] >= 0 && pt > 0 && !(d2 > tv.rc2[p1]);
-            const float rk = (float)(d2 - ptrmin) * tv.vdr2[p1] + 1.0f;
-            int kk = (int)rk;
-            kk = kk < 1 ? 1 : (kk > ptsize ? ptsize : kk);
-            const double w = (double)rk - (double)kk;
-            const int base = p1 * T + kk - 1;
-            const double fk1 = tv.tF[base + 1], fk = tv.tF[base];
-            double df = w * fk1 + (1.0 - w) * fk;
-            df = ok ? df / d2 : 0.0;
-            fx = fx + r0 * df;
-            fy = fy + r1 * df;
-            fz = fz + r2 * df;
-            if (cu && ok) pe = pe + (w * tv.tP[base + 1] + (1.0 - w) * tv.tP[base]);
-            if (cv) {
-              vir[0] = vir[0] + r0 * r0 * df;
-              vir[1] = vir[1] + r1 * r1 * df;
-              vir[2] = vir[2] + r2 * r2 * df;
-              vir[3] = vir[3] + r0 * r1 * df;
-              vir[4] = vir[4] + r0 * r2 * df;
-              vir[5] = vir[5] + r1 * r2 * df;
+            for (int q = 0; q < UNR_D; ++q) {
+              const int pt = ONE ? 1 : pmr[(tw_type(tw_of(pj[q].w)) - 1) * ntypes];
+              const int p1 = ONE ? 0 : (pt > 0 ? pt - 1 : 0);
+              double s0 = pi.x - pj[q].x, s1 = pi.y - pj[q].y, s2 = pi.z - pj[q].z;
+              s0 = s0 - round(s0);
+              s1 = s1 - round(s1);
+              s2 = s2 - round(s2);
+              const double r0 = b0 * s0, r1 = b1 * s1, r2 = b2 * s2;
+              double d2 = r0 * r0;
+              d2 = d2 + r1 * r1;
+              d2 = d2 + r2 * r2;
+              const bool ok = qq[q] >= 0 && pt > 0 && !(d2 > tv.rc2[p1]);
+              const float rk = (float)(d2 - ptrmin) * tv.vdr2[p1] + 1.0f;
+              int kk = (int)rk;
+              kk = kk < 1 ? 1 : (kk > ptsize ? ptsize : kk);
+              const double w = (double)rk - (double)kk;
+              const int base = p1 * T + kk - 1;
+              const double fk1 = tv.tF[base + 1], fk = tv.tF[base];
+              double df = w * fk1 + (1.0 - w) * fk;
+              df = ok ? df / d2 : 0.0;
+              fx = fx + r0 * df;
+              fy = fy + r1 * df;
+              fz = fz + r2 * df;
+              if (cu && ok) pe = pe + (w * tv.tP[base + 1] + (1.0 - w) * tv.tP[base]);
+              if (cv) {
+                vir[0] = vir[0] + r0 * r0 * df;
+                vir[1] = vir[1] + r1 * r1 * df;
+                vir[2] = vir[2] + r2 * r2 * df;
+                vir[3] = vir[3] + r0 * r1 * df;
+                vir[4] = vir[4] + r0 * r2 * df;
+                vir[5] = vir[5] + r1 * r2 * df;
+              }
             }
           }
-        }
+        };
+        if (one) loop(std::true_type{});
+        else loop(std::false_type{});
       } else {
         const int4 pi = c.pfx[i];
         ti = tw_type(pi.w);
@@ -1312,126 +1454,132 @@ __global__ __launch_bounds__(TILE * TPA) void k_pair(DevCtx c, int host_flags, i
         const float sb1 = (float)(S->box[1] * (1.0 / FX_ONE));
         const float sb2 = (float)(S->box[2] * (1.0 / FX_ONE));
         const float ptrmin = (float)P->ptrmin;
-        const float rc2f1 = tv.rc2f[0], vdr21 = tv.vdr2[0];
-        const float rlo1 = rc2f1 * (1.f - NEAR_CUT), rhi1 = rc2f1 * (1.f + NEAR_CUT);
         const int nch = (cnt + CHUNK - 1) / CHUNK;
-        for (int m = la; m < nch; m += TPA) {
-          const int kb = m * CHUNK;
-          int qq[CHUNK];
+        auto loop = [&](auto one_t) {
+          constexpr bool ONE = decltype(one_t)::value;
+          const float4 pp1 = ONE ? pair_params<STAB>(tv, 0) : make_float4(0.f, 0.f, 0.f, 0.f);
+          for (int m = la; m < nch; m += TPA) {
+            const int kb = m * CHUNK;
+            int qq[CHUNK];
 #pragma unroll
-          for (int q = 0; q < CHUNK; ++q) qq[q] = kb + q < cnt ? __ldg(nb + (kb + q) * TILE) : -1;
-          float ax = 0.f, ay = 0.f, az = 0.f, ape = 0.f;
-          float av0 = 0.f, av1 = 0.f, av2 = 0.f, av3 = 0.f, av4 = 0.f, av5 = 0.f;
-          unsigned nm = 0;  // entries of this chunk within FP32 rounding of the cutoff
+            for (int q = 0; q < CHUNK; ++q)
+              qq[q] = kb + q < cnt ? __ldg(nb + (kb + q) * TILE) : -1;
+            float ax = 0.f, ay = 0.f, az = 0.f, ape = 0.f;
+            float av0 = 0.f, av1 = 0.f, av2 = 0.f, av3 = 0.f, av4 = 0.f, av5 = 0.f;
+            unsigned nm = 0;  // entries of this chunk within FP32 rounding of the cutoff
 #pragma unroll
-          for (int h = 0; h < CHUNK; h += GATHER) {
-            int4 pj[GATHER];
+            for (int h = 0; h < CHUNK; h += GATHER) {
+              int4 pj[GATHER];
 #pragma unroll
-            for (int q = 0; q < GATHER; ++q) pj[q] = c.pfx[qq[h + q] >= 0 ? qq[h + q] : i];
+              for (int q = 0; q < GATHER; ++q) pj[q] = c.pfx[qq[h + q] >= 0 ? qq[h + q] : i];
 #pragma unroll
-            for (int q = 0; q < GATHER; ++q) {
-              const int pt = ONE ? 1 : pmr[(tw_type(pj[q].w) - 1) * ntypes];
-              const int p1 = ONE ? 0 : (pt > 0 ? pt - 1 : 0);
-              // minimum image by 32-bit wrap-around of the fixed-point difference
-              const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj[q].x) * sb0;
-              const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj[q].y) * sb1;
-              const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj[q].z) * sb2;
-              const float d2 = __fmaf_rn(r0, r0, __fmaf_rn(r1, r1, __fmul_rn(r2, r2)));
-              const bool live = qq[h + q] >= 0 && pt > 0;
-              const float rlo = ONE ? rlo1 : tv.rc2f[p1] * (1.f - NEAR_CUT);
-              const float rhi = ONE ? rhi1 : tv.rc2f[p1] * (1.f + NEAR_CUT);
-              const bool ok = live && d2 <= rlo;
-              nm |= (live && d2 > rlo && d2 <= rhi) ? (1u << (h + q)) : 0u;
-              // branch-free: every lane evaluates the pair, excluded ones add 0
-              const float rk = __fmaf_rn(d2 - ptrmin, ONE ? vdr21 : tv.vdr2[p1], 1.0f);
-              int kk = (int)rk;
-              kk = kk < 1 ? 1 : (kk > ptsize ? ptsize : kk);
-              const float w = rk - (float)kk;
-              const int base = p1 * T + kk - 1;
-              const float2 F = tv.tF2[base];
-              const float df = ok ? __fdividef(__fmaf_rn(w, F.y - F.x, F.x), d2) : 0.f;
-              ax = __fmaf_rn(r0, df, ax);
-              ay = __fmaf_rn(r1, df, ay);
-              az = __fmaf_rn(r2, df, az);
-              if (cu && ok) {
-                const float2 Pp = tv.tP2[base];
-                ape += __fmaf_rn(w, Pp.y - Pp.x, Pp.x);
-              }
-              if (cv) {
-                const float r0d = r0 * df, r1d = r1 * df;
-                av0 = __fmaf_rn(r0d, r0, av0);
-                av1 = __fmaf_rn(r1d, r1, av1);
-                av2 = __fmaf_rn(r2 * df, r2, av2);
-                av3 = __fmaf_rn(r0d, r1, av3);
-                av4 = __fmaf_rn(r0d, r2, av4);
-                av5 = __fmaf_rn(r1d, r2, av5);
+              for (int q = 0; q < GATHER; ++q) {
+                const int pt = ONE ? 1 : pmr[(tw_type(pj[q].w) - 1) * ntypes];
+                const int p1 = ONE ? 0 : (pt > 0 ? pt - 1 : 0);
+                const float4 prm = ONE ? pp1 : pair_params<STAB>(tv, p1);
+                // minimum image by 32-bit wrap-around of the fixed-point difference
+                const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj[q].x) * sb0;
+                const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj[q].y) * sb1;
+                const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj[q].z) * sb2;
+                const float d2 = __fmaf_rn(r0, r0, __fmaf_rn(r1, r1, __fmul_rn(r2, r2)));
+                const bool live = qq[h + q] >= 0 && pt > 0;
+                const bool ok = live && d2 <= prm.x;
+                nm |= (live && d2 > prm.x && d2 <= prm.y) ? (1u << (h + q)) : 0u;
+                // branch-free: every lane evaluates the pair, excluded ones add 0
+                const float rk = __fmaf_rn(d2 - ptrmin, prm.z, 1.0f);
+                int kk = (int)rk;
+                kk = kk < 1 ? 1 : (kk > ptsize ? ptsize : kk);
+                const float w = rk - (float)kk;
+                const int base = p1 * T + kk - 1;
+                const float2 F = tv.tF2[base];
+                const float df = ok ? __fdividef(__fmaf_rn(w, F.y - F.x, F.x), d2) : 0.f;
+                ax = __fmaf_rn(r0, df, ax);
+                ay = __fmaf_rn(r1, df, ay);
+                az = __fmaf_rn(r2, df, az);
+                if (cu && ok) {
+                  const float2 Pp = tv.tP2[base];
+                  ape += __fmaf_rn(w, Pp.y - Pp.x, Pp.x);
+                }
+                if (cv) {
+                  const float r0d = r0 * df, r1d = r1 * df;
+                  av0 = __fmaf_rn(r0d, r0, av0);
+                  av1 = __fmaf_rn(r1d, r1, av1);
+                  av2 = __fmaf_rn(r2 * df, r2, av2);
+                  av3 = __fmaf_rn(r0d, r1, av3);
+                  av4 = __fmaf_rn(r0d, r2, av4);
+                  av5 = __fmaf_rn(r1d, r2, av5);
+                }
               }
             }
-          }
-          if (nm) {
-            // the chunk's entries near the cutoff: compute0's FP64 test
-            // decides (src/nd.f90:283-296), then the same FP32 evaluation
-            const double4 pid = c.pos[i];
-            const double b0 = S->box[0], b1 = S->box[1], b2 = S->box[2];
+            if (nm) {
+              // the chunk's entries near the cutoff: compute0's FP64 test
+              // decides (src/nd.f90:283-296), then the same FP32 evaluation
+              const double4 pid = c.pos[i];
+              const double b0 = S->box[0], b1 = S->box[1], b2 = S->box[2];
 #pragma unroll 1
-            while (nm) {
-              const int q = __ffs(nm) - 1;
-              nm &= nm - 1;
-              const int j = __ldg(nb + (kb + q) * TILE);
-              const int4 pj = c.pfx[j];
-              const int p1 = ONE ? 0 : pmr[(tw_type(pj.w) - 1) * ntypes] - 1;
-              const double4 pjd = c.pos[j];
-              double s0 = pid.x - pjd.x, s1 = pid.y - pjd.y, s2 = pid.z - pjd.z;
-              s0 = s0 - round(s0);
-              s1 = s1 - round(s1);
-              s2 = s2 - round(s2);
-              const double x0 = b0 * s0, x1 = b1 * s1, x2 = b2 * s2;
-              double dd = x0 * x0;
-              dd = dd + x1 * x1;
-              dd = dd + x2 * x2;
-              if (dd > tv.rc2[p1]) continue;
-              const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * sb0;
-              const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * sb1;
-              const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * sb2;
-              const float d2 = __fmaf_rn(r0, r0, __fmaf_rn(r1, r1, __fmul_rn(r2, r2)));
-              const float rk = __fmaf_rn(d2 - ptrmin, ONE ? vdr21 : tv.vdr2[p1], 1.0f);
-              int kk = (int)rk;
-              kk = kk < 1 ? 1 : (kk > ptsize ? ptsize : kk);
-              const float w = rk - (float)kk;
-              const int base = p1 * T + kk - 1;
-              const float2 F = tv.tF2[base];
-              const float df = __fdividef(__fmaf_rn(w, F.y - F.x, F.x), d2);
-              ax = __fmaf_rn(r0, df, ax);
-              ay = __fmaf_rn(r1, df, ay);
-              az = __fmaf_rn(r2, df, az);
-              if (cu) {
-                const float2 Pp = tv.tP2[base];
-                ape += __fmaf_rn(w, Pp.y - Pp.x, Pp.x);
-              }
-              if (cv) {
-                const float r0d = r0 * df, r1d = r1 * df;
-                av0 = __fmaf_rn(r0d, r0, av0);
-                av1 = __fmaf_rn(r1d, r1, av1);
-                av2 = __fmaf_rn(r2 * df, r2, av2);
-                av3 = __fmaf_rn(r0d, r1, av3);
-                av4 = __fmaf_rn(r0d, r2, av4);
-                av5 = __fmaf_rn(r1d, r2, av5);
+              while (nm) {
+                const int q = __ffs(nm) - 1;
+                nm &= nm - 1;
+                const int j = __ldg(nb + (kb + q) * TILE);
+                const int4 pj = c.pfx[j];
+                const int p1 = ONE ? 0 : pmr[(tw_type(pj.w) - 1) * ntypes] - 1;
+                const double4 pjd = c.pos[j];
+                double s0 = pid.x - pjd.x, s1 = pid.y - pjd.y, s2 = pid.z - pjd.z;
+                s0 = s0 - round(s0);
+                s1 = s1 - round(s1);
+                s2 = s2 - round(s2);
+                const double x0 = b0 * s0, x1 = b1 * s1, x2 = b2 * s2;
+                double dd = x0 * x0;
+                dd = dd + x1 * x1;
+                dd = dd + x2 * x2;
+                if (dd > tv.rc2[p1]) continue;
+                const float4 prm = ONE ? pp1 : pair_params<STAB>(tv, p1);
+                const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * sb0;
+                const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * sb1;
+                const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * sb2;
+                const float d2 = __fmaf_rn(r0, r0, __fmaf_rn(r1, r1, __fmul_rn(r2, r2)));
+                const float rk = __fmaf_rn(d2 - ptrmin, prm.z, 1.0f);
+                int kk = (int)rk;
+                kk = kk < 1 ? 1 : (kk > ptsize ? ptsize : kk);
+                const float w = rk - (float)kk;
+                const int base = p1 * T + kk - 1;
+                const float2 F = tv.tF2[base];
+                const float df = __fdividef(__fmaf_rn(w, F.y - F.x, F.x), d2);
+                ax = __fmaf_rn(r0, df, ax);
+                ay = __fmaf_rn(r1, df, ay);
+                az = __fmaf_rn(r2, df, az);
+                if (cu) {
+                  const float2 Pp = tv.tP2[base];
+                  ape += __fmaf_rn(w, Pp.y - Pp.x, Pp.x);
+                }
+                if (cv) {
+                  const float r0d = r0 * df, r1d = r1 * df;
+                  av0 = __fmaf_rn(r0d, r0, av0);
+                  av1 = __fmaf_rn(r1d, r1, av1);
+                  av2 = __fmaf_rn(r2 * df, r2, av2);
+                  av3 = __fmaf_rn(r0d, r1, av3);
+                  av4 = __fmaf_rn(r0d, r2, av4);
+                  av5 = __fmaf_rn(r1d, r2, av5);
+                }
               }
             }
+            qx += __float2ll_rn(ax * (float)FORCE_FX);
+            qy += __float2ll_rn(ay * (float)FORCE_FX);
+            qz += __float2ll_rn(az * (float)FORCE_FX);
+            if (EV) {
+              unsigned long long *q = evq + threadIdx.x;
+              q[0] += (unsigned long long)__float2ll_rn(ape * (float)FORCE_FX);
+              q[NT] += (unsigned long long)__float2ll_rn(av0 * (float)FORCE_FX);
+              q[2 * NT] += (unsigned long long)__float2ll_rn(av1 * (float)FORCE_FX);
+              q[3 * NT] += (unsigned long long)__float2ll_rn(av2 * (float)FORCE_FX);
+              q[4 * NT] += (unsigned long long)__float2ll_rn(av3 * (float)FORCE_FX);
+              q[5 * NT] += (unsigned long long)__float2ll_rn(av4 * (float)FORCE_FX);
+              q[6 * NT] += (unsigned long long)__float2ll_rn(av5 * (float)FORCE_FX);
+            }
           }
-          qx += __float2ll_rn(ax * (float)FORCE_FX);
-          qy += __float2ll_rn(ay * (float)FORCE_FX);
-          qz += __float2ll_rn(az * (float)FORCE_FX);
-          if (EV) {
-            qpe += __float2ll_rn(ape * (float)FORCE_FX);
-            qv[0] += __float2ll_rn(av0 * (float)FORCE_FX);
-            qv[1] += __float2ll_rn(av1 * (float)FORCE_FX);
-            qv[2] += __float2ll_rn(av2 * (float)FORCE_FX);
-            qv[3] += __float2ll_rn(av3 * (float)FORCE_FX);
-            qv[4] += __float2ll_rn(av4 * (float)FORCE_FX);
-            qv[5] += __float2ll_rn(av5 * (float)FORCE_FX);
-          }
-        }
+        };
+        if (one) loop(std::true_type{});
+        else loop(std::false_type{});
       }
     }
     if (!MIXED) {
@@ -1488,13 +1636,15 @@ __global__ __launch_bounds__(TILE * TPA) void k_pair(DevCtx c, int host_flags, i
     // end-of-step epilogue
     const bool ck = FUSE && (flags & F_CK);
     if (EV && MIXED) {
-      // exact integer sums: warp butterfly, then one shared atomic per warp
-      long long v7[7] = {qpe, qv[0], qv[1], qv[2], qv[3], qv[4], qv[5]};
+      // exact integer sums: the thread's slots, a warp butterfly, then one
+      // shared atomic per warp; the slots start the next tile at zero
 #pragma unroll
       for (int k = 0; k < 7; ++k) {
+        long long v = (long long)evq[k * NT + threadIdx.x];
+        evq[k * NT + threadIdx.x] = 0ull;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v7[k] += __shfl_xor_sync(0xffffffffu, v7[k], o);
-        if ((threadIdx.x & 31) == 0) atomicAdd(&s_q[k], (unsigned long long)v7[k]);
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&s_q[k], (unsigned long long)v);
       }
     }
     if (la == 0) {
@@ -1546,6 +1696,12 @@ __global__ __launch_bounds__(TILE * TPA) void k_pair(DevCtx c, int host_flags, i
   }
 }
 
+// ---------------------------------------------------------------------------
+// launchers
+void launch_integrate1(const DevCtx &c, cudaStream_t st, int standalone, int mixed) {
+  k_integrate1<<<c.nchunks, BLOCK, 0, st>>>(c, standalone, mixed);
+}
+
 static int sm_count() {
   static int n = 0;
   if (!n) {
@@ -1557,16 +1713,10 @@ static int sm_count() {
   return n;
 }
 
-// ---------------------------------------------------------------------------
-// launchers
-void launch_integrate1(const DevCtx &c, cudaStream_t st, int standalone, int mixed) {
-  k_integrate1<<<c.nchunks, BLOCK, 0, st>>>(c, standalone, mixed);
-}
-
-template <int TPA, bool MIXED, bool FUSE, int MODE, bool EV>
+template <int TPA, bool MIXED, bool FUSE, bool STAB, bool EV>
 static void pair_go(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh) {
-  auto kern = k_pair<TPA, MIXED, FUSE, MODE, EV>;
-  const int smem = MODE ? c.stab_smem : 0;
+  auto kern = k_pair<TPA, MIXED, FUSE, STAB, EV>;
+  const int smem = (STAB ? c.stab_smem : 0) + ((MIXED && EV) ? 7 * 8 * TILE * TPA : 0);
   static int cfg_smem = -1, occ = 0;
   if (smem != cfg_smem) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -1583,23 +1733,22 @@ static void pair_go(const DevCtx &c, cudaStream_t st, int hf, unsigned long long
 // FUSE (a dynamics step): the kernel without energy/virial takes the
 // systems whose step needs neither, then the EV kernel the others; each
 // skips the other's tiles.  Standalone compute0: the host flags choose.
-template <int TPA, bool MIXED, bool FUSE, int MODE>
+template <int TPA, bool MIXED, bool FUSE, bool STAB>
 static void pair_ev(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh) {
   if (FUSE) {
-    pair_go<TPA, MIXED, FUSE, MODE, false>(c, st, hf, nh);
-    pair_go<TPA, MIXED, FUSE, MODE, true>(c, st, hf, nh);
+    pair_go<TPA, MIXED, FUSE, STAB, false>(c, st, hf, nh);
+    pair_go<TPA, MIXED, FUSE, STAB, true>(c, st, hf, nh);
   } else if (hf & (F_CU | F_CV)) {
-    pair_go<TPA, MIXED, FUSE, MODE, true>(c, st, hf, nh);
+    pair_go<TPA, MIXED, FUSE, STAB, true>(c, st, hf, nh);
   } else {
-    pair_go<TPA, MIXED, FUSE, MODE, false>(c, st, hf, nh);
+    pair_go<TPA, MIXED, FUSE, STAB, false>(c, st, hf, nh);
   }
 }
 
 template <int TPA, bool MIXED, bool FUSE>
 static void pair_mode(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh) {
-  if (c.stab_smem <= 0) pair_ev<TPA, MIXED, FUSE, 0>(c, st, hf, nh);
-  else if (c.one_pair) pair_ev<TPA, MIXED, FUSE, 2>(c, st, hf, nh);
-  else pair_ev<TPA, MIXED, FUSE, 1>(c, st, hf, nh);
+  if (c.stab_smem <= 0) pair_ev<TPA, MIXED, FUSE, false>(c, st, hf, nh);
+  else pair_ev<TPA, MIXED, FUSE, true>(c, st, hf, nh);
 }
 
 template <int TPA>
@@ -1664,14 +1813,18 @@ void launch_rebuild(const DevCtx &c, cudaStream_t st, int counting, int mixed) {
   k_build<<<gtile, NBT, c.nb_smem, st>>>(c);
 }
 
-void launch_begin_run(const DevCtx &c, cudaStream_t st, int nsys_cap, int nsteps, int cont) {
-  (void)nsys_cap;
-  k_begin_run<<<(nsys_cap + 127) / 128, 128, 0, st>>>(c, nsys_cap, nsteps, cont);
+void launch_arm(const DevCtx &c, cudaStream_t st, int nsys_cap, int sys, int nsteps, int start) {
+  k_arm<<<(nsys_cap + 127) / 128, 128, 0, st>>>(c, nsys_cap, sys, nsteps, start);
 }
 
-void launch_flush(const DevCtx &c, cudaStream_t st, int nsys_cap) {
-  k_flush<<<c.nchunks, BLOCK, 0, st>>>(c);
-  k_clear_pend<<<(nsys_cap + 127) / 128, 128, 0, st>>>(c, nsys_cap);
+void launch_begin_block(const DevCtx &c, cudaStream_t st, int nsys_cap, int K) {
+  k_begin_block<<<(nsys_cap + 127) / 128, 128, 0, st>>>(c, nsys_cap, K);
+}
+
+// apply and clear the pending velocity scales of every system (sys < 0) or one
+void launch_flush(const DevCtx &c, cudaStream_t st, int nsys_cap, int sys) {
+  k_flush<<<c.nchunks, BLOCK, 0, st>>>(c, sys);
+  k_clear_pend<<<(nsys_cap + 127) / 128, 128, 0, st>>>(c, nsys_cap, sys);
 }
 
 void launch_check(const DevCtx &c, cudaStream_t st, int nsys_cap) {

@@ -22,10 +22,7 @@ struct DevCtx {
   int *gid;
   int *nbr;  // blocked neighbour list (128-atom tiles), atom slots
   int *nnb;
-  int *tile_nc, *tile_cell, *tile_coff;  // per 128-atom tile: cells staged by the build
   int *tile_rows;  // per tile: rows of its list in use (L2 prefetch size)
-  int cand_cap;  // candidates a tile may stage in the pair kernel
-  int one_pair;  // every system has one type and one pair potential
   int *atom_cell, *atom_slot, *cell_count, *cell_start;
   int *perm, *tmp_src, *tmp_key;
   double4 *s_pos;
@@ -55,8 +52,9 @@ void launch_pair(const DevCtx &c, cudaStream_t st, int tpa, int mixed, int fuse,
 void launch_decide(const DevCtx &c, cudaStream_t st, unsigned long long h);
 void launch_integrate2(const DevCtx &c, cudaStream_t st, int ck);
 void launch_rebuild(const DevCtx &c, cudaStream_t st, int counting, int mixed);
-void launch_begin_run(const DevCtx &c, cudaStream_t st, int nsys_cap, int nsteps, int cont);
-void launch_flush(const DevCtx &c, cudaStream_t st, int nsys_cap);
+void launch_arm(const DevCtx &c, cudaStream_t st, int nsys_cap, int sys, int nsteps, int start);
+void launch_begin_block(const DevCtx &c, cudaStream_t st, int nsys_cap, int K);
+void launch_flush(const DevCtx &c, cudaStream_t st, int nsys_cap, int sys);
 void launch_check(const DevCtx &c, cudaStream_t st, int nsys_cap);
 void launch_scale_vel(const DevCtx &c, cudaStream_t st, int sys, double lam);
 void launch_refresh_pfx(const DevCtx &c, cudaStream_t st);
@@ -65,8 +63,9 @@ void launch_refresh_pfx(const DevCtx &c, cudaStream_t st);
 // pair kernel: pair matrix, per-pair cutoffs/scales, then the F and P tables
 NDG_HD int stab_bytes(int ntypes, int npairs, int ptsize) {
   int b = (ntypes * ntypes * 4 + 15) / 16 * 16;
-  b += npairs * 16;  // rc2 (double) + rc2f + vdr2
+  b += npairs * 8;  // rc2 (double)
   b = (b + 15) / 16 * 16;
+  b += npairs * 16;  // packed float4 per pair
   b += npairs * (ptsize + 1) * 16;  // F and P: a double each, or a float2 each
   return b;
 }

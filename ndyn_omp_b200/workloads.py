@@ -168,3 +168,10 @@ def add_to_context(ctx, spec, precision_tables=None):
                          vel=spec.get("vel"))
     ctx.set_control(sid, **spec["control"])
     return sid
+
+
+def submit_to_server(srv, spec, nsteps=None):
+    """Queue a workload dict on a Server; returns its ticket."""
+    return srv.submit(spec["masses"], spec["pairs"], spec["typ"], spec["pos"], spec["box"],
+                      int(nsteps if nsteps is not None else spec["steps"]), vel=spec.get("vel"),
+                      **spec["control"])

@@ -303,3 +303,27 @@ def test_autotune_restores_state(specs):
         assert np.array_equal(a, b)
     assert res[0][1] == res[1][1]
     assert res[0][2] == res[1][2]
+
+
+@pytest.mark.parametrize("quirk", ["ref", "fixed"])
+def test_direct_build_coarse_cells(quirk):
+    """A 12 A list radius on a 36 A box: a 3x3x3 cell grid, ~4000 candidates
+    per tile and lists of ~800, beyond the staged build's shared buffers.
+    The direct build path must give the same cells, pairs and forces."""
+    spec = W.cu_crystal(10, 300.0, seed=51, quirk=quirk)
+    spec = _jitter(spec, 0.05, 52)
+    spec["control"] = dict(spec["control"], skin=6.0)
+    o = oracle_from_spec(spec)
+    assert o.setup_lists() == 0
+    o.compute0(1, 1)
+    fo, peo, _, _ = o.forces()
+    with nd.Context(0, "fp64") as ctx:
+        sid = gpu_from_spec(ctx, spec)
+        ctx.setup_lists()
+        assert list(ctx.mcell(sid)) == [3, 3, 3]
+        assert np.array_equal(ctx.cells(sid), o.cells())
+        assert np.array_equal(pair_multiset(ctx.neighbors(sid)), pair_multiset(o.neighbors()))
+        ctx.compute0(True, True)
+        fg, peg, _, _ = ctx.forces(sid)
+    assert rel_l2(fg, fo) < 1e-12
+    assert abs(peg - peo) <= 1e-12 * abs(peo)
