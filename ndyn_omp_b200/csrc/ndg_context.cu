@@ -128,7 +128,7 @@ struct ndg_ctx {
   int tpa = 0, graph_steps = 100;
   int stab_smem = 0;  // staged-table bytes of the pair kernel (0: tables from global)
   int nb_smem = 0;  // neighbour-build dynamic smem
-  int nb_maxnb = 8, nb_vcap = 8192;
+  int nb_vcap = 4096;
   std::map<int, cudaGraphExec_t> graphs;
   int captures = 0;  // graphs captured (a changed arena or layout drops them)
   // per-kernel timing of the last profiled block
@@ -182,7 +182,6 @@ DevCtx devctx(ndg_ctx *c) {
   d.gid = c->gid;
   d.nbr = c->nbr;
   d.tile_rows = c->tile_rows;
-  d.nb_maxnb = c->nb_maxnb;
   d.nb_vcap = c->nb_vcap;
   d.nnb = c->nnb;
   d.atom_cell = c->atom_cell;
@@ -404,17 +403,12 @@ int upload_params(ndg_ctx *c) {
     c->stab_smem = stab;
     drop_graphs(c);
   }
-  // neighbour build: 3072 staged candidates (16 B each), the 16-bit lists
-  // of the tile's 128 atoms, and the runs' flat candidate lists
-  int mx = 8;
-  for (auto &h : c->sys)
-    if (h.alive) mx = std::max(mx, h.maxnb);
-  mx = std::min(mx, 512);  // systems with longer lists build directly
-  const int vcap = 8192;
-  const int nbs = 3072 * 16 + 128 * mx * 2 + vcap * 2;
-  if (nbs != c->nb_smem || mx != c->nb_maxnb) {
+  // neighbour build: 3072 staged candidates (16 B position + 4 B slot each)
+  // and the runs' flat candidate lists (16-bit entries)
+  const int vcap = 4096;
+  const int nbs = 3072 * (16 + 4) + vcap * 2;
+  if (nbs != c->nb_smem) {
     c->nb_smem = nbs;
-    c->nb_maxnb = mx;
     c->nb_vcap = vcap;
     drop_graphs(c);
   }

@@ -735,7 +735,7 @@ constexpr int TC_MAX = 256;    // link cells a tile may stage
 constexpr int HSLOTS = 1024;   // shared hash slots for the tile's cell set
 constexpr float NB_MARGIN = 1e-5f;
 constexpr int BUILD_CAP = 3072;  // candidates the build stages per tile
-constexpr int NBT = 512;         // threads of the build CTA (16 warps)
+constexpr int NBT = 256;         // threads of the build CTA (8 warps)
 
 __device__ __forceinline__ int stencil_cell(int cl, int st, int M0, int M1, int M2) {
   const int cx = cl % M0, cy = (cl / M0) % M1, cz = cl / (M0 * M1);
@@ -798,6 +798,24 @@ __device__ __forceinline__ bool nb_hit(const DevCtx &c, const SysParam *P, const
   const bool near_cut = fabsf(d2f - rlf) <= NB_MARGIN * rlf;
   const bool near_min = center && d2f >= ptrlo && d2f <= ptrhi;
   if (!(near_cut || near_min)) return !(center && d2f < ptrlo) && d2f < rlf;
+  double s0 = pid.x - pjd.x, s1 = pid.y - pjd.y, s2 = pid.z - pjd.z;
+  s0 = s0 - round(s0);
+  s1 = s1 - round(s1);
+  s2 = s2 - round(s2);
+  const double x0 = b0 * s0, x1 = b1 * s1, x2 = b2 * s2;
+  double d2 = x0 * x0;
+  d2 = d2 + x1 * x1;
+  d2 = d2 + x2 * x2;
+  return !(center && d2 < ptrmin) && !(d2 > rl);
+}
+
+// the reference's FP64 list test for one candidate (src/nd.f90:1362-1377,
+// 1419-1420): out of line, the build loop calls it only for the rare
+// candidates within NB_MARGIN of the list radius or of PTrMin
+__device__ __noinline__ bool nb_exact(const DevCtx &c, double4 pid, int j, bool center,
+                                      double rl, double ptrmin, double b0, double b1,
+                                      double b2) {
+  const double4 pjd = c.pos[j];
   double s0 = pid.x - pjd.x, s1 = pid.y - pjd.y, s2 = pid.z - pjd.z;
   s0 = s0 - round(s0);
   s1 = s1 - round(s1);
@@ -886,8 +904,8 @@ __device__ void build_tile(const DevCtx &c, int sys, int tile) {
   const int ne = S->nstencil;
   const int maxnb = P->maxnb;
   int4 *cpf = (int4 *)dsm;                                   // BUILD_CAP candidates
-  unsigned short *lst = (unsigned short *)(cpf + BUILD_CAP);  // TILE * maxnb
-  unsigned short *vlist = lst + TILE * c.nb_maxnb;             // flat per-run lists
+  int *cgid = (int *)(cpf + BUILD_CAP);                       // their atom slots
+  unsigned short *vlist = (unsigned short *)(cgid + BUILD_CAP);  // flat per-run lists
   const int vcap = c.nb_vcap;
   __shared__ int hset[HSLOTS];
   __shared__ int ucell[TC_MAX + 1], coff[TC_MAX + 1], ustart[TC_MAX];
@@ -901,14 +919,7 @@ __device__ void build_tile(const DevCtx &c, int sys, int tile) {
   __shared__ int nu, bad, nruns, rows_s;
   __shared__ int pm_s[16 * 16];
   __shared__ int scan_w[NBT / 32];
-  if (maxnb > c.nb_maxnb) {
-    // lists longer than the shared list buffer holds
-    if (threadIdx.x < ne) stc[threadIdx.x] = S->stencil[threadIdx.x];
-    __syncthreads();
-    build_tile_direct(c, sys, tile, stc, ne, ncnt, &rows_s);
-    return;
-  }
-  __shared__ float rl2f_s[136];
+  __shared__ float2 rlb_s[136];  // FP32 band (1 -+ NB_MARGIN) of each pair's rlist^2
   __shared__ double rl2_s[136];
   const int nt = P->ntypes, npr = P->npairs;
   const bool small = nt <= 16 && npr <= 136;
@@ -923,7 +934,8 @@ __device__ void build_tile(const DevCtx &c, int sys, int tile) {
     for (int k = threadIdx.x; k < nt * nt; k += NBT) pm_s[k] = c.pairmat[P->pm_off + k];
     for (int k = threadIdx.x; k < npr; k += NBT) {
       rl2_s[k] = c.rlist2[P->pair_off + k];
-      rl2f_s[k] = (float)rl2_s[k];
+      const float r = (float)rl2_s[k];
+      rlb_s[k] = make_float2(r * (1.f - NB_MARGIN), r * (1.f + NB_MARGIN));
     }
   }
   __syncthreads();
@@ -950,7 +962,7 @@ __device__ void build_tile(const DevCtx &c, int sys, int tile) {
     }
   }
   __syncthreads();
-  if (nu > TC_MAX) bad = 1;
+  if (threadIdx.x == 0 && nu >= TC_MAX) bad = 1;  // the scan below sets coff[nu] by thread nu
   __syncthreads();
   if (!bad) {
     // compact and sort the cell ids (bitonic over TC_MAX slots)
@@ -1003,6 +1015,7 @@ __device__ void build_tile(const DevCtx &c, int sys, int tile) {
     for (int e = threadIdx.x & 31; e < len; e += 32) {
       const double4 p = c.pos[j0 + e];
       cpf[q0 + e] = make_int4(fx32(p.x), fx32(p.y), fx32(p.z), tw_of(p.w));
+      cgid[q0 + e] = j0 + e;
     }
   }
   __syncthreads();
@@ -1057,7 +1070,9 @@ __device__ void build_tile(const DevCtx &c, int sys, int tile) {
   }
   __syncthreads();
   const int *__restrict__ pmg = pm;
-  const bool one = nt == 1 && npr == 1;
+  const bool one = nt == 1 && npr == 1 && pm[0] == 1;
+  const float2 band1 = one ? rlb_s[0] : make_float2(0.f, 0.f);
+  int *dst = c.nbr + P->nbr_off + (long long)(local0 / TILE) * maxnb * TILE;
   for (int rb = 0; rb < nruns;) {
     // the runs whose lists fit the buffer together
     __shared__ int re_s;
@@ -1083,67 +1098,59 @@ __device__ void build_tile(const DevCtx &c, int sys, int tile) {
       for (int k = lane; k < len; k += 32) dst[k] = (unsigned short)(q0 + k) | cflag;
     }
     __syncthreads();
-    // 3. one warp per own atom, 32 candidates of the flat list per pass
+    // 3. one warp per own atom, 32 candidates of the flat list per pass;
+    // hits go straight to the atom's column of the blocked list
     for (int t = run_t0[rb] + warp; t < run_t0[re]; t += NBT / 32) {
       const int i = a0 + t;
       const int r = run_of[t];
       const double4 pid = c.pos[i];
       const int4 pi = make_int4(fx32(pid.x), fx32(pid.y), fx32(pid.z), tw_of(pid.w));
       const int ti = tw_type(pi.w);
-      // the atom's own slot among the staged candidates
-      const int uo = find_cell(ucell, U, run_cell[r]);
-      const int qi = coff[uo] + (i - (P->atom_off + ustart[uo]));
       const unsigned short *vl = vlist + vstart[r];
       const int V = vsize[r];
-      unsigned short *mylst = lst + t * maxnb;
       int cnt = 0;
       for (int vb = 0; vb < V; vb += 32) {
         const int v = vb + lane;
-        bool hit = false;
-        int q = 0;
+        bool hit = false, unsure = false, center = false;
+        int q = 0, mx = 1;
         if (v < V) {
           const unsigned short raw = vl[v];
           q = raw & 0x7fff;
-          const bool center = raw >> 15;
+          center = raw >> 15;
           const int4 pj = cpf[q];
-          int mx = 1;
           if (!one) {
             const int tj = tw_type(pj.w);
             const int a = pmg[(ti - 1) + (tj - 1) * nt];
             const int b = pmg[(tj - 1) + (ti - 1) * nt];
             mx = a > b ? a : b;
           }
-          if (q != qi && mx > 0) {
-            const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * sb0;
-            const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * sb1;
-            const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * sb2;
-            const float d2f = r0 * r0 + r1 * r1 + r2 * r2;
-            const float rlf = small ? rl2f_s[mx - 1] : (float)c.rlist2[P->pair_off + mx - 1];
-            const bool near_cut = fabsf(d2f - rlf) <= NB_MARGIN * rlf;
-            const bool near_min = center && d2f >= ptrlo && d2f <= ptrhi;
-            if (near_cut || near_min) {
-              // the reference's FP64 test (src/nd.f90:1362-1377)
-              const int u = find_cell(coff + 1, U, q + 1);
-              const double4 pjd = c.pos[P->atom_off + ustart[u] + (q - coff[u])];
-              double s0 = pid.x - pjd.x, s1 = pid.y - pjd.y, s2 = pid.z - pjd.z;
-              s0 = s0 - round(s0);
-              s1 = s1 - round(s1);
-              s2 = s2 - round(s2);
-              const double x0 = b0 * s0, x1 = b1 * s1, x2 = b2 * s2;
-              double d2 = x0 * x0;
-              d2 = d2 + x1 * x1;
-              d2 = d2 + x2 * x2;
-              const double rl = small ? rl2_s[mx - 1] : c.rlist2[P->pair_off + mx - 1];
-              hit = !(center && d2 < ptrmin) && !(d2 > rl);
+          const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * sb0;
+          const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * sb1;
+          const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * sb2;
+          const float d2f = r0 * r0 + r1 * r1 + r2 * r2;
+          const bool live = cgid[q] != i && mx > 0;
+          float2 band = band1;
+          if (!one && live) {
+            if (small) {
+              band = rlb_s[mx - 1];
             } else {
-              hit = !(center && d2f < ptrlo) && d2f < rlf;
+              const float rf = (float)c.rlist2[P->pair_off + mx - 1];
+              band = make_float2(rf * (1.f - NB_MARGIN), rf * (1.f + NB_MARGIN));
             }
           }
+          // outside both margins FP32 decides; inside either, FP64 does
+          hit = live && d2f < band.x && !(center && d2f < ptrhi);
+          unsure = live && ((d2f >= band.x && d2f <= band.y) ||
+                            (center && d2f >= ptrlo && d2f <= ptrhi));
+        }
+        if (__any_sync(0xffffffffu, unsure) && unsure) {
+          const double rl = small ? rl2_s[mx - 1] : c.rlist2[P->pair_off + mx - 1];
+          hit = nb_exact(c, pid, cgid[q], center, rl, ptrmin, b0, b1, b2);
         }
         const unsigned bal = __ballot_sync(0xffffffffu, hit);
         if (hit) {
           const int k = cnt + __popc(bal & ((1u << lane) - 1u));
-          if (k < maxnb) mylst[k] = (unsigned short)q;
+          if (k < maxnb) dst[k * TILE + t] = cgid[q];
         }
         cnt += __popc(bal);
       }
@@ -1157,7 +1164,7 @@ __device__ void build_tile(const DevCtx &c, int sys, int tile) {
     build_tile_direct(c, sys, tile, stc, ne, ncnt, &rows_s);
     return;
   }
-  // 4. write the tile's lists row by row (consecutive threads, consecutive atoms)
+  // 4. the tile's row count (longest list) and each atom's count
   if (threadIdx.x == 0) rows_s = 0;
   __syncthreads();
   if (threadIdx.x < TILE) {
@@ -1165,25 +1172,14 @@ __device__ void build_tile(const DevCtx &c, int sys, int tile) {
     if ((threadIdx.x & 31) == 0) atomicMax(&rows_s, r);
   }
   __syncthreads();
-  const int rows = rows_s;
-  int *dst = c.nbr + P->nbr_off + (long long)(local0 / TILE) * maxnb * TILE;
-  for (int idx = threadIdx.x; idx < rows * TILE; idx += NBT) {
-    const int k = idx / TILE, t = idx - k * TILE;
-    if (t < nown && k < min(ncnt[t], maxnb)) {
-      // staged candidate -> its atom slot
-      const int q = lst[t * maxnb + k];
-      const int u = find_cell(coff + 1, U, q + 1);
-      dst[k * TILE + t] = P->atom_off + ustart[u] + (q - coff[u]);
-    }
-  }
-  if (threadIdx.x == 0) c.tile_rows[tile] = rows;
+  if (threadIdx.x == 0) c.tile_rows[tile] = rows_s;
   if (threadIdx.x < nown) {
     c.nnb[a0 + threadIdx.x] = ncnt[threadIdx.x];
     if (ncnt[threadIdx.x] > maxnb) set_err(c, S, E_NEIMAX);
   }
 }
 
-__global__ __launch_bounds__(NBT) void k_build(DevCtx c) {
+__global__ __launch_bounds__(NBT, 2) void k_build(DevCtx c) {
   for_listed(c,
              [&](int s, int &f, int &n) {
                f = c.P[s].atom_off / TILE;

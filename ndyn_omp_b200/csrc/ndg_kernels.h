@@ -15,7 +15,7 @@ struct DevCtx {
   int nchunks, ncells, nsys_cap;
   int stab_smem;  // shared-memory bytes of the staged pair tables, 0 = read from global
   int nb_smem;  // neighbour build dynamic smem
-  int nb_maxnb, nb_vcap;  // its per-atom list size and flat candidate-list capacity
+  int nb_vcap;  // flat candidate-list capacity of the build
   double4 *pos;
   int4 *pfx;
   double *vel, *acc, *disp, *force;
