@@ -1,0 +1,449 @@
+// ndyn_main.cpp -- directive-script driver over the C ABI: the host program
+// that replaces Ndyn's Fortran main loop where no Fortran compiler exists.
+//
+//   ndyn_gpu [--mixed] [--fixed] [--device N] < input.sh
+//
+// Reads an Ndyn directive script on stdin from START (read_input,
+// src/read_input.f90:2-219): Types, Pairs, Model (dump/xyz,
+// src/read_input.f90:277-392), BoxSize, Skin, NeiMax, ReNeighbor,
+// Isokinetic/Isoenergetic/Isobaric and their Aniso* forms, BoxVel /
+// StopBoxVel, Velocity / Seed, OutFreq, StepNumber, Print and Run, and
+// prints the reference's write_thermo lines (src/read_input.f90:433-446).
+// Every Run is one call of ndg_run (the dynamics prologue and loop,
+// src/nd.f90:60-199) on the GPU.  --mixed selects NDG_PREC_MIXED, --fixed
+// the corrected list semantics.
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ndyn_gpu.h"
+
+namespace {
+
+std::vector<std::string> split(const std::string &line) {
+  std::vector<std::string> w;
+  size_t p = 0;
+  while (p < line.size()) {
+    while (p < line.size() && std::strchr(" \t\r\n", line[p])) ++p;
+    if (p >= line.size()) break;
+    size_t q = p;
+    while (q < line.size() && !std::strchr(" \t\r\n", line[q])) ++q;
+    w.push_back(line.substr(p, q - p));
+    p = q;
+  }
+  return w;
+}
+
+std::string strip_comment(const std::string &s) {
+  const size_t h = s.find('#');
+  return h == std::string::npos ? s : s.substr(0, h);
+}
+
+// Fortran list-directed logical: optional '.', then T/t or F/f
+bool parse_logical(const std::string &v) {
+  size_t k = v.size() && v[0] == '.' ? 1 : 0;
+  return k < v.size() && (v[k] == 'T' || v[k] == 't');
+}
+
+// Fortran G14.6 (write_thermo, src/read_input.f90:440)
+std::string g14_6(double x) {
+  char buf[64];
+  if (x == 0.0) {
+    std::snprintf(buf, sizeof buf, "%10s    ", std::signbit(x) ? "-0.00000" : "0.00000");
+    return buf;
+  }
+  if (!std::isfinite(x)) {
+    std::snprintf(buf, sizeof buf, "%14s", std::isnan(x) ? "NaN" : (x > 0 ? "Infinity" : "-Infinity"));
+    return buf;
+  }
+  char e6[64];
+  std::snprintf(e6, sizeof e6, "%.5e", x);
+  const int ex = std::atoi(std::strchr(e6, 'e') + 1) + 1;  // x = 0.dddddd * 10^ex
+  if (ex >= 0 && ex <= 6) {
+    const int dec = 6 - ex;
+    if (dec > 0) std::snprintf(buf, sizeof buf, "%10.*f    ", dec, x);
+    else std::snprintf(buf, sizeof buf, "%9.0f.    ", x);  // F10.0 keeps the point
+    return buf;
+  }
+  char tmp[64], dig[8];
+  std::snprintf(tmp, sizeof tmp, "%.5e", std::fabs(x));
+  dig[0] = tmp[0];
+  std::memcpy(dig + 1, tmp + 2, 5);
+  dig[6] = 0;
+  char body[64];
+  if (ex >= -99 && ex <= 99)
+    std::snprintf(body, sizeof body, "%s0.%sE%c%02d", x < 0 ? "-" : "", dig, ex < 0 ? '-' : '+',
+                  ex < 0 ? -ex : ex);
+  else
+    std::snprintf(body, sizeof body, "%s0.%s%c%03d", x < 0 ? "-" : "", dig, ex < 0 ? '-' : '+',
+                  ex < 0 ? -ex : ex);
+  std::snprintf(buf, sizeof buf, "%14s", body);
+  return buf;
+}
+
+void thermo_line(const ndg_thermo *t, void *) {
+  std::printf(" %8d %s %s %s %s %s\n", t->step, g14_6(t->potential).c_str(),
+              g14_6(t->kinetic).c_str(), g14_6(t->energy_error).c_str(),
+              g14_6(t->pressure).c_str(), g14_6(t->volume).c_str());
+  std::fflush(stdout);
+}
+
+// Seeded Maxwell-Boltzmann velocities with the reference's semantics
+// (normalVelocityDistribution, src/nd.f90:1598-1621: sigma^2 = 2 kt /
+// (3 m), mean removed).  The reference draws from gfortran's
+// random_number; this driver uses SplitMix64 uniforms and the
+// Kinderman-Monahan ratio-of-uniforms normal, the generator the CPU
+// restatement uses, so both start from the same velocities.
+uint64_t splitmix64(uint64_t *x) {
+  uint64_t z = (*x += 0x9E3779B97F4A7C15ULL);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+
+float uniform(uint64_t *st) {
+  return ((float)(splitmix64(st) >> 40) + 0.5f) * (1.0f / 16777216.0f);
+}
+
+float normal_ratio_of_uniforms(uint64_t *st) {
+  const float s = 0.449871f, t = -0.386595f, a = 0.19600f, b = 0.25472f;
+  const float r1 = 0.27597f, r2 = 0.27846f;
+  for (;;) {
+    const float u = uniform(st);
+    float v = uniform(st);
+    v = 1.7156f * (v - 0.5f);
+    const float x = u - s, y = std::fabs(v) - t;
+    const float q = x * x + y * (a * y - b * x);
+    if (q < r1) return v / u;
+    if (q > r2) continue;
+    if (v * v < -4.0f * std::log(u) * u * u) return v / u;
+  }
+}
+
+struct Driver {
+  int precision = NDG_PREC_FP64, quirk = NDG_QUIRK_REF, device = 0;
+  ndg_ctx *ctx = nullptr;
+  int sys = -1;
+  bool dirty = true;  // host state newer than the device's
+  std::vector<std::string> tname;
+  std::vector<double> mass, charge;
+  // pair tables
+  int npairs = 0, ptsize = 1000;
+  double ptrmin = 0.25;
+  std::vector<int> pairmat;
+  std::vector<double> rcpair, ppair, fpair;
+  // model
+  std::vector<int> typ;
+  std::vector<double> pos, vel, acc;
+  double box[3] = {0, 0, 0};
+  double boxset[3] = {10.0, 10.0, 10.0};
+  std::string model, model_type = "xyz";
+  uint64_t seed = 123456789ULL;
+  ndg_control c{};
+
+  int type_id(const std::string &t) const {
+    for (size_t i = 0; i < tname.size(); ++i)
+      if (tname[i] == t) return (int)i + 1;
+    return 0;
+  }
+
+  // read_model, 'dump' and 'xyz' formats (src/read_input.f90:277-392)
+  bool read_model() {
+    FILE *f = std::fopen(model.c_str(), "r");
+    if (!f) {
+      std::fprintf(stderr, "read_model: ERROR: opening model file: %s\n", model.c_str());
+      return false;
+    }
+    char line[1024];
+    int np = 0;
+    double b[3] = {boxset[0], boxset[1], boxset[2]};
+    const bool dump = model_type == "dump" || model_type == "trj";
+    auto next = [&]() { return std::fgets(line, sizeof line, f) != nullptr; };
+    if (dump) {
+      for (int k = 0; k < 3; ++k) next();
+      next();
+      np = std::atoi(line);
+      next();
+      for (int k = 0; k < 3; ++k) {
+        float lm = 0, lx = 0;
+        next();
+        std::sscanf(line, "%f %f", &lm, &lx);
+        b[k] = (double)(lx - lm);  // real(4) read, src/read_input.f90:334-336
+      }
+      next();
+    } else {
+      next();
+      np = std::atoi(line);
+      next();
+    }
+    typ.assign(np, 0);
+    pos.assign(3 * (size_t)np, 0.0);
+    for (int i = 0; i < np; ++i) {
+      if (!next()) {
+        std::fclose(f);
+        return false;
+      }
+      if (dump) {
+        int id = 0, ty = 0;
+        float x[3] = {0, 0, 0};
+        std::sscanf(line, "%d %d %f %f %f", &id, &ty, &x[0], &x[1], &x[2]);
+        if (id < 1 || id > np) {
+          std::fclose(f);
+          return false;
+        }
+        typ[id - 1] = ty;
+        for (int k = 0; k < 3; ++k) pos[3 * (size_t)(id - 1) + k] = (double)(x[k] - 0.5f);
+      } else {
+        char ct[64];
+        double x[3] = {0, 0, 0};
+        std::sscanf(line, "%63s %lf %lf %lf", ct, &x[0], &x[1], &x[2]);
+        typ[i] = type_id(ct);
+        if (!typ[i]) {
+          std::fprintf(stderr, "ERROR: no atom type defined for atom %d\n", i + 1);
+          std::fclose(f);
+          return false;
+        }
+        for (int k = 0; k < 3; ++k) pos[3 * (size_t)i + k] = x[k] / b[k];
+      }
+    }
+    std::fclose(f);
+    for (int k = 0; k < 3; ++k) box[k] = b[k];
+    vel.assign(3 * (size_t)np, 0.0);
+    acc.assign(3 * (size_t)np, 0.0);  // the first Run starts from acc = 0
+    dirty = true;
+    std::printf("#  read_model: successfully read %8d model nodes.\n", np);
+    return true;
+  }
+
+  // the device state back into the host copies (before a host-side change)
+  bool pull() {
+    if (sys < 0 || dirty) return true;
+    return ndg_get_state(ctx, sys, pos.data(), vel.data(), acc.data(), box) == NDG_OK;
+  }
+
+  void velocity(float kt) {
+    pull();
+    const int np = (int)typ.size();
+    uint64_t st = seed;
+    double vt[3] = {0, 0, 0};
+    for (int i = 0; i < np; ++i) {
+      float nn[3];
+      for (int d = 0; d < 3; ++d) nn[d] = normal_ratio_of_uniforms(&st);
+      const float coeff = std::sqrt(2.0f * kt / (3.0f * (float)mass[typ[i] - 1]));
+      for (int d = 0; d < 3; ++d) {
+        vel[3 * (size_t)i + d] = (double)(nn[d] * coeff);
+        vt[d] += vel[3 * (size_t)i + d];
+      }
+    }
+    for (int d = 0; d < 3; ++d) vt[d] = vt[d] / (double)np;
+    for (int i = 0; i < np; ++i)
+      for (int d = 0; d < 3; ++d) vel[3 * (size_t)i + d] -= vt[d];
+    dirty = true;
+  }
+
+  int run(int nsteps) {
+    int rc = NDG_OK;
+    if (!ctx) {
+      rc = ndg_create(&ctx, device, precision);
+      if (rc) return rc;
+    }
+    if (sys < 0) {
+      rc = ndg_add_system(ctx, (int)typ.size(), (int)mass.size(), npairs, ptsize, ptrmin,
+                          mass.data(), pairmat.data(), rcpair.data(), ppair.data(), fpair.data(),
+                          typ.data(), pos.data(), vel.data(), acc.data(), box, &sys);
+      if (rc) return rc;
+    } else if (dirty) {
+      rc = ndg_load_state(ctx, sys, pos.data(), vel.data(), acc.data(), box);
+      if (rc) return rc;
+    }
+    dirty = false;
+    c.quirk = quirk;
+    rc = ndg_set_control(ctx, sys, &c);
+    if (rc) return rc;
+    rc = ndg_run(ctx, nsteps, thermo_line, nullptr);
+    if (rc) return rc;
+    ndg_control after{};
+    ndg_get_control(ctx, sys, &after);
+    c.step = after.step;  // StepNumber carries over between Runs
+    c.skin = after.skin;  // the default skin, once set, persists (src/nd.f90:77-79)
+    return NDG_OK;
+  }
+};
+
+}  // namespace
+
+int main(int argc, char **argv) {
+  Driver d;
+  ndg_default_control(&d.c);
+  for (int a = 1; a < argc; ++a) {
+    if (!std::strcmp(argv[a], "--mixed")) d.precision = NDG_PREC_MIXED;
+    else if (!std::strcmp(argv[a], "--fixed")) d.quirk = NDG_QUIRK_FIXED;
+    else if (!std::strcmp(argv[a], "--device") && a + 1 < argc) d.device = std::atoi(argv[++a]);
+  }
+  char raw[4096];
+  bool started = false;
+  while (std::fgets(raw, sizeof raw, stdin)) {
+    auto w = split(raw);
+    if (!w.empty() && w[0] == "START") {
+      started = true;
+      break;
+    }
+  }
+  if (!started) {
+    std::fprintf(stderr, "read_input: no START line\n");
+    return 1;
+  }
+  int ln = 0;
+  auto arg = [](const std::vector<std::string> &w, size_t n) -> std::string {
+    return n < w.size() ? w[n] : std::string("0");
+  };
+  while (std::fgets(raw, sizeof raw, stdin)) {
+    ++ln;
+    auto w = split(strip_comment(raw));
+    if (w.empty()) continue;
+    const std::string &k = w[0];
+    if (k == "help" || k == "WritePotentialTable" || k == "ConfOutFreq") {
+      // no output on the timestep path
+    } else if (k == "BoxSize") {
+      for (int q = 0; q < 3; ++q) d.boxset[q] = std::atof(arg(w, q + 1).c_str());
+    } else if (k == "Model") {
+      d.model = arg(w, 1);
+      if (w.size() >= 3) d.model_type = w[2];
+      if (!d.read_model()) return 2;
+    } else if (k == "Seed") {
+      d.seed = std::strtoull(arg(w, 1).c_str(), nullptr, 10);
+    } else if (k == "Velocity") {
+      d.velocity((float)std::atof(arg(w, 1).c_str()));
+    } else if (k == "ReNeibour" || k == "ReNeighbor") {
+      d.c.renei = parse_logical(arg(w, 1));
+      if (w.size() >= 3) d.c.renei_freq = std::atoi(w[2].c_str());
+    } else if (k == "Skin") {
+      d.c.skin = std::atof(arg(w, 1).c_str());
+    } else if (k == "NeiMax") {
+      d.c.neimax = std::atoi(arg(w, 1).c_str());
+    } else if (k == "Types") {
+      const int nt = std::atoi(arg(w, 1).c_str());
+      d.tname.clear();
+      d.mass.clear();
+      d.charge.clear();
+      for (int i = 0; i < nt; ++i) {
+        if (!std::fgets(raw, sizeof raw, stdin)) return 3;
+        auto tw = split(raw);
+        d.tname.push_back(tw.size() > 0 ? tw[0].substr(0, 8) : "");
+        d.mass.push_back(tw.size() > 1 ? std::atof(tw[1].c_str()) : 0.0);
+        d.charge.push_back(tw.size() > 2 ? std::atof(tw[2].c_str()) : 0.0);
+      }
+    } else if (k == "Pairs") {
+      const int np = std::atoi(arg(w, 1).c_str());
+      d.ptrmin = w.size() >= 3 ? std::atof(w[2].c_str()) : 0.25;
+      d.ptsize = w.size() >= 4 ? std::atoi(w[3].c_str()) : 1000;
+      const int nt = (int)d.mass.size();
+      std::vector<char> names(8 * (size_t)np, ' ');
+      std::vector<double> par(4 * (size_t)np, 0.0), q(np, 0.0);
+      d.pairmat.assign((size_t)nt * nt, 0);
+      for (int i = 0; i < np; ++i) {
+        if (!std::fgets(raw, sizeof raw, stdin)) return 3;
+        auto tw = split(strip_comment(raw));
+        const int a = tw.size() > 0 ? d.type_id(tw[0]) : 0;
+        const int b = tw.size() > 1 ? d.type_id(tw[1]) : 0;
+        const bool sym = tw.size() > 2 && tw[2] == "sym";
+        if (tw.size() > 3) std::memcpy(names.data() + 8 * i, tw[3].c_str(), std::min<size_t>(8, tw[3].size()));
+        for (size_t j = 4; j < tw.size() && j < 8; ++j) par[4 * i + (j - 4)] = std::atof(tw[j].c_str());
+        if (!a || !b) {
+          std::fprintf(stderr, "Pairs: unknown type on pair %d\n", i + 1);
+          return 4;
+        }
+        if (!sym) {
+          std::fprintf(stderr, "Pairs: one-sided pairs (compute1) are not on this path\n");
+          return 4;
+        }
+        q[i] = d.charge[a - 1] * d.charge[b - 1];
+        // PairMat(a,b) (column-major), both orders for 'sym' (src/read_input.f90:159-164)
+        d.pairmat[(a - 1) + (size_t)(b - 1) * nt] = i + 1;
+        d.pairmat[(b - 1) + (size_t)(a - 1) * nt] = i + 1;
+      }
+      d.npairs = np;
+      d.ppair.assign((size_t)(d.ptsize + 1) * np, 0.0);
+      d.fpair.assign((size_t)(d.ptsize + 1) * np, 0.0);
+      std::vector<double> rc2(np), dr2(np);
+      const int rc = ndg_build_pair_tables(np, d.ptsize, d.ptrmin, names.data(), par.data(),
+                                           q.data(), d.ppair.data(), d.fpair.data(), rc2.data(),
+                                           dr2.data());
+      if (rc) {
+        std::fprintf(stderr, "Pairs: %s\n", ndg_error_string(rc));
+        return 4;
+      }
+      d.rcpair.assign(np, 0.0);
+      double rcut = 0.0;
+      for (int i = 0; i < np; ++i) {
+        d.rcpair[i] = par[4 * i];
+        rcut = std::max(rcut, par[4 * i]);
+      }
+      std::printf("# Global maximum cutoff radius: %g\n", rcut);
+    } else if (k == "Isokinetic") {
+      d.c.isokinetic = 1;
+      d.c.ke_target = std::atof(arg(w, 1).c_str());
+      d.c.ke_parm = std::atof(arg(w, 2).c_str());
+      if (w.size() >= 4) d.c.ke_freq = std::atoi(w[3].c_str());
+    } else if (k == "Anisokinetic") {
+      d.c.isokinetic = 0;
+    } else if (k == "Isoenergetic") {
+      d.c.isoenergetic = 1;
+      d.c.e_parm = std::atof(arg(w, 1).c_str());
+      if (w.size() >= 3) d.c.e_freq = std::atoi(w[2].c_str());
+    } else if (k == "Anisoenergetic") {
+      d.c.isoenergetic = 0;
+    } else if (k == "Isobaric") {
+      d.c.isobaric = 1;
+      for (int q = 0; q < 3; ++q) d.c.p_target[q] = std::atof(arg(w, q + 1).c_str());
+      d.c.p_parm = std::atof(arg(w, 4).c_str());
+      if (w.size() >= 6) d.c.p_freq = std::atoi(w[5].c_str());
+    } else if (k == "Anisobaric") {
+      d.c.isobaric = 0;
+    } else if (k == "BoxVel") {
+      d.c.box_load = 1;
+      for (int q = 0; q < 3; ++q) d.c.box_vel[q] = std::atof(arg(w, q + 1).c_str());
+    } else if (k == "StopBoxVel") {
+      d.c.box_load = 0;
+    } else if (k == "Exec") {
+      std::printf("# Exec not executed\n");
+    } else if (k == "Print") {
+      const std::string s(raw);
+      std::printf("# %s", s.size() > 6 ? s.c_str() + 6 : "\n");
+    } else if (k == "OutFreq") {
+      d.c.out_steps = std::atoi(arg(w, 1).c_str());
+    } else if (k == "StepNumber") {
+      d.c.step = std::atoi(arg(w, 1).c_str());
+    } else if (k == "Run") {
+      const int nsteps = std::atoi(arg(w, 1).c_str());
+      if (w.size() >= 3) d.c.dt = std::atof(w[2].c_str());
+      if (d.typ.empty() || !d.npairs) {
+        std::fprintf(stderr, "Run: no model or no pairs\n");
+        return 5;
+      }
+      std::printf("#  Step   Potential     Kinetic        EnergyError    pressure       volume\n");
+      const int rc = d.run(nsteps);
+      if (rc) {
+        std::fprintf(stderr, "dynamics: %s (%d) %s\n", ndg_error_string(rc), rc,
+                     ndg_last_error(d.ctx));
+        return 5;
+      }
+      int nup = 0;
+      ndg_get_list_updates(d.ctx, d.sys, &nup);
+      std::printf("# Number of neighbour list updates:%8d\n", nup);
+      std::fflush(stdout);
+    } else if (k == "END" || k == "DONE" || k == "end" || k == "done") {
+      break;
+    } else if (k == "EXIT" || k == "exit" || k == "quit" || k == "abort") {
+      break;
+    } else {
+      std::fprintf(stderr, "#  read_input: unsupported directive: %s line:%4d\n", k.c_str(), ln);
+    }
+  }
+  if (d.ctx) ndg_destroy(d.ctx);
+  return 0;
+}

@@ -1,0 +1,103 @@
+"""The C++ driver (ndyn_omp_b200/bin/ndyn_gpu) on the reference's own example
+scripts: it reads the directive script and model file as read_input does
+and must print the reference's logged thermo lines (the committed golden
+rows of tests/golden/reference_logs.json) to the precision of the log, as
+the CPU oracle does in tests/test_oracle_golden.py.  FP64 path; one
+mixed-precision run with the stated force error's effect on energies.
+"""
+import json
+import os
+import subprocess
+
+import pytest
+
+from golden import lattice
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXE = os.path.join(ROOT, "ndyn_omp_b200", "bin", "ndyn_gpu")
+GOLD = json.load(open(os.path.join(ROOT, "tests", "golden", "reference_logs.json")))
+
+
+def _run(name, tmp_path, nsteps=None, flags=()):
+    if not os.path.exists(EXE):
+        pytest.fail("driver not built: python -m ndyn_omp_b200.build")
+    case = GOLD[name]
+    lattice.materialise(case["model"], str(tmp_path))
+    script = list(case["script"])
+    if nsteps is not None:
+        script = [(" ".join(["Run", str(nsteps)] + ln.split()[2:3]) if ln.split()[:1] == ["Run"]
+                   else ln) for ln in script]
+    r = subprocess.run([EXE, *flags], input="START\n" + "\n".join(script) + "\n", text=True,
+                       capture_output=True, cwd=str(tmp_path), timeout=600)
+    assert r.returncode == 0, r.stderr
+    rows = []
+    for ln in r.stdout.splitlines():
+        w = ln.split()
+        if len(w) == 6 and w[0].isdigit():
+            rows.append(dict(step=int(w[0]), pe=float(w[1]), ke=float(w[2]), eerr=float(w[3]),
+                             press=float(w[4]), vol=float(w[5]), text=ln))
+    return rows, case["rows"], r.stdout
+
+
+def _close(ours, ref, rel, absol):
+    return abs(ours - ref) <= max(rel * abs(ref), absol)
+
+
+def _check(name, rows, ref_rows, ke_rel, press_abs, pe_rel=6e-6, eerr_rel=1e-3, limit=1):
+    byref = {r["step"]: r for r in ref_rows}
+    n = 0
+    for r in rows:
+        g = byref.get(r["step"])
+        if g is None:
+            continue
+        n += 1
+        assert _close(r["pe"], g["pe"], pe_rel, 0), (name, r, g["text"])
+        assert _close(r["vol"], g["vol"], 6e-6, 0), (name, r, g["text"])
+        assert _close(r["ke"], g["ke"], ke_rel, 0), (name, r, g["text"])
+        assert _close(r["press"], g["press"], 6e-6, press_abs), (name, r, g["text"])
+        assert _close(r["eerr"], g["eerr"], eerr_rel, 1e-13), (name, r, g["text"])
+    assert n >= limit
+
+
+def test_driver_morse_lattice(tmp_path):
+    """examples/MorseTest/out:38-138: 4000 NVE steps of the Cu lattice."""
+    rows, ref, out = _run("MorseTest", tmp_path)
+    assert len(rows) == len(ref) == 101
+    _check("MorseTest", rows, ref, ke_rel=2e-5, press_abs=0)
+    assert "Number of neighbour list updates:       0" in out
+    same = sum(a["text"].rstrip() == b["text"].rstrip() for a, b in zip(rows, ref))
+    assert same >= 95
+
+
+def test_driver_isobaric_relaxation(tmp_path):
+    """examples/testT/out:38-57: the barostat relaxes V 49836.0 -> 56637.5."""
+    rows, ref, _ = _run("testT_run1", tmp_path)
+    assert len(rows) == 21
+    _check("testT", rows, ref, ke_rel=5e-3, press_abs=5e-9)
+    assert rows[-1]["vol"] == pytest.approx(56637.5, abs=0.06)
+
+
+def test_driver_soft_potential(tmp_path):
+    """examples/SineTest/out:38: the 'soft' table."""
+    rows, ref, _ = _run("SineTest", tmp_path, nsteps=400)
+    _check("SineTest", rows, ref, ke_rel=2e-5, press_abs=0, limit=10)
+
+
+def test_driver_skin0_large_lattice(tmp_path):
+    """examples/testCAF/OMP_4/out_omp1:38: 23328 atoms, skin 0 (a list
+    rebuild every step)."""
+    rows, ref, _ = _run("testCAF_omp1", tmp_path, nsteps=3)
+    _check("testCAF", rows, ref, ke_rel=2e-3, press_abs=0)
+    assert rows[0]["text"].rstrip() == ref[0]["text"].rstrip()
+
+
+def test_driver_mixed_precision(tmp_path):
+    """--mixed on the MorseTest lattice: energies within 1e-5 of the log
+    (FP32 pair math at <=1e-5 relative force error)."""
+    rows, ref, _ = _run("MorseTest", tmp_path, nsteps=400, flags=("--mixed",))
+    # the lattice's kinetic energy is round-off noise of the forces, so only
+    # the potential energy, pressure and volume are compared
+    _check("MorseTest mixed", rows, ref, ke_rel=1e30, press_abs=1e-6, pe_rel=1e-5,
+           eerr_rel=1e30, limit=10)

@@ -327,3 +327,32 @@ def test_direct_build_coarse_cells(quirk):
         fg, peg, _, _ = ctx.forces(sid)
     assert rel_l2(fg, fo) < 1e-12
     assert abs(peg - peo) <= 1e-12 * abs(peo)
+
+
+def test_nve_drift_1000_steps_fp64_and_mixed():
+    """C1 (Cu 10^3 cells, Morse, 300 K, NVE, reference semantics), 1000 steps
+    in the oracle, the FP64 path and the mixed path.  Stated tolerances on
+    the energy error (PE+KE-e0)/e0 at every write_thermo row: FP64 within
+    1e-8 absolute of the oracle (summation order only; the trajectories
+    separate slowly), mixed within 1e-7 absolute, and the mixed drift over
+    steps 100..1000 within 1e-8 of the FP64 drift."""
+    spec = W.cu_crystal(10, 300.0, seed=1, quirk="ref")
+    spec["control"] = dict(spec["control"], out_steps=100)
+    o = oracle_from_spec(spec)
+    rc, ro = o.run(1000, spec["control"]["dt"])
+    assert rc == 0
+    res = {}
+    for p in ("fp64", "mixed"):
+        with nd.Context(0, p) as ctx:
+            gpu_from_spec(ctx, spec)
+            res[p] = ctx.run(1000)
+    g, m = res["fp64"], res["mixed"]
+    assert len(ro) == len(g) == len(m) == 11
+    for a, b, c in zip(ro, g, m):
+        assert a["step"] == b["step"] == c["step"]
+        assert abs(b["eerr"] - a["eerr"]) <= 1e-8
+        assert abs(c["eerr"] - a["eerr"]) <= 1e-7
+        assert c["pe"] == pytest.approx(a["pe"], rel=1e-7)
+    drift_g = g[-1]["eerr"] - g[1]["eerr"]
+    drift_m = m[-1]["eerr"] - m[1]["eerr"]
+    assert abs(drift_m - drift_g) <= 1e-8
