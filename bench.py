@@ -254,34 +254,24 @@ def plain_fp64_rate(specs, local, steps, stride):
 
 # ---------------------------------------------------------------------------
 def dist_init():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
-        import datetime
-
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    return ws, rank, local
+    from ndyn_omp_b200 import replicas as R
+    return R.init()
 
 
 def barrier(ws):
-    if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from ndyn_omp_b200 import replicas as R
+    R.barrier(ws)
 
 
 def allmax(x, ws):
-    if ws == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    """the slowest rank's value (times are max over ranks)"""
+    from ndyn_omp_b200 import replicas as R
+    return R.reduce_max(x, ws)
+
+
+def finish(ws):
+    from ndyn_omp_b200 import replicas as R
+    R.finish(ws)
 
 
 def run_reference(args, ws, rank):
@@ -439,15 +429,11 @@ def main():
     ws, rank, local = dist_init()
     if args.config == "c5" and args.impl != "reference":
         run_serving(args, ws, rank, local)
-        if ws > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
+        finish(ws)
         return
     if args.impl == "reference":
         run_reference(args, ws, rank)
-        if ws > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
+        finish(ws)
         return
     import torch
 
@@ -594,9 +580,7 @@ def main():
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
-    if ws > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    finish(ws)
 
 
 if __name__ == "__main__":
