@@ -50,6 +50,9 @@ def parse():
     ap.add_argument("--precision", default=None, choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tpa", type=int, default=0, help="threads per atom (0 = library choice)")
+    ap.add_argument("--bare", action="store_true",
+                    help="only the warm-up and timed steps (for profiler launch lists): no "
+                         "force error, plain baseline, e2e, CPU baseline or kernel timing")
     ap.add_argument("--graph-steps", type=int, default=100,
                     help="steps per CUDA graph (1 = eager launches, as ncu needs)")
     return ap.parse_args()
@@ -447,13 +450,13 @@ def main():
     # stated force error of this precision against the FP64 path (the FP64
     # path itself matches the CPU oracle to 1e-12, tests/test_gpu_parity.py)
     force_err = None
-    if prec == "mixed" and args.config != "c4":
+    if prec == "mixed" and args.config != "c4" and not args.bare:
         force_err, _ = force_error(specs[:1], [None], local)
 
     ctx = nd.Context(local, prec)
     ids = [W.add_to_context(ctx, s) for s in specs]
     ctx.set_tuning(args.tpa, args.graph_steps)
-    if args.config == "c4":
+    if args.config == "c4" and not args.bare:
         ctx.autotune(10)
     # warm-up (includes the dynamics prologue: cell + Verlet list build)
     ctx.run(max(args.warmup, 3))
@@ -475,6 +478,18 @@ def main():
     ms = allmax(ms, ws)
     value = N * args.steps * ws / (ms / 1e3)
     clocks = clk.summary()
+    if args.bare:
+        if rank == 0:
+            print(json.dumps({"metric": "atom-steps/s", "value": value, "unit": "atom-steps/s",
+                              "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+                              "ms_per_step": ms / args.steps, "bare": True,
+                              "config": {"workload": WORKLOAD_TEXT[args.config], "atoms": N,
+                                         "graph_steps": args.graph_steps},
+                              "list_rebuilds_in_timed_region": rebuilds, "clocks": clocks}),
+                  flush=True)
+        ctx.close()
+        finish(ws)
+        return
 
     extra = {}
     if args.config == "c4":

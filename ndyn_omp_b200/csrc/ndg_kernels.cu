@@ -1274,6 +1274,23 @@ __device__ __forceinline__ void global_tables(const DevCtx &c, const SysParam *P
   tv.tP2 = c.tabP2 + P->tab_off;
 }
 
+// L2 eviction priority for streams read once per step (the neighbour list
+// rows): their lines go first, so the gathered positions, which every tile
+// re-reads, keep their place in L2
+__device__ __forceinline__ unsigned long long l2_evict_first() {
+  unsigned long long p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+__device__ __forceinline__ int ld_stream(const int *a, unsigned long long pol) {
+  int v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.b32 %0, [%1], %2;"
+      : "=r"(v)
+      : "l"(a), "l"(pol));
+  return v;
+}
+
 // per-pair cutoff band and table scale of the mixed loop
 template <bool STAB>
 __device__ __forceinline__ float4 pair_params(const TabView &tv, int p1) {
@@ -1361,9 +1378,9 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV>() * 128 / (TILE *
         const int *src = c.nbr + Pn->nbr_off + (long long)((nt_ * TILE - Pn->atom_off) / TILE) *
                                                    Pn->maxnb * TILE;
         if (rows > 0) {
-          asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(
+          asm volatile("cp.async.bulk.prefetch.L2.global.L2::cache_hint [%0], %1, %2;" ::"l"(
                            __cvta_generic_to_global(src)),
-                       "r"(rows * TILE * 4)
+                       "r"(rows * TILE * 4), "l"(l2_evict_first())
                        : "memory");
         }
       }
@@ -1451,6 +1468,7 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV>() * 128 / (TILE *
         const float sb2 = (float)(S->box[2] * (1.0 / FX_ONE));
         const float ptrmin = (float)P->ptrmin;
         const int nch = (cnt + CHUNK - 1) / CHUNK;
+        const unsigned long long lpol = l2_evict_first();
         auto loop = [&](auto one_t) {
           constexpr bool ONE = decltype(one_t)::value;
           const float4 pp1 = ONE ? pair_params<STAB>(tv, 0) : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -1459,7 +1477,7 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV>() * 128 / (TILE *
             int qq[CHUNK];
 #pragma unroll
             for (int q = 0; q < CHUNK; ++q)
-              qq[q] = kb + q < cnt ? __ldg(nb + (kb + q) * TILE) : -1;
+              qq[q] = kb + q < cnt ? ld_stream(nb + (kb + q) * TILE, lpol) : -1;
             float ax = 0.f, ay = 0.f, az = 0.f, ape = 0.f;
             float av0 = 0.f, av1 = 0.f, av2 = 0.f, av3 = 0.f, av4 = 0.f, av5 = 0.f;
             unsigned nm = 0;  // entries of this chunk within FP32 rounding of the cutoff
@@ -1611,11 +1629,16 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV>() * 128 / (TILE *
         const double dt = P->dt;
         double *v = c.vel + 3 * (size_t)i;
         double *a = c.acc + 3 * (size_t)i;
-        const double v0 = v[0] + 0.5 * dt * (fx * rmass + a[0]);
-        const double v1 = v[1] + 0.5 * dt * (fy * rmass + a[1]);
-        const double v2 = v[2] + 0.5 * dt * (fz * rmass + a[2]);
-        v[0] = v0; v[1] = v1; v[2] = v2;
-        a[0] = fx * rmass; a[1] = fy * rmass; a[2] = fz * rmass;
+        // velocities and accelerations stream through once per step
+        const double v0 = __ldcs(v) + 0.5 * dt * (fx * rmass + __ldcs(a));
+        const double v1 = __ldcs(v + 1) + 0.5 * dt * (fy * rmass + __ldcs(a + 1));
+        const double v2 = __ldcs(v + 2) + 0.5 * dt * (fz * rmass + __ldcs(a + 2));
+        __stcs(v, v0);
+        __stcs(v + 1, v1);
+        __stcs(v + 2, v2);
+        __stcs(a, fx * rmass);
+        __stcs(a + 1, fy * rmass);
+        __stcs(a + 2, fz * rmass);
         if (flags & F_CK) {
           double kt = v0 * v0;
           kt = kt + v1 * v1;
