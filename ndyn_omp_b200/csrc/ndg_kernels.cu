@@ -23,6 +23,8 @@
 
 namespace ndg {
 
+constexpr int TILE = 128;  // atoms per tile of the neighbour list and the pair kernel
+
 __device__ __forceinline__ int tw_of(double w) { return (int)__double_as_longlong(w); }
 
 // record an error on the system and in the context-wide error word
@@ -695,11 +697,14 @@ __device__ void copyback_chunk(const DevCtx &c, int sys, int chunk, int mixed) {
     c.itop[2 * chunk] = 0.0;  // dispList was reset: the displacement measure is 0
     c.itop[2 * chunk + 1] = 0.0;
   }
+  if (threadIdx.x < ATOM_ALIGN / TILE) c.tile_rows[chunk * (ATOM_ALIGN / TILE) + threadIdx.x] = 0;
   const int i = chunk * ATOM_ALIGN + threadIdx.x;
   if (i - P->atom_off >= P->n) return;
   const double4 p = c.s_pos[i];
   c.pos[i] = p;
-  if (mixed) c.pfx[i] = make_int4(fx32(p.x), fx32(p.y), fx32(p.z), tw_of(p.w));
+  // the fixed-point positions the list build (and the mixed pair loop) read
+  c.pfx[i] = make_int4(fx32(p.x), fx32(p.y), fx32(p.z), tw_of(p.w));
+  (void)mixed;
   for (int d = 0; d < 3; ++d) {
     c.vel[3 * (size_t)i + d] = c.s_vel[3 * (size_t)i + d];
     c.acc[3 * (size_t)i + d] = c.s_acc[3 * (size_t)i + d];
@@ -730,7 +735,6 @@ __global__ __launch_bounds__(BLOCK) void k_copyback(DevCtx c, int mixed) {
 //      candidate indices and written to the blocked list row by row.
 // A tile whose cells or candidates do not fit the shared buffers takes
 // build_tile_direct (same test, same list order, no staging).
-constexpr int TILE = 128;      // atoms per tile
 constexpr int TC_MAX = 256;    // link cells a tile may stage
 constexpr int HSLOTS = 1024;   // shared hash slots for the tile's cell set
 constexpr float NB_MARGIN = 1e-5f;
