@@ -577,10 +577,8 @@ __global__ __launch_bounds__(BLOCK) void k_bin(DevCtx c) {
              [&](int s, int u) { bin_chunk(c, s, u); });
 }
 
-// exclusive scan of the cell counts of one listed system per block
-__global__ __launch_bounds__(1024) void k_scan(DevCtx c, int counting) {
-  if ((int)blockIdx.x >= c.ring_count[3]) return;
-  const int s = c.rb_list[blockIdx.x];
+// exclusive scan of one system's cell counts (a whole block)
+__device__ void scan_system(const DevCtx &c, int s, int counting) {
   const SysParam *__restrict__ P = c.P + s;
   SysState *S = c.S + s;
   __shared__ int wsum[32];
@@ -624,6 +622,15 @@ __global__ __launch_bounds__(1024) void k_scan(DevCtx c, int counting) {
     S->nstencil = make_stencil(S->mcell, P->quirk, S->stencil);
     for (int d = 0; d < 3; ++d) S->box_build[d] = S->box[d];
     if (counting) S->nlist_updates += 1;  // NlistUpdates, src/nd.f90:1495
+  }
+}
+
+// exclusive scan of the cell counts, one listed system at a time per block
+__global__ __launch_bounds__(1024) void k_scan(DevCtx c, int counting) {
+  const int nl = c.ring_count[3];
+  for (int k = blockIdx.x; k < nl; k += gridDim.x) {
+    scan_system(c, c.rb_list[k], counting);
+    __syncthreads();  // carry and wsum are reused by the next system
   }
 }
 
@@ -1823,7 +1830,7 @@ void launch_rebuild(const DevCtx &c, cudaStream_t st, int counting, int mixed) {
   const int gcell = std::min((c.ncells + BLOCK / 32 - 1) / (BLOCK / 32), nsm * 8);
   const int gtile = std::min(c.nchunks * (ATOM_ALIGN / TILE), nsm * 2);
   k_bin<<<gchunk, BLOCK, 0, st>>>(c);
-  k_scan<<<c.nsys_cap, 1024, 0, st>>>(c, counting);
+  k_scan<<<std::min(c.nsys_cap, nsm), 1024, 0, st>>>(c, counting);
   k_scatter<<<gchunk, BLOCK, 0, st>>>(c);
   k_order<<<gcell, BLOCK, 0, st>>>(c);
   k_permute<<<gchunk, BLOCK, 0, st>>>(c);
