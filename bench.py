@@ -580,7 +580,8 @@ def main():
                    "parallelism": f"replicas x{ws} (one system per GPU)" if ws > 1 else "1 GPU",
                    "l2": f"inputs larger than L2: ~{touched / 1e6:.0f} MB touched per step "
                          f"vs 126 MB L2" if touched > L2_BYTES else "L2-resident workload",
-                   "threads_per_atom": tpa, "graph_steps": gsteps,
+                   "threads_per_atom": tpa, "gather_depth": ctx.gather_depth(),
+                   "graph_steps": gsteps,
                    "baseline_metric": "atom-steps/s at 1 GPU, batched mixed vs plain FP64 at "
                                       "stated force error; p50/p99"},
         "force_rel_err_vs_fp64": force_err,

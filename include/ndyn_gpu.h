@@ -238,8 +238,13 @@ int ndg_compute0_static(int np, int ntypes, int npairs, int ptsize, double ptrmi
  * count and mean neighbour count) and steps per CUDA-graph block */
 int ndg_set_tuning(ndg_ctx *ctx, int threads_per_atom, int graph_steps);
 int ndg_get_tuning(ndg_ctx *ctx, int *threads_per_atom, int *graph_steps);
-/* time candidate launch shapes on the current systems for a few steps and
- * keep the fastest (state is restored afterwards) */
+/* neighbour gathers in flight per thread in the mixed one-thread-per-atom
+ * pair loop: 4 (more resident warps) or 8 (more latency hidden) */
+int ndg_set_gather_depth(ndg_ctx *ctx, int depth);
+int ndg_get_gather_depth(ndg_ctx *ctx, int *depth);
+/* time candidate launch shapes (threads per atom; gather depth for one
+ * thread per atom in mixed precision) on the current systems for a few
+ * steps and keep the fastest (state is restored afterwards) */
 int ndg_autotune(ndg_ctx *ctx, int steps_per_trial);
 /* device bytes the context holds, and the bytes one more system of np
  * atoms with ntypes/npairs/ptsize would need */

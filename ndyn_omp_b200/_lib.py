@@ -48,6 +48,8 @@ SIGNATURES = [
     ("ndg_get_neighbor_count", i, [vp, i, vp]),
     ("ndg_set_tuning", i, [vp, i, i]),
     ("ndg_get_tuning", i, [vp, vp, vp]),
+    ("ndg_set_gather_depth", i, [vp, i]),
+    ("ndg_get_gather_depth", i, [vp, vp]),
     ("ndg_autotune", i, [vp, i]),
     ("ndg_device_bytes", i, [vp, vp]),
     ("ndg_system_bytes", ll, [i, i, i, i, d, d, i]),

@@ -316,6 +316,14 @@ class Context:
         _ok(self.L.ndg_get_tuning(self._c, ctypes.byref(t), ctypes.byref(g)), "get_tuning")
         return t.value, g.value
 
+    def set_gather_depth(self, depth):
+        _ok(self.L.ndg_set_gather_depth(self._c, int(depth)), "set_gather_depth")
+
+    def gather_depth(self):
+        d = ctypes.c_int()
+        _ok(self.L.ndg_get_gather_depth(self._c, ctypes.byref(d)), "get_gather_depth")
+        return d.value
+
     def autotune(self, steps=20):
         _ok(self.L.ndg_autotune(self._c, int(steps)), "autotune")
         return self.tuning()

@@ -126,6 +126,7 @@ struct ndg_ctx {
   bool params_dirty = true;
   // tuning and graphs
   int tpa = 0, graph_steps = 100;
+  int gather = 4;  // mixed pair loop gather depth (4 or 8)
   int stab_smem = 0;  // staged-table bytes of the pair kernel (0: tables from global)
   int nb_smem = 0;  // neighbour-build dynamic smem
   int nb_vcap = 4096;
@@ -183,6 +184,7 @@ DevCtx devctx(ndg_ctx *c) {
   d.nbr = c->nbr;
   d.tile_rows = c->tile_rows;
   d.nb_vcap = c->nb_vcap;
+  d.gather = c->gather;
   d.nnb = c->nnb;
   d.atom_cell = c->atom_cell;
   d.atom_slot = c->atom_slot;
@@ -1470,6 +1472,19 @@ int ndg_set_tuning(ndg_ctx *c, int tpa, int graph_steps) {
   return NDG_OK;
 }
 
+int ndg_set_gather_depth(ndg_ctx *c, int depth) {
+  if (!c || (depth != 4 && depth != 8)) return NDG_ERR_ARG;
+  if (depth != c->gather) drop_graphs(c);
+  c->gather = depth;
+  return NDG_OK;
+}
+
+int ndg_get_gather_depth(ndg_ctx *c, int *depth) {
+  if (!c || !depth) return NDG_ERR_ARG;
+  *depth = c->gather;
+  return NDG_OK;
+}
+
 int ndg_get_tuning(ndg_ctx *c, int *tpa, int *graph_steps) {
   if (!c) return NDG_ERR_ARG;
   if (tpa) *tpa = choose_tpa(c);
@@ -1547,13 +1562,19 @@ int ndg_autotune(ndg_ctx *c, int steps) {
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  const int keep_tpa = c->tpa;
-  int best = 0;
+  const int keep_tpa = c->tpa, keep_gather = c->gather;
+  int best = 0, best_g = 4;
   float best_ms = 0.f;
   cudaError_t ce = copy(true);
-  const int cand[4] = {1, 2, 4, 8};
-  for (int k = 0; k < 4 && ce == cudaSuccess && rc == NDG_OK; ++k) {
-    c->tpa = cand[k];
+  // launch shapes: threads per atom, and for one thread per atom in mixed
+  // precision the gather depth
+  const int cand[5][2] = {{1, 4}, {1, 8}, {2, 4}, {4, 4}, {8, 4}};
+  const int ncand = c->precision == NDG_PREC_MIXED ? 5 : 4;
+  for (int k = 0, kk = 0; kk < ncand && ce == cudaSuccess && rc == NDG_OK; ++k) {
+    if (c->precision != NDG_PREC_MIXED && cand[k][1] != 4) continue;
+    ++kk;
+    c->tpa = cand[k][0];
+    c->gather = cand[k][1];
     drop_graphs(c);
     CK(c, cudaMemset(c->ring_count, 0, 4 * sizeof(int)));
     DevCtx d = devctx(c);
@@ -1567,7 +1588,8 @@ int ndg_autotune(ndg_ctx *c, int steps) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
     if (!rc && (best == 0 || ms < best_ms)) {
-      best = cand[k];
+      best = cand[k][0];
+      best_g = cand[k][1];
       best_ms = ms;
     }
     ce = copy(false);
@@ -1577,6 +1599,7 @@ int ndg_autotune(ndg_ctx *c, int steps) {
   cudaFree(snap);
   CK(c, cudaMemset(c->ring_count, 0, 4 * sizeof(int)));
   c->tpa = best ? best : keep_tpa;
+  c->gather = best ? best_g : keep_gather;
   drop_graphs(c);
   if (ce != cudaSuccess) return cuda_fail(c, ce, "autotune snapshot");
   return rc;

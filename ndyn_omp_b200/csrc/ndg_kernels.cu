@@ -1325,19 +1325,21 @@ __device__ __forceinline__ float4 pair_params(const TabView &tv, int p1) {
 // chunks and the integer totals, which do not depend on the order of
 // addition, are the same bits for any TPA, grid or batch composition.
 constexpr int CHUNK = 8;   // mixed: list entries per FP32 partial sum
-constexpr int GATHER = 4;  // mixed: neighbour gathers in flight per thread
+// mixed: neighbour gathers in flight per thread, 4 or 8 (a tuning choice:
+// 8 hides more latency when the gathers miss L2, 4 keeps more warps resident)
 
 // resident 128-thread CTAs per SM each variant is compiled for (register
-// budget 65536 / (128 * n)): the mixed lean loop fits 72 registers, its
-// energy/virial form about 100, the FP64 ones 100 and 128
-template <bool MIXED, bool EV>
+// budget 65536 / (128 * n)): the mixed lean loop fits 72 registers (80 with
+// eight gathers in flight), its energy/virial form about 100, the FP64 ones
+// 100 and 128
+template <bool MIXED, bool EV, int GATHER>
 constexpr int pair_ctas() {
-  return MIXED ? (EV ? 5 : 7) : (EV ? 4 : 5);
+  return MIXED ? (EV ? 5 : (GATHER > 4 ? 6 : 7)) : (EV ? 4 : 5);
 }
 
-template <int TPA, bool MIXED, bool FUSE, bool STAB, bool EV>
-__global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV>() * 128 / (TILE * TPA)) > 0
-                                             ? pair_ctas<MIXED, EV>() * 128 / (TILE * TPA)
+template <int TPA, bool MIXED, bool FUSE, bool STAB, bool EV, int GATHER>
+__global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 / (TILE * TPA)) > 0
+                                             ? pair_ctas<MIXED, EV, GATHER>() * 128 / (TILE * TPA)
                                              : 1) void k_pair(DevCtx c, int host_flags, int ntiles,
                                                      unsigned long long next_h) {
   constexpr int NT = TILE * TPA;
@@ -1743,9 +1745,9 @@ static int sm_count() {
   return n;
 }
 
-template <int TPA, bool MIXED, bool FUSE, bool STAB, bool EV>
-static void pair_go(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh) {
-  auto kern = k_pair<TPA, MIXED, FUSE, STAB, EV>;
+template <int TPA, bool MIXED, bool FUSE, bool STAB, bool EV, int GATHER>
+static void pair_launch(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh) {
+  auto kern = k_pair<TPA, MIXED, FUSE, STAB, EV, GATHER>;
   const int smem = (STAB ? c.stab_smem : 0) + ((MIXED && EV) ? 7 * 8 * TILE * TPA : 0);
   static int cfg_smem = -1, occ = 0;
   if (smem != cfg_smem) {
@@ -1758,6 +1760,13 @@ static void pair_go(const DevCtx &c, cudaStream_t st, int hf, unsigned long long
   const int ntiles = c.nchunks * (ATOM_ALIGN / TILE);
   const int grid = ntiles < nsm * occ ? ntiles : nsm * occ;
   kern<<<grid, TILE * TPA, smem, st>>>(c, hf, ntiles, nh);
+}
+
+// the deeper gather only for the mixed one-thread-per-atom loop
+template <int TPA, bool MIXED, bool FUSE, bool STAB, bool EV>
+static void pair_go(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh) {
+  if (MIXED && TPA == 1 && c.gather > 4) pair_launch<TPA, MIXED, FUSE, STAB, EV, 8>(c, st, hf, nh);
+  else pair_launch<TPA, MIXED, FUSE, STAB, EV, 4>(c, st, hf, nh);
 }
 
 // FUSE (a dynamics step): the kernel without energy/virial takes the

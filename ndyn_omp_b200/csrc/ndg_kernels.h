@@ -16,6 +16,7 @@ struct DevCtx {
   int stab_smem;  // shared-memory bytes of the staged pair tables, 0 = read from global
   int nb_smem;  // neighbour build dynamic smem
   int nb_vcap;  // flat candidate-list capacity of the build
+  int gather;   // mixed pair loop: neighbour gathers in flight (4 or 8)
   double4 *pos;
   int4 *pfx;
   double *vel, *acc, *disp, *force;

@@ -356,3 +356,22 @@ def test_nve_drift_1000_steps_fp64_and_mixed():
     drift_g = g[-1]["eerr"] - g[1]["eerr"]
     drift_m = m[-1]["eerr"] - m[1]["eerr"]
     assert abs(drift_m - drift_g) <= 1e-8
+
+
+def test_gather_depth_same_bits(specs):
+    """The mixed loop's gather depth (4 or 8 neighbour loads in flight) is a
+    pure launch choice: the same chunks are summed in the same order, so
+    forces and trajectories are the same bits."""
+    spec = specs["ar_fixed"]
+    out = []
+    for depth in (4, 8):
+        with nd.Context(0, "mixed") as ctx:
+            sid = gpu_from_spec(ctx, spec)
+            ctx.set_tuning(1, 100)
+            ctx.set_gather_depth(depth)
+            assert ctx.gather_depth() == depth
+            rows = ctx.run(40)
+            out.append((ctx.state(sid), rows))
+    for a, b in zip(out[0][0], out[1][0]):
+        assert np.array_equal(a, b)
+    assert out[0][1] == out[1][1]
