@@ -899,6 +899,29 @@ __device__ __noinline__ void build_tile_direct(const DevCtx &c, int sys, int til
   }
 }
 
+// Squared distance from candidate pj to the box around a run's own atoms is
+// at most rl2.  The box is kept relative to the run's first atom (fixed
+// point, b[0..2]) as offset bounds b[3..5] (low) and b[6..8] (high): atoms
+// of one cell differ by far less than half the box, so their wrap-around
+// differences are exact even where the cell holds the atoms the reference's
+// anint places at +0.5.  A candidate's wrap-around difference from the
+// first atom is its minimum image while it lies within half a box of it,
+// which holds on link-cell grids of five or more cells per axis.
+__device__ __forceinline__ bool near_box(const int4 &pj, const int *b, float sb0, float sb1,
+                                         float sb2, float rl2) {
+  const int pv[3] = {pj.x, pj.y, pj.z};
+  const float sb[3] = {sb0, sb1, sb2};
+  float d2 = 0.f;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int o = (int)((unsigned)pv[d] - (unsigned)b[d]);
+    const float gap = o < b[3 + d] ? (float)b[3 + d] - (float)o
+                                   : (o > b[6 + d] ? (float)o - (float)b[6 + d] : 0.f);
+    d2 = __fmaf_rn(gap * sb[d], gap * sb[d], d2);
+  }
+  return d2 <= rl2;
+}
+
 __device__ void build_tile(const DevCtx &c, int sys, int tile) {
   extern __shared__ __align__(16) unsigned char dsm[];
   __syncthreads();  // the block's previous tile is done with shared memory
@@ -925,7 +948,7 @@ __device__ void build_tile(const DevCtx &c, int sys, int tile) {
   __shared__ short run_of[TILE];               // own atom -> run of equal cells
   __shared__ int run_cell[TILE];
   __shared__ short ent_u[TILE * MAX_STENCIL];  // run x stencil entry -> staged cell
-  __shared__ short epre[TILE * MAX_STENCIL];   // run x entry -> offset in the run's list
+  __shared__ int rbox[TILE][9];                // run -> box of its own atoms (first atom, offsets)
   __shared__ int vsize[TILE], vstart[TILE], run_t0[TILE + 1];
   __shared__ int nu, bad, nruns, rows_s;
   __shared__ int pm_s[16 * 16];
@@ -1066,18 +1089,56 @@ __device__ void build_tile(const DevCtx &c, int sys, int tile) {
         (short)find_cell(ucell, U, stencil_cell(run_cell[r], stc[e], M0, M1, M2));
   }
   __syncthreads();
-  // each run's candidates as one flat list: its stencil entries' staged
-  // ranges back to back (entries repeat where the reference's half stencil
-  // reaches a cell twice), bit 15 marks the run's own cell (PTrMin test)
-  if (threadIdx.x < nruns) {
-    const int r = threadIdx.x;
-    int tot = 0;
-    for (int e = 0; e < ne; ++e) {
-      epre[r * MAX_STENCIL + e] = (short)tot;
-      const int u = ent_u[r * MAX_STENCIL + e];
-      tot += coff[u + 1] - coff[u];
+  // Each run's candidates as one flat list: its stencil entries' staged
+  // ranges back to back, in stencil order (entries repeat where the
+  // reference's half stencil reaches a cell twice), bit 15 marking the run's
+  // own cell (PTrMin test).  On grids of five or more cells per axis a
+  // candidate farther than the list radius from the box around the run's
+  // own atoms is left out: it cannot be a neighbour of any of them, so the
+  // lists are unchanged and each own atom tests fewer candidates.
+  const bool prune = M0 >= 5 && M1 >= 5 && M2 >= 5;
+  const float rl2box = (float)(P->rlist * P->rlist) * (1.f + 4.f * NB_MARGIN);
+  const float sbx = (float)(S->box[0] * (1.0 / FX_ONE)), sby = (float)(S->box[1] * (1.0 / FX_ONE)),
+              sbz = (float)(S->box[2] * (1.0 / FX_ONE));
+  if (prune) {
+    for (int r = threadIdx.x; r < nruns; r += NBT) {
+      const double4 p = c.pos[a0 + run_t0[r]];
+      rbox[r][0] = fx32(p.x);
+      rbox[r][1] = fx32(p.y);
+      rbox[r][2] = fx32(p.z);
+      rbox[r][3] = rbox[r][4] = rbox[r][5] = 0;
+      rbox[r][6] = rbox[r][7] = rbox[r][8] = 0;
     }
-    vsize[r] = tot;
+    __syncthreads();
+    if (threadIdx.x < nown) {
+      const double4 p = c.pos[a0 + threadIdx.x];
+      const int f[3] = {fx32(p.x), fx32(p.y), fx32(p.z)};
+      const int r = run_of[threadIdx.x];
+      for (int d = 0; d < 3; ++d) {
+        const int o = (int)((unsigned)f[d] - (unsigned)rbox[r][d]);
+        atomicMin(&rbox[r][3 + d], o);
+        atomicMax(&rbox[r][6 + d], o);
+      }
+    }
+    __syncthreads();
+  }
+  // pass 1: each run's list length (a warp per run)
+  for (int r = warp; r < nruns; r += NBT / 32) {
+    int kept = 0;
+    for (int e = 0; e < ne; ++e) {
+      const int u = ent_u[r * MAX_STENCIL + e];
+      const int q0 = coff[u], len = coff[u + 1] - q0;
+      if (!prune) {
+        kept += len;
+        continue;
+      }
+      for (int kb = 0; kb < len; kb += 32) {
+        const int k = kb + lane;
+        const bool keep = k < len && near_box(cpf[q0 + k], rbox[r], sbx, sby, sbz, rl2box);
+        kept += __popc(__ballot_sync(0xffffffffu, keep));
+      }
+    }
+    if (lane == 0) vsize[r] = kept;
   }
   __syncthreads();
   const int *__restrict__ pmg = pm;
@@ -1100,13 +1161,23 @@ __device__ void build_tile(const DevCtx &c, int sys, int tile) {
     __syncthreads();
     if (bad) break;
     const int re = re_s;
-    for (int w = warp; w < (re - rb) * ne; w += NBT / 32) {
-      const int r = rb + w / ne, e = w % ne;
-      const int u = ent_u[r * MAX_STENCIL + e];
-      const int q0 = coff[u], len = coff[u + 1] - q0;
-      const unsigned short cflag = ((stc[e] >> 12) & 1) ? 0x8000u : 0u;
-      unsigned short *dst = vlist + vstart[r] + epre[r * MAX_STENCIL + e];
-      for (int k = lane; k < len; k += 32) dst[k] = (unsigned short)(q0 + k) | cflag;
+    // pass 2: the runs' lists, compacted in order (a warp per run)
+    for (int r = rb + warp; r < re; r += NBT / 32) {
+      unsigned short *vd = vlist + vstart[r];
+      int at = 0;
+      for (int e = 0; e < ne; ++e) {
+        const int u = ent_u[r * MAX_STENCIL + e];
+        const int q0 = coff[u], len = coff[u + 1] - q0;
+        const unsigned short cflag = ((stc[e] >> 12) & 1) ? 0x8000u : 0u;
+        for (int kb = 0; kb < len; kb += 32) {
+          const int k = kb + lane;
+          const bool keep =
+              k < len && (!prune || near_box(cpf[q0 + k], rbox[r], sbx, sby, sbz, rl2box));
+          const unsigned bal = __ballot_sync(0xffffffffu, keep);
+          if (keep) vd[at + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)(q0 + k) | cflag;
+          at += __popc(bal);
+        }
+      }
     }
     __syncthreads();
     // 3. one warp per own atom, 32 candidates of the flat list per pass;

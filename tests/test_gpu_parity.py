@@ -28,6 +28,7 @@ def small_specs():
         "nacl_fixed": W.nacl_solid((6, 6, 6), 600.0, seed=13, quirk="fixed"),  # 1728 atoms
         "cu_m2_ref": W.cu_crystal(5, 900.0, seed=14, quirk="ref"),        # 500 atoms, M=2
         "cu_m2_fixed": W.cu_crystal(5, 900.0, seed=14, quirk="fixed"),
+        "cu_m6_ref": W.cu_crystal(12, 600.0, seed=15, quirk="ref"),      # 6912 atoms, M=6
     }
 
 
@@ -42,10 +43,12 @@ def _jitter(spec, amp, seed):
 def specs():
     s = small_specs()
     s["cu_ref"] = _jitter(s["cu_ref"], 0.05, 99)
+    s["cu_m6_ref"] = _jitter(s["cu_m6_ref"], 0.1, 98)
     return s
 
 
-@pytest.mark.parametrize("name", ["cu_ref", "ar_fixed", "nacl_fixed", "cu_m2_ref", "cu_m2_fixed"])
+@pytest.mark.parametrize("name", ["cu_ref", "ar_fixed", "nacl_fixed", "cu_m2_ref", "cu_m2_fixed",
+                                  "cu_m6_ref"])
 def test_cells_and_neighbour_pairs_bit_exact(specs, name):
     spec = specs[name]
     o = oracle_from_spec(spec)
