@@ -33,7 +33,6 @@ constexpr int ATOM_ALIGN = 256;   // padding unit of a system's atom range
 constexpr int BLOCK = 256;        // threads of the atom-parallel kernels
 constexpr int MAX_STENCIL = 27;   // neighbour-cell entries incl. repeats
 constexpr int MAX_TYPES = 64;
-constexpr int NB_TILE = 32;       // atoms per tile of the blocked neighbour list
 constexpr double FX_ONE = 4294967296.0;  // 2^32: one box length in pfx units
 constexpr double FORCE_FX = 4294967296.0; // 2^32 fixed-point units per eV/A
 
@@ -66,8 +65,6 @@ struct SysParam {
   int pair_off, type_off, pm_off;
   int ntypes, npairs, ptsize;
   int quirk;
-  int nstencil;
-  int stencil[MAX_STENCIL];      // (dx+1) | (dy+1)<<4 | (dz+1)<<8 | center<<12
   double ptrmin;
   double dt, skin, skinsq, rlist; // rlist = rcut + skin
   int renei, renei_freq, out_steps;
@@ -89,8 +86,8 @@ struct SysState {
   int pend;              // bit0: lam_ke pending, bit1: lam_e pending
   int rebuild;           // rebuild lists before the next integrate1
   int nlist_updates;
-  int nstencil;                  // neighbour-cell stencil of the current grid
-  int stencil[MAX_STENCIL];
+  int nstencil;                  // neighbour-cell stencil of the current grid:
+  int stencil[MAX_STENCIL];      // (dx+1) | (dy+1)<<4 | (dz+1)<<8 | center<<12
   int err;
   unsigned int ticket;   // last-block election of the pair kernel
   unsigned int ticket_i; // last-block election of integrate2 (standalone)

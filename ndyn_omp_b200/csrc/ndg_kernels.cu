@@ -1906,8 +1906,8 @@ void launch_integrate2(const DevCtx &c, cudaStream_t st, int ck) {
 // the rebuild to each system's NlistUpdates (not for the setup builds)
 void launch_rebuild(const DevCtx &c, cudaStream_t st, int counting, int mixed) {
   const int nsm = sm_count();
-  const int gchunk = std::min(c.nchunks, nsm * 8);
-  const int gcell = std::min((c.ncells + BLOCK / 32 - 1) / (BLOCK / 32), nsm * 8);
+  const int gchunk = std::min(c.nchunks, nsm * 4);
+  const int gcell = std::min((c.ncells + BLOCK / 32 - 1) / (BLOCK / 32), nsm * 4);
   const int gtile = std::min(c.nchunks * (ATOM_ALIGN / TILE), nsm * 2);
   k_bin<<<gchunk, BLOCK, 0, st>>>(c);
   k_scan<<<std::min(c.nsys_cap, nsm), 1024, 0, st>>>(c, counting);
