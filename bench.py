@@ -587,10 +587,11 @@ def main():
         "force_rel_err_vs_fp64": force_err,
         **extra,
         "list_rebuilds_in_timed_region": rebuilds,
-        # per step integrate1 + pair; per graph block k_decide; the 7 rebuild
-        # kernels on steps whose conditional node fires (at most one per
-        # step, at most one per list update)
-        "gpu_launches": 2 * args.steps + -(-args.steps // gsteps) + 7 * min(args.steps, rebuilds),
+        # per step integrate1 (with the work plan) and the two pair kernels; per
+        # graph block k_begin_block and k_decide; the 7 rebuild kernels on
+        # steps whose conditional node fires (at most one per step, at most
+        # one per list update)
+        "gpu_launches": 3 * args.steps + 2 * -(-args.steps // gsteps) + 7 * min(args.steps, rebuilds),
         "clocks": clocks,
         "roofline": roof,
         "cpu_baseline": cpu,

@@ -93,6 +93,7 @@ struct SysState {
   unsigned int ticket_i; // last-block election of integrate2 (standalone)
   int run_left;          // steps of the current run not yet given to a block
   int start;             // how the next block begins: START_* (0 = continue)
+  unsigned long long rows;  // rows of the last list build summed over the tiles
 };
 
 // SysState::start: a block continues the run, or starts a new one (tt = 1)

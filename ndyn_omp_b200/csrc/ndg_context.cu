@@ -113,6 +113,9 @@ struct ndg_ctx {
   int *nbr = nullptr;
   int *tile_rows = nullptr;
   int *rb_list = nullptr;  // systems listed for a list rebuild
+  PlanEnt *plan = nullptr;  // pair-launch work plan (integrate1's extra block)
+  int *plan_kb = nullptr;
+  PlanHdr *plan_hdr = nullptr;
   double *red = nullptr, *itop = nullptr, *ired = nullptr;
   int *pairmat = nullptr;
   double *mass = nullptr, *rc2 = nullptr, *rlist2 = nullptr;
@@ -128,6 +131,7 @@ struct ndg_ctx {
   int tpa = 0, graph_steps = 100;
   int gather = 4;  // mixed pair loop gather depth (4 or 8)
   int stab_smem = 0;  // staged-table bytes of the pair kernel (0: tables from global)
+  int stab_lean = 0;  // the same without the energy table
   int nb_smem = 0;  // neighbour-build dynamic smem
   int nb_vcap = 4096;
   std::map<int, cudaGraphExec_t> graphs;
@@ -214,8 +218,12 @@ DevCtx devctx(ndg_ctx *c) {
   d.ring = c->ring;
   d.ring_count = c->ring_count;
   d.rb_list = c->rb_list;
+  d.plan = c->plan;
+  d.plan_kb = c->plan_kb;
+  d.plan_hdr = c->plan_hdr;
   d.ring_cap = c->ring_cap;
   d.stab_smem = c->stab_smem;
+  d.stab_lean = c->stab_lean;
   d.nb_smem = c->nb_smem;
   return d;
 }
@@ -303,7 +311,11 @@ int grow_sys(ndg_ctx *c, int n) {
   rc |= grow(c, c->dP, (size_t)c->nsys_cap, (size_t)n);
   rc |= grow(c, c->dS, (size_t)c->nsys_cap, (size_t)n);
   rc |= grow(c, c->rb_list, 0, (size_t)n);
+  rc |= grow(c, c->plan, 0, 2 * (size_t)n);
+  if (!c->plan_kb) rc |= grow(c, c->plan_kb, 0, 2 * (size_t)PLAN_GMAX);
+  if (!c->plan_hdr) rc |= grow(c, c->plan_hdr, 0, 1);
   if (rc) return NDG_ERR_NOMEM;
+  drop_graphs(c);
   std::vector<SysParam> z(n - c->nsys_cap);
   std::vector<SysState> zs(n - c->nsys_cap);
   memset(z.data(), 0, z.size() * sizeof(SysParam));
@@ -397,12 +409,16 @@ int upload_params(ndg_ctx *c) {
   }
   // stage the tables in shared memory when every system's fit (B200 allows
   // 227 KB per block; keep room for two resident blocks per SM)
-  int stab = 0;
+  int stab = 0, lean = 0;
   for (auto &h : c->sys)
-    if (h.alive) stab = std::max(stab, stab_bytes(h.ntypes, h.npairs, h.ptsize));
-  if (stab > 100 * 1024) stab = 0;
-  if (stab != c->stab_smem) {
+    if (h.alive) {
+      stab = std::max(stab, stab_bytes(h.ntypes, h.npairs, h.ptsize));
+      lean = std::max(lean, stab_bytes_lean(h.ntypes, h.npairs, h.ptsize));
+    }
+  if (stab > 100 * 1024) stab = lean = 0;
+  if (stab != c->stab_smem || lean != c->stab_lean) {
     c->stab_smem = stab;
+    c->stab_lean = lean;
     drop_graphs(c);
   }
   // neighbour build: 3072 staged candidates (16 B position + 4 B slot each)
@@ -661,7 +677,7 @@ void enqueue_steps(ndg_ctx *c, int nsteps) {
   const int tpa = choose_tpa(c);
   for (int k = 0; k < nsteps; ++k) {
     launch_rebuild(d, c->st, 1, mixed);
-    launch_integrate1(d, c->st, 0, mixed);
+    launch_integrate1(d, c->st, 0, mixed, tpa);
     launch_pair(d, c->st, tpa, mixed, 1, 0);
   }
 }
@@ -728,7 +744,7 @@ int capture_block(ndg_ctx *c, int g, cudaGraphExec_t *out) {
     launch_rebuild(d, c->st2, 1, mixed);
     cudaGraph_t body_out;
     CK(c, cudaStreamEndCapture(c->st2, &body_out));
-    launch_integrate1(d, c->st, 0, mixed);
+    launch_integrate1(d, c->st, 0, mixed, tpa);
     launch_pair(d, c->st, tpa, mixed, 1, 0, k + 1 < g ? (unsigned long long)h[k + 1] : 0ull);
   }
   cudaGraph_t done;
@@ -795,7 +811,7 @@ ndg_ctx::~ndg_ctx() {
   drop_graphs(this);
   void *ptrs[] = {dP, dS, chunk_sys, cell_sys, pos, s_pos, pfx, vel, acc, disp, force, s_vel,
                   s_acc, gid, s_gid, s_cell, nnb, atom_cell, atom_slot, perm, tmp_src, tmp_key,
-                  cell_count, cell_start, rb_list, nbr, tile_rows, red, itop, ired, pairmat, mass, rc2, rlist2,
+                  cell_count, cell_start, rb_list, plan, plan_kb, plan_hdr, nbr, tile_rows, red, itop, ired, pairmat, mass, rc2, rlist2,
                   vdr2, rc2f, tabF, tabP, tabF2, tabP2, ring, ring_count};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -1628,7 +1644,7 @@ int ndg_profile_run(ndg_ctx *c, int nsteps) {
     CK(c, cudaEventRecord(ev[4 * k], c->st));
     launch_rebuild(d, c->st, 1, mixed);
     CK(c, cudaEventRecord(ev[4 * k + 1], c->st));
-    launch_integrate1(d, c->st, 0, mixed);
+    launch_integrate1(d, c->st, 0, mixed, tpa);
     CK(c, cudaEventRecord(ev[4 * k + 2], c->st));
     launch_pair(d, c->st, tpa, mixed, 1, 0);
     CK(c, cudaEventRecord(ev[4 * k + 3], c->st));

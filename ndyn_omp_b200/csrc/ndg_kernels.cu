@@ -8,7 +8,9 @@
 // Kernels of one MD step (src/nd.f90:137-178), all systems in one launch:
 //   [rebuild]  k_bin -> k_scan -> k_scatter -> k_order -> k_permute ->
 //              k_copyback -> k_build        (only systems whose check fired)
-//   k_integrate1                           (integrate1 + pending mkIso* scales)
+//   k_integrate1                           (integrate1 + pending mkIso* scales;
+//                                           one more block plans the pair
+//                                           launches' shares of the systems)
 //   k_pair<TPA,MIXED,FUSE>                 (compute0 + integrate2, and in the
 //                                           last block of each system:
 //                                           reductions, write_thermo,
@@ -78,11 +80,124 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double *sm /*NV*32*/)
 }
 
 // ---------------------------------------------------------------------------
+// Work plan of a dynamics step's two pair launches (g0 and g1 blocks), made
+// by one extra block of the step's integrate1 (the flags and lists are set
+// by then).  An active system's tile costs the mean row count of its last
+// list build plus TILE_OVH (the per-tile integration and reduction work);
+// every block of a launch takes the tiles whose first cost unit falls in
+// its equal share of the launch's total, so systems with long lists, short
+// lists or the other launch's flags leave no block idle and no block steps
+// over tiles.
+constexpr int TILE_OVH = 16;
+
+__device__ void plan_block(const DevCtx &c, int g0, int g1) {
+  __shared__ long long w_cost[2][32];
+  __shared__ int w_cnt[2][32];
+  __shared__ long long carry_cost[2];
+  __shared__ int carry_cnt[2];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (threadIdx.x < 2) {
+    carry_cost[threadIdx.x] = 0;
+    carry_cnt[threadIdx.x] = 0;
+  }
+  __syncthreads();
+  for (int base = 0; base < c.nsys_cap; base += blockDim.x) {
+    const int s = base + threadIdx.x;
+    int L = -1, cpt = 0;
+    long long cost = 0;
+    if (s < c.nsys_cap) {
+      const SysParam *P = c.P + s;
+      const SysState *S = c.S + s;
+      const int f = S->flags;  // F_DONE of the last step is being cleared
+      if (P->n > 0 && (f & F_ACTIVE)) {
+        const long long nt = P->npad / TILE;
+        L = (f & (F_CU | F_CV)) ? 1 : 0;
+        cpt = (int)((S->rows + nt / 2) / nt) + TILE_OVH;
+        cost = nt * cpt;
+      }
+    }
+    // block-wide inclusive scans of (systems, cost) of both launches
+    int n0 = L == 0, n1 = L == 1;
+    long long q0 = L == 0 ? cost : 0, q1 = L == 1 ? cost : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y0 = __shfl_up_sync(0xffffffffu, n0, o), y1 = __shfl_up_sync(0xffffffffu, n1, o);
+      const long long z0 = __shfl_up_sync(0xffffffffu, q0, o);
+      const long long z1 = __shfl_up_sync(0xffffffffu, q1, o);
+      if (lane >= o) {
+        n0 += y0;
+        n1 += y1;
+        q0 += z0;
+        q1 += z1;
+      }
+    }
+    if (lane == 31) {
+      w_cnt[0][warp] = n0;
+      w_cnt[1][warp] = n1;
+      w_cost[0][warp] = q0;
+      w_cost[1][warp] = q1;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      int a0 = lane < nw ? w_cnt[0][lane] : 0, a1 = lane < nw ? w_cnt[1][lane] : 0;
+      long long b0 = lane < nw ? w_cost[0][lane] : 0, b1 = lane < nw ? w_cost[1][lane] : 0;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y0 = __shfl_up_sync(0xffffffffu, a0, o), y1 = __shfl_up_sync(0xffffffffu, a1, o);
+        const long long z0 = __shfl_up_sync(0xffffffffu, b0, o);
+        const long long z1 = __shfl_up_sync(0xffffffffu, b1, o);
+        if (lane >= o) {
+          a0 += y0;
+          a1 += y1;
+          b0 += z0;
+          b1 += z1;
+        }
+      }
+      w_cnt[0][lane] = a0;
+      w_cnt[1][lane] = a1;
+      w_cost[0][lane] = b0;
+      w_cost[1][lane] = b1;
+    }
+    __syncthreads();
+    if (L >= 0) {
+      const int k = carry_cnt[L] + (warp ? w_cnt[L][warp - 1] : 0) + (L ? n1 : n0) - 1;
+      const long long cum = carry_cost[L] + (warp ? w_cost[L][warp - 1] : 0) + (L ? q1 : q0) - cost;
+      c.plan[(size_t)L * c.nsys_cap + k] = PlanEnt{cum, s, cpt};
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+      carry_cnt[threadIdx.x] += w_cnt[threadIdx.x][nw - 1];
+      carry_cost[threadIdx.x] += w_cost[threadIdx.x][nw - 1];
+    }
+    __syncthreads();
+  }
+  // block b of launch L starts in the entry whose cost range holds
+  // lo_b = floor(b * tot / G): the blocks with cum * G <= b * tot < end * G
+  for (int L = 0; L < 2; ++L) {
+    const int m = carry_cnt[L], G = L ? g1 : g0;
+    const long long tot = carry_cost[L];
+    const PlanEnt *pl = c.plan + (size_t)L * c.nsys_cap;
+    for (int k = threadIdx.x; k < m; k += blockDim.x) {
+      const long long cum = pl[k].cum, end = k + 1 < m ? pl[k + 1].cum : tot;
+      const long long b0 = (cum * G + tot - 1) / tot, b1 = (end * G + tot - 1) / tot;
+      for (long long b = b0; b < b1 && b < G; ++b) c.plan_kb[L * PLAN_GMAX + b] = k;
+    }
+  }
+  if (threadIdx.x < 2) {
+    c.plan_hdr->tot[threadIdx.x] = carry_cost[threadIdx.x];
+    c.plan_hdr->m[threadIdx.x] = carry_cnt[threadIdx.x];
+  }
+}
+
 // integrate1, src/nd.f90:1027-1046; applies velocity scales left pending by
 // the previous step's mkIsoKE/mkIsoE first (src/nd.f90:1145-1155,1173-1180).
 // Emits each chunk's two largest displacement measures for the next
-// CheckListUpdate.
-__global__ __launch_bounds__(BLOCK) void k_integrate1(DevCtx c, int standalone, int mixed) {
+// CheckListUpdate.  A dynamics step's launch has one more block, which
+// plans the step's pair launches.
+__global__ __launch_bounds__(BLOCK) void k_integrate1(DevCtx c, int standalone, int mixed, int g0,
+                                                     int g1) {
+  if (blockIdx.x == c.nchunks) {  // the extra block of a dynamics step
+    plan_block(c, g0, g1);
+    return;
+  }
   const int chunk = blockIdx.x;
   const int sys = c.chunk_sys[chunk];
   double t1 = 0.0, t2 = 0.0;
@@ -583,7 +698,10 @@ __device__ void scan_system(const DevCtx &c, int s, int counting) {
   SysState *S = c.S + s;
   __shared__ int wsum[32];
   __shared__ int carry;
-  if (threadIdx.x == 0) carry = 0;
+  if (threadIdx.x == 0) {
+    carry = 0;
+    S->rows = 0;  // the build that follows sums its tiles' rows
+  }
   __syncthreads();
   const int ncell = S->ncell;
   int *cnt = c.cell_count + P->cell_off;
@@ -892,7 +1010,10 @@ __device__ __noinline__ void build_tile_direct(const DevCtx &c, int sys, int til
     if ((threadIdx.x & 31) == 0) atomicMax(rows_s, r);
   }
   __syncthreads();
-  if (threadIdx.x == 0) c.tile_rows[tile] = *rows_s;
+  if (threadIdx.x == 0) {
+    c.tile_rows[tile] = *rows_s;
+    atomicAdd(&S->rows, (unsigned long long)*rows_s);
+  }
   if (threadIdx.x < nown) {
     c.nnb[a0 + threadIdx.x] = ncnt[threadIdx.x];
     if (ncnt[threadIdx.x] > maxnb) set_err(c, S, E_NEIMAX);
@@ -1254,7 +1375,10 @@ __device__ void build_tile(const DevCtx &c, int sys, int tile) {
     if ((threadIdx.x & 31) == 0) atomicMax(&rows_s, r);
   }
   __syncthreads();
-  if (threadIdx.x == 0) c.tile_rows[tile] = rows_s;
+  if (threadIdx.x == 0) {
+    c.tile_rows[tile] = rows_s;
+    atomicAdd(&S->rows, (unsigned long long)rows_s);
+  }
   if (threadIdx.x < nown) {
     c.nnb[a0 + threadIdx.x] = ncnt[threadIdx.x];
     if (ncnt[threadIdx.x] > maxnb) set_err(c, S, E_NEIMAX);
@@ -1418,8 +1542,21 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 /
   // mixed EV: 7 fixed-point slots (energy, virial) per thread, after the tables
   unsigned long long *evq = (unsigned long long *)(dsm + (STAB ? c.stab_smem : 0));
   const int G = gridDim.x;
-  const int t0 = (int)((long long)blockIdx.x * ntiles / G);
-  const int t1 = (int)((long long)(blockIdx.x + 1) * ntiles / G);
+  // the block's tiles: in a dynamics step its equal share of the planned
+  // cost of this launch's systems (runs of consecutive tiles, usually of
+  // one or two systems), in standalone compute0 an even split of all tiles
+  // (only tcur, tend and the plan entry kk stay live across tiles; the
+  // block's cost range is worked out again where a system starts)
+  constexpr int L = EV ? 1 : 0;
+  int tcur = 0, tend = 0, kk = -1;
+  if (FUSE) {
+    const long long tot = c.plan_hdr->tot[L];
+    if ((long long)blockIdx.x * tot / G < (long long)(blockIdx.x + 1) * tot / G)
+      kk = c.plan_kb[L * PLAN_GMAX + blockIdx.x];
+  } else {
+    tcur = (int)((long long)blockIdx.x * ntiles / G);
+    tend = (int)((long long)(blockIdx.x + 1) * ntiles / G);
+  }
   int loaded = -1;
   TabView tv;
   __shared__ int last;
@@ -1431,7 +1568,25 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 /
     for (int k = 0; k < 7; ++k) evq[k * NT + threadIdx.x] = 0ull;
   __syncthreads();
 
-  for (int tile = t0; tile < t1; ++tile) {
+  for (;;) {
+    if (tcur >= tend) {
+      // next system of the plan: its tiles whose first cost unit lies in
+      // [lo, hi), tile j starting at cum + j * cpt
+      if (!FUSE || kk < 0 || kk >= c.plan_hdr->m[L]) break;
+      const long long tot = c.plan_hdr->tot[L];
+      const long long lo = (long long)blockIdx.x * tot / G;
+      const long long hi = (long long)(blockIdx.x + 1) * tot / G;
+      const PlanEnt e = c.plan[(size_t)L * c.nsys_cap + kk++];
+      if (e.cum >= hi) break;
+      const SysParam *Pe = c.P + e.sys;
+      const long long nt = Pe->npad / TILE;
+      const long long j0 = lo > e.cum ? (lo - e.cum + e.cpt - 1) / e.cpt : 0;
+      const long long j1 = min(nt, (hi - e.cum + e.cpt - 1) / e.cpt);
+      tcur = Pe->atom_off / TILE + (int)j0;
+      tend = Pe->atom_off / TILE + (int)j1;
+      continue;
+    }
+    const int tile = tcur++;
     const int a0 = tile * TILE;
     const int sys = c.chunk_sys[a0 / ATOM_ALIGN];
     if (sys < 0) continue;
@@ -1453,8 +1608,8 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 /
     }
     // prefetch the next tile's neighbour list (one contiguous region of
     // rows x TILE ints) into L2 while this tile computes
-    if (threadIdx.x == 0 && tile + 1 < t1) {
-      const int nt_ = tile + 1;
+    if (threadIdx.x == 0 && tcur < tend) {
+      const int nt_ = tcur;
       const int ns = c.chunk_sys[nt_ * TILE / ATOM_ALIGN];
       if (ns >= 0) {
         const SysParam *Pn = c.P + ns;
@@ -1801,8 +1956,16 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 /
 
 // ---------------------------------------------------------------------------
 // launchers
-void launch_integrate1(const DevCtx &c, cudaStream_t st, int standalone, int mixed) {
-  k_integrate1<<<c.nchunks, BLOCK, 0, st>>>(c, standalone, mixed);
+static void pair_grids(const DevCtx &c, int tpa, int mixed, int *g);
+
+void launch_integrate1(const DevCtx &c, cudaStream_t st, int standalone, int mixed, int tpa) {
+  if (standalone || !c.plan_hdr) {
+    k_integrate1<<<c.nchunks, BLOCK, 0, st>>>(c, standalone, mixed, 0, 0);
+    return;
+  }
+  int g[2];
+  pair_grids(c, tpa, mixed, g);
+  k_integrate1<<<c.nchunks + 1, BLOCK, 0, st>>>(c, 0, mixed, g[0], g[1]);
 }
 
 static int sm_count() {
@@ -1816,10 +1979,14 @@ static int sm_count() {
   return n;
 }
 
+// grid of a pair-kernel variant (one wave of resident blocks); with launch
+// set, also launches it
 template <int TPA, bool MIXED, bool FUSE, bool STAB, bool EV, int GATHER>
-static void pair_launch(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh) {
+static int pair_launch(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh,
+                       bool launch) {
   auto kern = k_pair<TPA, MIXED, FUSE, STAB, EV, GATHER>;
-  const int smem = (STAB ? c.stab_smem : 0) + ((MIXED && EV) ? 7 * 8 * TILE * TPA : 0);
+  const int smem = (STAB ? (EV ? c.stab_smem : c.stab_lean) : 0) +
+                   ((MIXED && EV) ? 7 * 8 * TILE * TPA : 0);
   static int cfg_smem = -1, occ = 0;
   if (smem != cfg_smem) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -1829,23 +1996,31 @@ static void pair_launch(const DevCtx &c, cudaStream_t st, int hf, unsigned long 
   }
   const int nsm = sm_count();
   const int ntiles = c.nchunks * (ATOM_ALIGN / TILE);
-  const int grid = ntiles < nsm * occ ? ntiles : nsm * occ;
-  kern<<<grid, TILE * TPA, smem, st>>>(c, hf, ntiles, nh);
+  const int grid = std::min(std::min(ntiles, nsm * occ), PLAN_GMAX);
+  if (launch) kern<<<grid, TILE * TPA, smem, st>>>(c, hf, ntiles, nh);
+  return grid;
 }
 
 // the deeper gather only for the mixed one-thread-per-atom loop
 template <int TPA, bool MIXED, bool FUSE, bool STAB, bool EV>
-static void pair_go(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh) {
-  if (MIXED && TPA == 1 && c.gather > 4) pair_launch<TPA, MIXED, FUSE, STAB, EV, 8>(c, st, hf, nh);
-  else pair_launch<TPA, MIXED, FUSE, STAB, EV, 4>(c, st, hf, nh);
+static int pair_go(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh,
+                   bool launch = true) {
+  if (MIXED && TPA == 1 && c.gather > 4)
+    return pair_launch<TPA, MIXED, FUSE, STAB, EV, 8>(c, st, hf, nh, launch);
+  return pair_launch<TPA, MIXED, FUSE, STAB, EV, 4>(c, st, hf, nh, launch);
 }
 
-// FUSE (a dynamics step): the kernel without energy/virial takes the
-// systems whose step needs neither, then the EV kernel the others; each
-// skips the other's tiles.  Standalone compute0: the host flags choose.
+// FUSE (a dynamics step, after the integrate1 that planned it): the kernel
+// without energy/virial takes the systems whose step needs neither, the EV
+// kernel the others.  Standalone compute0: the host flags choose.  With g
+// set, only the two dynamics grids are worked out.
 template <int TPA, bool MIXED, bool FUSE, bool STAB>
-static void pair_ev(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh) {
-  if (FUSE) {
+static void pair_ev(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh, int *g) {
+  if (g) {
+    g[0] = pair_go<TPA, MIXED, FUSE, STAB, false>(c, st, hf, nh, false);
+    g[1] = pair_go<TPA, MIXED, FUSE, STAB, true>(c, st, hf, nh, false);
+  } else if (FUSE) {
+    if (!c.plan_hdr) return;  // no system was ever added
     pair_go<TPA, MIXED, FUSE, STAB, false>(c, st, hf, nh);
     pair_go<TPA, MIXED, FUSE, STAB, true>(c, st, hf, nh);
   } else if (hf & (F_CU | F_CV)) {
@@ -1856,31 +2031,41 @@ static void pair_ev(const DevCtx &c, cudaStream_t st, int hf, unsigned long long
 }
 
 template <int TPA, bool MIXED, bool FUSE>
-static void pair_mode(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh) {
-  if (c.stab_smem <= 0) pair_ev<TPA, MIXED, FUSE, false>(c, st, hf, nh);
-  else pair_ev<TPA, MIXED, FUSE, true>(c, st, hf, nh);
+static void pair_mode(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh, int *g) {
+  if (c.stab_smem <= 0) pair_ev<TPA, MIXED, FUSE, false>(c, st, hf, nh, g);
+  else pair_ev<TPA, MIXED, FUSE, true>(c, st, hf, nh, g);
 }
 
 template <int TPA>
 static void pair_tpa(const DevCtx &c, cudaStream_t st, int mixed, int fuse, int hf,
-                     unsigned long long nh) {
+                     unsigned long long nh, int *g) {
   if (mixed) {
-    if (fuse) pair_mode<TPA, true, true>(c, st, hf, nh);
-    else pair_mode<TPA, true, false>(c, st, hf, nh);
+    if (fuse) pair_mode<TPA, true, true>(c, st, hf, nh, g);
+    else pair_mode<TPA, true, false>(c, st, hf, nh, g);
   } else {
-    if (fuse) pair_mode<TPA, false, true>(c, st, hf, nh);
-    else pair_mode<TPA, false, false>(c, st, hf, nh);
+    if (fuse) pair_mode<TPA, false, true>(c, st, hf, nh, g);
+    else pair_mode<TPA, false, false>(c, st, hf, nh, g);
+  }
+}
+
+static void pair_dispatch(const DevCtx &c, cudaStream_t st, int tpa, int mixed, int fuse, int hf,
+                          unsigned long long next_h, int *g) {
+  switch (tpa) {
+    case 1: pair_tpa<1>(c, st, mixed, fuse, hf, next_h, g); break;
+    case 2: pair_tpa<2>(c, st, mixed, fuse, hf, next_h, g); break;
+    case 4: pair_tpa<4>(c, st, mixed, fuse, hf, next_h, g); break;
+    default: pair_tpa<8>(c, st, mixed, fuse, hf, next_h, g); break;
   }
 }
 
 void launch_pair(const DevCtx &c, cudaStream_t st, int tpa, int mixed, int fuse, int hf,
                  unsigned long long next_h) {
-  switch (tpa) {
-    case 1: pair_tpa<1>(c, st, mixed, fuse, hf, next_h); break;
-    case 2: pair_tpa<2>(c, st, mixed, fuse, hf, next_h); break;
-    case 4: pair_tpa<4>(c, st, mixed, fuse, hf, next_h); break;
-    default: pair_tpa<8>(c, st, mixed, fuse, hf, next_h); break;
-  }
+  pair_dispatch(c, st, tpa, mixed, fuse, hf, next_h, nullptr);
+}
+
+// the grids of a dynamics step's two pair launches
+static void pair_grids(const DevCtx &c, int tpa, int mixed, int *g) {
+  pair_dispatch(c, 0, tpa, mixed, 1, 0, 0ull, g);
 }
 
 __global__ void k_decide(DevCtx c, unsigned long long h) {

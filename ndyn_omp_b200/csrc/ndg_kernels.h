@@ -6,6 +6,20 @@
 
 namespace ndg {
 
+// Work plan of the two pair launches of a dynamics step (made by integrate1): launch L
+// (0 without energy/virial, 1 with) lists its systems in id order with the
+// exclusive prefix of their cost, and names for each of its blocks the
+// entry that holds the block's first unit of cost.
+struct PlanEnt {
+  long long cum;  // cost of the launch's earlier systems
+  int sys, cpt;   // system, cost of one of its tiles
+};
+struct PlanHdr {
+  long long tot[2];  // total cost of each launch
+  int m[2];          // systems of each launch
+};
+constexpr int PLAN_GMAX = 8192;  // largest pair-kernel grid the plan covers
+
 // Everything a kernel needs, passed by value (pointers into the arenas).
 struct DevCtx {
   const SysParam *P;
@@ -14,6 +28,7 @@ struct DevCtx {
   const int *cell_sys;   // per global cell: system id or -1
   int nchunks, ncells, nsys_cap;
   int stab_smem;  // shared-memory bytes of the staged pair tables, 0 = read from global
+  int stab_lean;  // the same without the energy table (kernel without energy/virial)
   int nb_smem;  // neighbour build dynamic smem
   int nb_vcap;  // flat candidate-list capacity of the build
   int gather;   // mixed pair loop: neighbour gathers in flight (4 or 8)
@@ -41,11 +56,16 @@ struct DevCtx {
   int *ring_count;  // [0] records written, [1] error bits of any system,
                     // [2] largest tile candidate count, [3] systems on rb_list
   int *rb_list;     // systems whose lists the next rebuild group rebuilds
+  PlanEnt *plan;    // 2 x nsys_cap entries
+  int *plan_kb;     // 2 x PLAN_GMAX block starts
+  PlanHdr *plan_hdr;
   int ring_cap;
 };
 
 // launchers (stream-ordered; safe to capture in a CUDA graph)
-void launch_integrate1(const DevCtx &c, cudaStream_t st, int standalone, int mixed);
+// a dynamics step's integrate1 (standalone 0) also plans the step's pair
+// launches for tpa threads per atom
+void launch_integrate1(const DevCtx &c, cudaStream_t st, int standalone, int mixed, int tpa = 1);
 // next_h: conditional-node handle of the next step's rebuild group (0 when
 // not launched inside a captured step block)
 void launch_pair(const DevCtx &c, cudaStream_t st, int tpa, int mixed, int fuse, int host_flags,
@@ -69,6 +89,11 @@ NDG_HD int stab_bytes(int ntypes, int npairs, int ptsize) {
   b += npairs * 16;  // packed float4 per pair
   b += npairs * (ptsize + 1) * 16;  // F and P: a double each, or a float2 each
   return b;
+}
+
+// the staged layout without the P table
+NDG_HD int stab_bytes_lean(int ntypes, int npairs, int ptsize) {
+  return stab_bytes(ntypes, npairs, ptsize) - npairs * (ptsize + 1) * 8;
 }
 
 // stencil of neighbour cells for a link-cell grid (shared host/device)
