@@ -67,6 +67,7 @@ struct HostSys {
   int n = 0, ntypes = 0, npairs = 0, ptsize = 0;
   double ptrmin = 0.25;
   std::vector<double> mass, rcpair, ppair, fpair;
+  std::vector<float2> tF2, tP2;  // FP32 (k, k+1) pairs of fpair and ppair
   std::vector<int> pairmat;
   ndg_control ctl{};
   Range atoms, cells, nbr;  // atoms/cells in elements, nbr in ints
@@ -112,6 +113,8 @@ struct ndg_ctx {
   int *cell_count = nullptr, *cell_start = nullptr;
   int *nbr = nullptr;
   int *tile_rows = nullptr;
+  char *pin = nullptr;  // pinned host staging of atom copies (reused)
+  size_t pin_cap = 0;
   int *rb_list = nullptr;  // systems listed for a list rebuild
   PlanEnt *plan = nullptr;  // pair-launch work plan (integrate1's extra block)
   int *plan_kb = nullptr;
@@ -374,6 +377,13 @@ int upload_params(ndg_ctx *c) {
   std::vector<float2> tF2, tP2;
   std::vector<SysParam> prm(c->nsys_cap);
   memset(prm.data(), 0, prm.size() * sizeof(SysParam));
+  size_t ntab = 0;
+  for (auto &h : c->sys)
+    if (h.alive) ntab += h.fpair.size();
+  tabF.reserve(ntab);
+  tabP.reserve(ntab);
+  tF2.reserve(ntab);
+  tP2.reserve(ntab);
   for (size_t s = 0; s < c->sys.size(); ++s) {
     HostSys &h = c->sys[s];
     if (!h.alive) continue;
@@ -394,17 +404,11 @@ int upload_params(ndg_ctx *c) {
       vdr2.push_back((float)(1.0 / pdr2));  // vPTdr2 = real(1.d0/PTdr2), src/nd.f90:254
       const double rl = skin + r;            // rcuts2 = skin + PairParams(1,.), :1375
       rlist2.push_back(rl * rl);
-      const int T = h.ptsize + 1;
-      for (int k = 0; k < T; ++k) {
-        const double f0 = h.fpair[(size_t)j * T + k], p0 = h.ppair[(size_t)j * T + k];
-        const double f1 = k + 1 < T ? h.fpair[(size_t)j * T + k + 1] : f0;
-        const double p1 = k + 1 < T ? h.ppair[(size_t)j * T + k + 1] : p0;
-        tabF.push_back(f0);
-        tabP.push_back(p0);
-        tF2.push_back(make_float2((float)f0, (float)f1));
-        tP2.push_back(make_float2((float)p0, (float)p1));
-      }
     }
+    tabF.insert(tabF.end(), h.fpair.begin(), h.fpair.end());
+    tabP.insert(tabP.end(), h.ppair.begin(), h.ppair.end());
+    tF2.insert(tF2.end(), h.tF2.begin(), h.tF2.end());
+    tP2.insert(tP2.end(), h.tP2.begin(), h.tP2.end());
     prm[s] = p;
   }
   // stage the tables in shared memory when every system's fit (B200 allows
@@ -416,6 +420,14 @@ int upload_params(ndg_ctx *c) {
       lean = std::max(lean, stab_bytes_lean(h.ntypes, h.npairs, h.ptsize));
     }
   if (stab > 100 * 1024) stab = lean = 0;
+  // a high-water mark while systems come and go (a change re-captures the
+  // step graphs), unless staging is off or no system is left
+  bool any = false;
+  for (auto &h : c->sys) any |= h.alive;
+  if (stab > 0 && c->stab_smem > 0 && any) {
+    stab = std::max(stab, c->stab_smem);
+    lean = std::max(lean, c->stab_lean);
+  }
   if (stab != c->stab_smem || lean != c->stab_lean) {
     c->stab_smem = stab;
     c->stab_lean = lean;
@@ -495,26 +507,54 @@ int put_state_dev(ndg_ctx *c, int s, const SysState &S) {
 }
 
 // upload atoms in caller order (identity permutation)
+// pinned host memory of at least `bytes` for the atom copies, or nullptr
+char *pinned(ndg_ctx *c, size_t bytes) {
+  if (bytes <= c->pin_cap) return c->pin;
+  if (c->pin) cudaFreeHost(c->pin);
+  c->pin = nullptr;
+  const size_t want = std::max(bytes, c->pin_cap + c->pin_cap / 2);
+  c->pin_cap = 0;
+  if (cudaHostAlloc((void **)&c->pin, want, cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    c->pin = nullptr;
+    return nullptr;
+  }
+  c->pin_cap = want;
+  return c->pin;
+}
+
 int upload_atoms(ndg_ctx *c, int s, const int *typ, const double *pos, const double *vel,
                  const double *acc) {
   HostSys &h = c->sys[s];
   const int n = h.n;
   const size_t off = (size_t)h.atoms.off * ATOM_ALIGN;
-  std::vector<double4> p4(n);
-  std::vector<int> g(n);
+  // staged in pinned memory: positions (with type words) | slots | velocities
+  // | accelerations, then copied in one stream-ordered batch
+  const size_t bp = (size_t)n * sizeof(double4), bg = ((size_t)n * sizeof(int) + 15) / 16 * 16;
+  const size_t b3 = 3 * (size_t)n * sizeof(double);
+  const size_t total = bp + bg + (vel ? b3 : 0) + (acc ? b3 : 0);
+  std::vector<char> pageable;
+  char *buf = pinned(c, total);
+  if (!buf) {
+    pageable.resize(total);
+    buf = pageable.data();
+  }
+  double4 *p4 = (double4 *)buf;
+  int *g = (int *)(buf + bp);
+  double *vs = (double *)(buf + bp + bg), *as = vs + (vel ? 3 * (size_t)n : 0);
   std::vector<int> tw(n);
   if (typ) {
     for (int i = 0; i < n; ++i) tw[i] = pack_tw(typ[i], s);
   } else {
-    // keep the types already on the device (they are in pos.w, device order)
-    std::vector<double4> old(n);
-    std::vector<int> og(n);
-    CK(c, cudaMemcpy(old.data(), c->pos + off, n * sizeof(double4), cudaMemcpyDeviceToHost));
-    CK(c, cudaMemcpy(og.data(), c->gid + off, n * sizeof(int), cudaMemcpyDeviceToHost));
+    // keep the types already on the device (they are in pos.w, device
+    // order), read through the same staging
+    CK(c, cudaMemcpyAsync(p4, c->pos + off, bp, cudaMemcpyDeviceToHost, c->st));
+    CK(c, cudaMemcpyAsync(g, c->gid + off, n * sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    CK(c, cudaStreamSynchronize(c->st));
     for (int i = 0; i < n; ++i) {
       long long w;
-      memcpy(&w, &old[i].w, 8);
-      tw[og[i]] = (int)w;
+      memcpy(&w, &p4[i].w, 8);
+      tw[g[i]] = (int)w;
     }
   }
   for (int i = 0; i < n; ++i) {
@@ -524,14 +564,17 @@ int upload_atoms(ndg_ctx *c, int s, const int *typ, const double *pos, const dou
     p4[i] = make_double4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], wd);
     g[i] = i;
   }
-  CK(c, cudaMemcpy(c->pos + off, p4.data(), n * sizeof(double4), cudaMemcpyHostToDevice));
-  CK(c, cudaMemcpy(c->gid + off, g.data(), n * sizeof(int), cudaMemcpyHostToDevice));
-  std::vector<double> z(3 * (size_t)n, 0.0);
-  CK(c, cudaMemcpy(c->vel + 3 * off, vel ? vel : z.data(), 3 * n * sizeof(double),
-                   cudaMemcpyHostToDevice));
-  CK(c, cudaMemcpy(c->acc + 3 * off, acc ? acc : z.data(), 3 * n * sizeof(double),
-                   cudaMemcpyHostToDevice));
-  CK(c, cudaMemcpy(c->disp + 3 * off, z.data(), 3 * n * sizeof(double), cudaMemcpyHostToDevice));
+  if (vel) memcpy(vs, vel, b3);
+  if (acc) memcpy(as, acc, b3);
+  cudaStream_t st = c->st;
+  CK(c, cudaMemcpyAsync(c->pos + off, p4, bp, cudaMemcpyHostToDevice, st));
+  CK(c, cudaMemcpyAsync(c->gid + off, g, n * sizeof(int), cudaMemcpyHostToDevice, st));
+  if (vel) CK(c, cudaMemcpyAsync(c->vel + 3 * off, vs, b3, cudaMemcpyHostToDevice, st));
+  else CK(c, cudaMemsetAsync(c->vel + 3 * off, 0, b3, st));
+  if (acc) CK(c, cudaMemcpyAsync(c->acc + 3 * off, as, b3, cudaMemcpyHostToDevice, st));
+  else CK(c, cudaMemsetAsync(c->acc + 3 * off, 0, b3, st));
+  CK(c, cudaMemsetAsync(c->disp + 3 * off, 0, b3, st));
+  CK(c, cudaStreamSynchronize(st));  // the staging buffer is reused
   h.lists_valid = false;
   return NDG_OK;
 }
@@ -815,6 +858,7 @@ ndg_ctx::~ndg_ctx() {
                   vdr2, rc2f, tabF, tabP, tabF2, tabP2, ring, ring_count};
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  if (pin) cudaFreeHost(pin);
   if (st) cudaStreamDestroy(st);
   if (st2) cudaStreamDestroy(st2);
 }
@@ -1011,6 +1055,18 @@ int ndg_add_system(ndg_ctx *c, int np, int ntypes, int npairs, int ptsize, doubl
   h.rcpair.assign(rcpair, rcpair + npairs);
   h.ppair.assign(ppair, ppair + (size_t)(ptsize + 1) * npairs);
   h.fpair.assign(fpair, fpair + (size_t)(ptsize + 1) * npairs);
+  {
+    // the mixed kernel's tables: entry k holds values k and k+1 in FP32
+    const int T = ptsize + 1;
+    h.tF2.resize((size_t)T * npairs);
+    h.tP2.resize((size_t)T * npairs);
+    for (int j = 0; j < npairs; ++j)
+      for (int k = 0; k < T; ++k) {
+        const size_t a = (size_t)j * T + k, b = k + 1 < T ? a + 1 : a;
+        h.tF2[a] = make_float2((float)h.fpair[a], (float)h.fpair[b]);
+        h.tP2[a] = make_float2((float)h.ppair[a], (float)h.ppair[b]);
+      }
+  }
   h.rcut = *std::max_element(rcpair, rcpair + npairs);  // src/potentials.f90:36
   ndg_default_control(&h.ctl);
   const long long nch = (np + ATOM_ALIGN - 1) / ATOM_ALIGN;
@@ -1072,8 +1128,13 @@ int ndg_remove_system(ndg_ctx *c, int s) {
   memset(&S, 0, sizeof(S));
   int rc = put_state_dev(c, s, S);
   if (rc) return rc;
+  // no kernel sees the system from here on; the other systems' parameters
+  // are packed again once, before the next launch that needs them
+  SysParam z;
+  memset(&z, 0, sizeof(z));
+  CK(c, cudaMemcpy(c->dP + s, &z, sizeof(z), cudaMemcpyHostToDevice));
   c->params_dirty = true;
-  return ensure_params(c);
+  return NDG_OK;
 }
 
 int ndg_num_systems(const ndg_ctx *c) {
@@ -1116,29 +1177,38 @@ int ndg_get_state(ndg_ctx *c, int s, double *pos, double *vel, double *acc, doub
   HostSys &h = c->sys[s];
   const int n = h.n;
   const size_t off = (size_t)h.atoms.off * ATOM_ALIGN;
-  CK(c, cudaStreamSynchronize(c->st));
-  std::vector<int> g(n);
-  CK(c, cudaMemcpy(g.data(), c->gid + off, n * sizeof(int), cudaMemcpyDeviceToHost));
-  if (pos) {
-    std::vector<double4> p(n);
-    CK(c, cudaMemcpy(p.data(), c->pos + off, n * sizeof(double4), cudaMemcpyDeviceToHost));
+  // one stream-ordered batch of copies into pinned staging: slots |
+  // positions | velocities | accelerations, then scattered to input order
+  const size_t bg = ((size_t)n * sizeof(int) + 15) / 16 * 16, bp = (size_t)n * sizeof(double4);
+  const size_t b3 = 3 * (size_t)n * sizeof(double);
+  const size_t total = bg + (pos ? bp : 0) + (vel ? b3 : 0) + (acc ? b3 : 0);
+  std::vector<char> pageable;
+  char *buf = pinned(c, total);
+  if (!buf) {
+    pageable.resize(total);
+    buf = pageable.data();
+  }
+  int *g = (int *)buf;
+  double4 *p = (double4 *)(buf + bg);
+  double *vt = (double *)(buf + bg + (pos ? bp : 0)), *at = vt + (vel ? 3 * (size_t)n : 0);
+  cudaStream_t st = c->st;
+  CK(c, cudaMemcpyAsync(g, c->gid + off, n * sizeof(int), cudaMemcpyDeviceToHost, st));
+  if (pos) CK(c, cudaMemcpyAsync(p, c->pos + off, bp, cudaMemcpyDeviceToHost, st));
+  if (vel) CK(c, cudaMemcpyAsync(vt, c->vel + 3 * off, b3, cudaMemcpyDeviceToHost, st));
+  if (acc) CK(c, cudaMemcpyAsync(at, c->acc + 3 * off, b3, cudaMemcpyDeviceToHost, st));
+  CK(c, cudaStreamSynchronize(st));
+  if (pos)
     for (int i = 0; i < n; ++i) {
       pos[3 * g[i]] = p[i].x;
       pos[3 * g[i] + 1] = p[i].y;
       pos[3 * g[i] + 2] = p[i].z;
     }
-  }
-  std::vector<double> t(3 * (size_t)n);
-  if (vel) {
-    CK(c, cudaMemcpy(t.data(), c->vel + 3 * off, 3 * n * sizeof(double), cudaMemcpyDeviceToHost));
+  if (vel)
     for (int i = 0; i < n; ++i)
-      for (int d = 0; d < 3; ++d) vel[3 * g[i] + d] = t[3 * i + d];
-  }
-  if (acc) {
-    CK(c, cudaMemcpy(t.data(), c->acc + 3 * off, 3 * n * sizeof(double), cudaMemcpyDeviceToHost));
+      for (int d = 0; d < 3; ++d) vel[3 * g[i] + d] = vt[3 * i + d];
+  if (acc)
     for (int i = 0; i < n; ++i)
-      for (int d = 0; d < 3; ++d) acc[3 * g[i] + d] = t[3 * i + d];
-  }
+      for (int d = 0; d < 3; ++d) acc[3 * g[i] + d] = at[3 * i + d];
   if (box) {
     SysState S;
     int rc = get_state_dev(c, s, S);
