@@ -51,6 +51,18 @@ enum : int {
                    // step's flags, cleared by the next integrate1)
 };
 
+// Entry (ti, tj) of the pair kernel's gather matrix: the table of the force
+// on an atom of type ti from one of type tj, max(PairMat(ti,tj),
+// PairMat(tj,ti)), when PairMat(tj,ti) > 0 and else 0, with PT_ASYM set
+// where the two directions differ (compute1, src/nd.f90:447,474-498: such
+// pairs add no energy and no virial).  Symmetric matrices gather PairMat.
+constexpr int PT_ASYM = 1 << 16, PT_MASK = PT_ASYM - 1;
+NDG_HD int gather_entry(const int *pm, int nt, int ti, int tj) {
+  const int ij = pm[(ti - 1) + (tj - 1) * nt], ji = pm[(tj - 1) + (ti - 1) * nt];
+  if (ji <= 0) return 0;
+  return (ij > ji ? ij : ji) | (ij != ji ? PT_ASYM : 0);
+}
+
 // error bits (SysState::err)
 enum : int { E_NEIMAX = 1, E_OUT_OF_BOX = 2, E_CELLS = 4 };
 

@@ -97,7 +97,7 @@ struct ndg_ctx {
   // arenas
   Arena atoms, cells, nbrs;  // atoms in chunks, cells in cells, nbrs in ints
   int nsys_cap = 0;
-  size_t cap_pm = 0, cap_mass = 0, cap_rc2 = 0, cap_rlist2 = 0, cap_vdr2 = 0, cap_rc2f = 0,
+  size_t cap_pm = 0, cap_pg = 0, cap_mass = 0, cap_rc2 = 0, cap_rlist2 = 0, cap_vdr2 = 0, cap_rc2f = 0,
          cap_tabF = 0, cap_tabP = 0, cap_tabF2 = 0, cap_tabP2 = 0;
   // device buffers
   SysParam *dP = nullptr;
@@ -120,7 +120,7 @@ struct ndg_ctx {
   int *plan_kb = nullptr;
   PlanHdr *plan_hdr = nullptr;
   double *red = nullptr, *itop = nullptr, *ired = nullptr;
-  int *pairmat = nullptr;
+  int *pairmat = nullptr, *pairg = nullptr;
   double *mass = nullptr, *rc2 = nullptr, *rlist2 = nullptr;
   float *vdr2 = nullptr, *rc2f = nullptr;
   double *tabF = nullptr, *tabP = nullptr;
@@ -206,6 +206,7 @@ DevCtx devctx(ndg_ctx *c) {
   d.s_gid = c->s_gid;
   d.s_cell = c->s_cell;
   d.pairmat = c->pairmat;
+  d.pairg = c->pairg;
   d.mass = c->mass;
   d.rc2 = c->rc2;
   d.rlist2 = c->rlist2;
@@ -371,7 +372,7 @@ int upload_vec(ndg_ctx *c, T *&dst, size_t &cap, const std::vector<T> &v) {
 
 // small per-pair/per-type arrays: rebuilt for all systems on any change
 int upload_params(ndg_ctx *c) {
-  std::vector<int> pm;
+  std::vector<int> pm, pg;
   std::vector<double> mass, rc2, rlist2, tabF, tabP;
   std::vector<float> vdr2, rc2f;
   std::vector<float2> tF2, tP2;
@@ -393,6 +394,8 @@ int upload_params(ndg_ctx *c) {
     p.type_off = (int)mass.size();
     p.pm_off = (int)pm.size();
     pm.insert(pm.end(), h.pairmat.begin(), h.pairmat.end());
+    for (int b = 1; b <= h.ntypes; ++b)
+      for (int a = 1; a <= h.ntypes; ++a) pg.push_back(gather_entry(h.pairmat.data(), h.ntypes, a, b));
     mass.insert(mass.end(), h.mass.begin(), h.mass.end());
     const double skin = h.ctl.skin < 0 ? 0.2 * h.rcut : h.ctl.skin;
     for (int j = 0; j < h.npairs; ++j) {
@@ -444,6 +447,7 @@ int upload_params(ndg_ctx *c) {
   }
   int rc = 0;
   rc |= upload_vec(c, c->pairmat, c->cap_pm, pm);
+  rc |= upload_vec(c, c->pairg, c->cap_pg, pg);
   rc |= upload_vec(c, c->mass, c->cap_mass, mass);
   rc |= upload_vec(c, c->rc2, c->cap_rc2, rc2);
   rc |= upload_vec(c, c->rlist2, c->cap_rlist2, rlist2);
@@ -854,7 +858,7 @@ ndg_ctx::~ndg_ctx() {
   drop_graphs(this);
   void *ptrs[] = {dP, dS, chunk_sys, cell_sys, pos, s_pos, pfx, vel, acc, disp, force, s_vel,
                   s_acc, gid, s_gid, s_cell, nnb, atom_cell, atom_slot, perm, tmp_src, tmp_key,
-                  cell_count, cell_start, rb_list, plan, plan_kb, plan_hdr, nbr, tile_rows, red, itop, ired, pairmat, mass, rc2, rlist2,
+                  cell_count, cell_start, rb_list, plan, plan_kb, plan_hdr, nbr, tile_rows, red, itop, ired, pairmat, pairg, mass, rc2, rlist2,
                   vdr2, rc2f, tabF, tabP, tabF2, tabP2, ring, ring_count};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -1021,11 +1025,8 @@ int ndg_add_system(ndg_ctx *c, int np, int ntypes, int npairs, int ptsize, doubl
     if (typ[i] < 1 || typ[i] > ntypes) return NDG_ERR_ARG;
   for (int k = 0; k < ntypes * ntypes; ++k)
     if (pairmat[k] < 0 || pairmat[k] > npairs) return NDG_ERR_ARG;
-  // one-sided ('asym') pairs take the compute1 path, which this library
-  // does not provide: PairMat must be symmetric (src/nd.f90:155-163)
-  for (int a = 0; a < ntypes; ++a)
-    for (int b = 0; b < ntypes; ++b)
-      if (pairmat[a + b * ntypes] != pairmat[b + a * ntypes]) return NDG_ERR_ARG;
+  // a PairMat with one-sided ('asym') entries selects compute1's rules
+  // (src/nd.f90:155-163): the kernels read it through the gather matrix
   cudaSetDevice(c->device);
   int s = -1;
   for (size_t k = 0; k < c->sys.size(); ++k)

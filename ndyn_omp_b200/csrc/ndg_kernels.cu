@@ -1436,7 +1436,7 @@ __device__ void stage_tables(const DevCtx &c, const SysParam *P, unsigned char *
   off = (off + np * 8 + 15) / 16 * 16;
   float4 *pp = (float4 *)(sm + off);
   off += np * 16;
-  for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) pm[k] = c.pairmat[P->pm_off + k];
+  for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) pm[k] = c.pairg[P->pm_off + k];
   for (int k = threadIdx.x; k < np; k += blockDim.x) {
     rc2[k] = c.rc2[P->pair_off + k];
     const float r = c.rc2f[P->pair_off + k];
@@ -1469,7 +1469,7 @@ __device__ void stage_tables(const DevCtx &c, const SysParam *P, unsigned char *
 }
 
 __device__ __forceinline__ void global_tables(const DevCtx &c, const SysParam *P, TabView &tv) {
-  tv.pm = c.pairmat + P->pm_off;
+  tv.pm = c.pairg + P->pm_off;
   tv.rc2 = c.rc2 + P->pair_off;
   tv.rc2f = c.rc2f + P->pair_off;
   tv.vdr2 = c.vdr2 + P->pair_off;
@@ -1662,7 +1662,9 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 /
             for (int q = 0; q < UNR_D; ++q) pj[q] = c.pos[qq[q] >= 0 ? qq[q] : i];
 #pragma unroll
             for (int q = 0; q < UNR_D; ++q) {
-              const int pt = ONE ? 1 : pmr[(tw_type(tw_of(pj[q].w)) - 1) * ntypes];
+              const int pg = ONE ? 1 : pmr[(tw_type(tw_of(pj[q].w)) - 1) * ntypes];
+              const int pt = pg & PT_MASK;
+              const bool sym = ONE || pg < PT_ASYM;  // energy and virial count
               const int p1 = ONE ? 0 : (pt > 0 ? pt - 1 : 0);
               double s0 = pi.x - pj[q].x, s1 = pi.y - pj[q].y, s2 = pi.z - pj[q].z;
               s0 = s0 - round(s0);
@@ -1684,8 +1686,8 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 /
               fx = fx + r0 * df;
               fy = fy + r1 * df;
               fz = fz + r2 * df;
-              if (cu && ok) pe = pe + (w * tv.tP[base + 1] + (1.0 - w) * tv.tP[base]);
-              if (cv) {
+              if (cu && ok && sym) pe = pe + (w * tv.tP[base + 1] + (1.0 - w) * tv.tP[base]);
+              if (cv && sym) {
                 vir[0] = vir[0] + r0 * r0 * df;
                 vir[1] = vir[1] + r1 * r1 * df;
                 vir[2] = vir[2] + r2 * r2 * df;
@@ -1727,7 +1729,9 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 /
               for (int q = 0; q < GATHER; ++q) pj[q] = c.pfx[qq[h + q] >= 0 ? qq[h + q] : i];
 #pragma unroll
               for (int q = 0; q < GATHER; ++q) {
-                const int pt = ONE ? 1 : pmr[(tw_type(pj[q].w) - 1) * ntypes];
+                const int pg = ONE ? 1 : pmr[(tw_type(pj[q].w) - 1) * ntypes];
+                const int pt = pg & PT_MASK;
+                const bool sym = ONE || pg < PT_ASYM;  // energy and virial count
                 const int p1 = ONE ? 0 : (pt > 0 ? pt - 1 : 0);
                 const float4 prm = ONE ? pp1 : pair_params<STAB>(tv, p1);
                 // minimum image by 32-bit wrap-around of the fixed-point difference
@@ -1749,15 +1753,16 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 /
                 ax = __fmaf_rn(r0, df, ax);
                 ay = __fmaf_rn(r1, df, ay);
                 az = __fmaf_rn(r2, df, az);
-                if (cu && ok) {
+                if (cu && ok && sym) {
                   const float2 Pp = tv.tP2[base];
                   ape += __fmaf_rn(w, Pp.y - Pp.x, Pp.x);
                 }
                 if (cv) {
-                  const float r0d = r0 * df, r1d = r1 * df;
+                  const float dv = sym ? df : 0.f;
+                  const float r0d = r0 * dv, r1d = r1 * dv;
                   av0 = __fmaf_rn(r0d, r0, av0);
                   av1 = __fmaf_rn(r1d, r1, av1);
-                  av2 = __fmaf_rn(r2 * df, r2, av2);
+                  av2 = __fmaf_rn(r2 * dv, r2, av2);
                   av3 = __fmaf_rn(r0d, r1, av3);
                   av4 = __fmaf_rn(r0d, r2, av4);
                   av5 = __fmaf_rn(r1d, r2, av5);
@@ -1775,7 +1780,9 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 /
                 nm &= nm - 1;
                 const int j = __ldg(nb + (kb + q) * TILE);
                 const int4 pj = c.pfx[j];
-                const int p1 = ONE ? 0 : pmr[(tw_type(pj.w) - 1) * ntypes] - 1;
+                const int pg = ONE ? 1 : pmr[(tw_type(pj.w) - 1) * ntypes];
+                const bool sym = ONE || pg < PT_ASYM;
+                const int p1 = (pg & PT_MASK) - 1;
                 const double4 pjd = c.pos[j];
                 double s0 = pid.x - pjd.x, s1 = pid.y - pjd.y, s2 = pid.z - pjd.z;
                 s0 = s0 - round(s0);
@@ -1801,11 +1808,11 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 /
                 ax = __fmaf_rn(r0, df, ax);
                 ay = __fmaf_rn(r1, df, ay);
                 az = __fmaf_rn(r2, df, az);
-                if (cu) {
+                if (cu && sym) {
                   const float2 Pp = tv.tP2[base];
                   ape += __fmaf_rn(w, Pp.y - Pp.x, Pp.x);
                 }
-                if (cv) {
+                if (cv && sym) {
                   const float r0d = r0 * df, r1d = r1 * df;
                   av0 = __fmaf_rn(r0d, r0, av0);
                   av1 = __fmaf_rn(r1d, r1, av1);

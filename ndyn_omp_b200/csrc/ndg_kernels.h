@@ -44,7 +44,8 @@ struct DevCtx {
   double4 *s_pos;
   double *s_vel, *s_acc;
   int *s_gid, *s_cell;
-  const int *pairmat;
+  const int *pairmat;  // PairMat per system (the list build)
+  const int *pairg;    // gather matrix per system (the pair kernel)
   const double *mass, *rc2, *rlist2;
   const float *vdr2, *rc2f;
   const double *tabF, *tabP;

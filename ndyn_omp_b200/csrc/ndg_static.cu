@@ -40,7 +40,7 @@ constexpr int STATIC_MAX_BLOCKS = (STATIC_MAX_ATOMS + SB - 1) / SB;
 struct StaticParams {
   int np, ntypes, npairs, ptsize, ncell, nstencil, quirk;
   int mcell[3];
-  int pairmat[STATIC_MAX_TYPES * STATIC_MAX_TYPES];
+  int pairmat[STATIC_MAX_TYPES * STATIC_MAX_TYPES];  // gather matrix (gather_entry)
   int stencil[MAX_STENCIL];
   double ptrmin;
   double box[3];
@@ -163,8 +163,10 @@ __global__ __launch_bounds__(SB) void ks_force(StaticScratch *s, const double *p
       for (int q = s->cell_start[nc]; q < s->cell_start[nc + 1]; ++q) {
         const int j = s->order[q];
         if (j == i) continue;
-        const int pt = p.pairmat[(ti - 1) + (typ[j] - 1) * p.ntypes];
+        const int pg = p.pairmat[(ti - 1) + (typ[j] - 1) * p.ntypes];  // gather matrix
+        const int pt = pg & PT_MASK;
         if (pt <= 0) continue;
+        const double ev = pg < PT_ASYM ? 1.0 : 0.0;  // one-sided pairs: force only
         double s0 = xi - pos[3 * (size_t)j], s1 = yi - pos[3 * (size_t)j + 1],
                s2 = zi - pos[3 * (size_t)j + 2];
         s0 = s0 - round(s0);
@@ -186,13 +188,15 @@ __global__ __launch_bounds__(SB) void ks_force(StaticScratch *s, const double *p
         fx = fx + r0 * df;
         fy = fy + r1 * df;
         fz = fz + r2 * df;
-        pe = pe + (w * tabP[base + 1] + (1.0 - w) * tabP[base]);
-        vir[0] = vir[0] + r0 * r0 * df;
-        vir[1] = vir[1] + r1 * r1 * df;
-        vir[2] = vir[2] + r2 * r2 * df;
-        vir[3] = vir[3] + r0 * r1 * df;
-        vir[4] = vir[4] + r0 * r2 * df;
-        vir[5] = vir[5] + r1 * r2 * df;
+        if (ev != 0.0) {
+          pe = pe + (w * tabP[base + 1] + (1.0 - w) * tabP[base]);
+          vir[0] = vir[0] + r0 * r0 * df;
+          vir[1] = vir[1] + r1 * r1 * df;
+          vir[2] = vir[2] + r2 * r2 * df;
+          vir[3] = vir[3] + r0 * r1 * df;
+          vir[4] = vir[4] + r0 * r2 * df;
+          vir[5] = vir[5] + r1 * r2 * df;
+        }
       }
     }
     force[3 * (size_t)i] = fx;
@@ -293,10 +297,11 @@ extern "C" int ndg_compute0_static(int np, int ntypes, int npairs, int ptsize, d
     return NDG_ERR_ARG;
   }
   p.ncell = ncell;
-  for (int k = 0; k < ntypes * ntypes; ++k) {
+  for (int k = 0; k < ntypes * ntypes; ++k)
     if (pairmat[k] < 0 || pairmat[k] > npairs) return NDG_ERR_ARG;
-    p.pairmat[k] = pairmat[k];
-  }
+  for (int b = 1; b <= ntypes; ++b)
+    for (int a = 1; a <= ntypes; ++a)
+      p.pairmat[(a - 1) + (b - 1) * ntypes] = gather_entry(pairmat, ntypes, a, b);
   for (int j = 0; j < npairs; ++j) {
     p.rc2[j] = rcpair[j] * rcpair[j];
     p.vdr2[j] = (float)(1.0 / ((p.rc2[j] - ptrmin) / (ptsize - 1)));

@@ -357,14 +357,11 @@ int main(int argc, char **argv) {
           std::fprintf(stderr, "Pairs: unknown type on pair %d\n", i + 1);
           return 4;
         }
-        if (!sym) {
-          std::fprintf(stderr, "Pairs: one-sided pairs (compute1) are not on this path\n");
-          return 4;
-        }
         q[i] = d.charge[a - 1] * d.charge[b - 1];
-        // PairMat(a,b) (column-major), both orders for 'sym' (src/read_input.f90:159-164)
+        // PairMat(a,b) (column-major), the reverse order too for 'sym'; an
+        // 'asym' pair acts one way and selects compute1 (src/read_input.f90:125-133)
         d.pairmat[(a - 1) + (size_t)(b - 1) * nt] = i + 1;
-        d.pairmat[(b - 1) + (size_t)(a - 1) * nt] = i + 1;
+        if (sym) d.pairmat[(b - 1) + (size_t)(a - 1) * nt] = i + 1;
       }
       d.npairs = np;
       d.ppair.assign((size_t)(d.ptsize + 1) * np, 0.0);

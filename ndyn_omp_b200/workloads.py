@@ -70,6 +70,27 @@ def cu_crystal(n_cells=10, T=300.0, seed=1, quirk="ref"):
                 control=dict(dt=0.1, skin=CU_MORSE["skin"], out_steps=100, quirk=quirk))
 
 
+# A random FCC alloy with a one-sided pair: type 1 pushes type 2 through an
+# 'asym' LJ line (PairMat(1,2) set, PairMat(2,1) not), so dynamics takes
+# compute1 (src/nd.f90:155-163, 364-530); the like pairs are symmetric Morse.
+ONESIDED = dict(masses=[63.546, 58.69],
+                pairs=[(1, 1, True, "morse", [6.0, 0.3429, 1.3588, 2.866]),
+                       (2, 2, True, "morse", [6.0, 0.4205, 1.4199, 2.780]),
+                       (1, 2, False, "LJ", [6.0, 0.02, 2.4])],
+                a=3.615, skin=0.5)
+
+
+def onesided_alloy(n_cells=8, T=300.0, seed=7, quirk="fixed", frac2=0.4):
+    """Random two-type FCC alloy with one one-sided (asym) pair, NVE."""
+    rng = np.random.default_rng(seed)
+    pos, box = lattice((n_cells,) * 3, ONESIDED["a"], FCC_BASIS)
+    typ = np.where(rng.random(len(pos)) < frac2, 2, 1).astype(np.int32)
+    vel = mb_velocities(typ, ONESIDED["masses"], T, rng)
+    return dict(name=f"onesided_alloy{n_cells}", masses=ONESIDED["masses"],
+                pairs=ONESIDED["pairs"], typ=typ, pos=pos, box=box, vel=vel,
+                control=dict(dt=0.1, skin=ONESIDED["skin"], out_steps=100, quirk=quirk))
+
+
 def ar_liquid(n_cells=40, T=120.0, seed=2, quirk="fixed", thermostat=True):
     """C2: LJ argon at reduced density 0.8442, +-0.05 sigma jitter, NVT."""
     rng = np.random.default_rng(seed)

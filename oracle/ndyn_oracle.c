@@ -31,6 +31,7 @@ struct ora_sys {
   double rcut, rcut2, ptrmin;
   int ntypes, npairs, ptsize;
   int *pairmat; /* ntypes x ntypes column-major, values 1..npairs or 0 */
+  int asympots; /* some Pairs line is one-sided ('asym'), src/read_input.f90:131-133 */
   double *mass;
   double *ptdr2, *ptrc2, *pairparams /* 4 x npairs */, *ppair, *fpair,
       *qprod;
@@ -292,7 +293,9 @@ int ora_set_pairs(ora_sys *s, int npairs, double ptrmin, int ptsize,
   s->qprod = (double *)calloc(npairs, sizeof(double));
   s->pairname = (char(*)[9])calloc(npairs, 9);
   for (int j = 0; j < npairs; ++j) s->pairparams[4 * j] = s->rcut; /* :156 */
+  s->asympots = 0;
   for (int j = 0; j < npairs; ++j) {
+    if (!sym[j]) s->asympots = 1;
     int a = p1[j], b = p2[j];
     if (a < 1 || a > s->ntypes || b < 1 || b > s->ntypes) return ORA_ERR_ARG;
     s->pairmat[(a - 1) + (b - 1) * s->ntypes] = j + 1;
@@ -711,6 +714,104 @@ void ora_compute0(ora_sys *s, int cv, int cu) {
   free(vtmp); free(ptmp); free(vdr2);
 }
 
+/* compute1, src/nd.f90:364-530: the half-list loop of compute0 for a
+ * PairMat with one-sided entries.  The table and cutoff are those of
+ * max(PTij, PTji) (:447,462-472); i feels the pair only if PTji > 0
+ * (:474-478), j only if PTij > 0 (:479-483); energy and virial count only
+ * pairs with PTij == PTji (:485-498).  The reference leaves k unclamped here
+ * (:467); a list entry closer than sqrt(PTrMin) would read outside the
+ * table, and this restatement clamps k to 1 as compute0 does. */
+void ora_compute1(ora_sys *s, int cv, int cu) {
+  const int T = s->nthreads, np = s->np, npairs = s->npairs;
+  const int stride = s->neimax + 1, tsz = s->ptsize + 1;
+  double *vtmp = (double *)calloc(6 * (size_t)T, sizeof(double));
+  double *ptmp = (double *)calloc((size_t)T, sizeof(double));
+  float *vdr2 = (float *)malloc(sizeof(float) * npairs);
+  if (cv) for (int k = 0; k < 6; ++k) s->virial[k] = 0.0;
+  if (cu) s->potential = 0.0;
+  for (int p = 0; p < npairs; ++p) vdr2[p] = (float)(1.0 / s->ptdr2[p]);
+  double *force = s->force, *ftmp = s->ftmp;
+  const double *pos = s->pos, *box = s->box, *fp = s->fpair, *pp = s->ppair;
+  const double *rc2 = s->ptrc2;
+  const double ptrmin = s->ptrmin;
+  memset(force, 0, sizeof(double) * 3 * (size_t)np);
+  memset(ftmp, 0, sizeof(double) * 3 * (size_t)np * T);
+#pragma omp parallel num_threads(T)
+  {
+    int tid = omp_get_thread_num();
+    int istart = (np / T) * tid;
+    int iend = (np / T) * (tid + 1);
+    if (iend < np && tid == T - 1) iend = np;
+    double *ft = ftmp + 3 * (size_t)np * tid;
+    double pt = 0.0, vt[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = istart; i < iend; ++i) {
+      const double *pi = pos + 3 * (size_t)i;
+      int typi = s->typ[i];
+      const int *row = s->vnl + (size_t)stride * i;
+      for (int jn = 1; jn < row[0]; ++jn) {
+        int j = row[jn];
+        int ptij = pm(s, typi, s->typ[j]), ptji = pm(s, s->typ[j], typi);
+        int mx = ptij > ptji ? ptij : ptji;
+        double rij[3];
+        double d2 = pair_d2(pi, pos + 3 * (size_t)j, box, rij);
+        if (d2 > rc2[mx - 1]) continue;
+        float rk = (float)(d2 - ptrmin) * vdr2[mx - 1] + 1.0f;
+        int k = (int)rk;
+        if (k < 1) k = 1;
+        double w = (double)rk - (double)k;
+        const double *F = fp + (size_t)tsz * (mx - 1) + (k - 1);
+        double df = w * F[1] + (1.0 - w) * F[0];
+        df = df / d2;
+        if (ptji > 0) {
+          ft[3 * (size_t)i] += rij[0] * df;
+          ft[3 * (size_t)i + 1] += rij[1] * df;
+          ft[3 * (size_t)i + 2] += rij[2] * df;
+        }
+        if (ptij > 0) {
+          ft[3 * (size_t)j] -= rij[0] * df;
+          ft[3 * (size_t)j + 1] -= rij[1] * df;
+          ft[3 * (size_t)j + 2] -= rij[2] * df;
+        }
+        if (cu && ptij == ptji) {
+          const double *P = pp + (size_t)tsz * (mx - 1) + (k - 1);
+          pt = pt + (w * P[1] + (1.0 - w) * P[0]);
+        }
+        if (cv && ptij == ptji) {
+          vt[0] += rij[0] * rij[0] * df;
+          vt[1] += rij[1] * rij[1] * df;
+          vt[2] += rij[2] * rij[2] * df;
+          vt[3] += rij[0] * rij[1] * df;
+          vt[4] += rij[0] * rij[2] * df;
+          vt[5] += rij[1] * rij[2] * df;
+        }
+      }
+    }
+    ptmp[tid] = pt;
+    for (int k = 0; k < 6; ++k) vtmp[6 * tid + k] = vt[k];
+#pragma omp barrier
+    for (int t = 0; t < T; ++t) {
+      const double *src = ftmp + 3 * (size_t)np * t;
+      for (int i = istart; i < iend; ++i) {
+        force[3 * (size_t)i] += src[3 * (size_t)i];
+        force[3 * (size_t)i + 1] += src[3 * (size_t)i + 1];
+        force[3 * (size_t)i + 2] += src[3 * (size_t)i + 2];
+      }
+    }
+  }
+  if (cv)
+    for (int t = 0; t < T; ++t)
+      for (int k = 0; k < 6; ++k) s->virial[k] += vtmp[6 * t + k];
+  if (cu)
+    for (int t = 0; t < T; ++t) s->potential += ptmp[t];
+  free(vtmp); free(ptmp); free(vdr2);
+}
+
+/* the force routine dynamics calls, src/nd.f90:155-163 (no spring pairs) */
+void ora_compute(ora_sys *s, int cv, int cu) {
+  if (s->asympots) ora_compute1(s, cv, cu);
+  else ora_compute0(s, cv, cu);
+}
+
 /* integrate2, src/nd.f90:1081-1121 */
 void ora_integrate2(ora_sys *s, int ck) {
   const int np = s->np, T = s->nthreads;
@@ -816,7 +917,7 @@ int ora_run_loop(ora_sys *s, int nsteps, double dt, ora_thermo_cb cb, void *user
       if (rc < 0) return rc;
     }
     ora_integrate1(s);
-    ora_compute0(s, cv, cu);
+    ora_compute(s, cv, cu);
     ora_integrate2(s, ck);
     if (tt == 1) s->e0 = s->potential + s->kinetic;
     if (out && cb) {

@@ -210,7 +210,6 @@ int main(int argc, char **argv) {
         npar[i] = n - 4 > 4 ? 4 : (n - 4 > 0 ? n - 4 : 0);
         for (int j = 0; j < npar[i]; ++j) par[4 * i + j] = atof(tw[4 + j]);
         if (p1[i] && p2[i]) q[i] = d.charge[p1[i] - 1] * d.charge[p2[i] - 1];
-        if (!sym[i]) fprintf(stderr, "# note: asymmetric pairs are outside this oracle\n");
       }
       int rc = ora_set_pairs(d.s, np, ptrmin, ptsize, p1, p2, sym, names, par, npar, q);
       if (rc) { fprintf(stderr, "Pairs: error %d\n", rc); return 4; }

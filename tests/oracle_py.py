@@ -81,8 +81,9 @@ def lib():
         for f in ("ora_integrate1", "ora_mk_iso_ke", "ora_mk_iso_e", "ora_mk_iso_p"):
             getattr(L, f).argtypes = [vp]
             getattr(L, f).restype = None
-        L.ora_compute0.argtypes = [vp, i, i]
-        L.ora_compute0.restype = None
+        for f in ("ora_compute0", "ora_compute1", "ora_compute"):
+            getattr(L, f).argtypes = [vp, i, i]
+            getattr(L, f).restype = None
         L.ora_integrate2.argtypes = [vp, i]
         L.ora_integrate2.restype = None
         L.ora_run.argtypes = [vp, i, d, THERMO_CB, vp]
@@ -225,6 +226,11 @@ class Oracle:
 
     def compute0(self, cv=1, cu=1):
         self.L.ora_compute0(self.s, cv, cu)
+
+    def compute(self, cv=1, cu=1):
+        """The force routine dynamics would call: compute1 when some pair
+        is one-sided, else compute0 (src/nd.f90:155-163)."""
+        self.L.ora_compute(self.s, cv, cu)
 
     def integrate1(self):
         self.L.ora_integrate1(self.s)

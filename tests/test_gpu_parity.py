@@ -29,6 +29,8 @@ def small_specs():
         "cu_m2_ref": W.cu_crystal(5, 900.0, seed=14, quirk="ref"),        # 500 atoms, M=2
         "cu_m2_fixed": W.cu_crystal(5, 900.0, seed=14, quirk="fixed"),
         "cu_m6_ref": W.cu_crystal(12, 600.0, seed=15, quirk="ref"),      # 6912 atoms, M=6
+        # two types, one one-sided (asym) pair: compute1's rules
+        "alloy_fixed": W.onesided_alloy(8, 300.0, seed=16, quirk="fixed"),  # 2048 atoms, M=4
     }
 
 
@@ -44,11 +46,12 @@ def specs():
     s = small_specs()
     s["cu_ref"] = _jitter(s["cu_ref"], 0.05, 99)
     s["cu_m6_ref"] = _jitter(s["cu_m6_ref"], 0.1, 98)
+    s["alloy_fixed"] = _jitter(s["alloy_fixed"], 0.05, 97)
     return s
 
 
 @pytest.mark.parametrize("name", ["cu_ref", "ar_fixed", "nacl_fixed", "cu_m2_ref", "cu_m2_fixed",
-                                  "cu_m6_ref"])
+                                  "cu_m6_ref", "alloy_fixed"])
 def test_cells_and_neighbour_pairs_bit_exact(specs, name):
     spec = specs[name]
     o = oracle_from_spec(spec)
@@ -104,6 +107,26 @@ def test_compute0_mixed_force_error(specs, name):
     assert err < 1e-5, err
     assert abs(peg - peo) <= 1e-6 * abs(peo)
     assert rel_l2(virg, viro) < 1e-5
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("mixed", 1e-5)])
+def test_onesided_pairs_compute1(specs, prec, tol):
+    """A one-sided (asym) pair: forces follow compute1 (src/nd.f90:364-530),
+    only symmetric pairs add energy and virial; same bars as compute0."""
+    spec = specs["alloy_fixed"]
+    o = oracle_from_spec(spec)
+    o.setup_lists()
+    o.compute(1, 1)
+    fo, peo, viro, _ = o.forces()
+    with nd.Context(0, prec) as ctx:
+        sid = gpu_from_spec(ctx, spec)
+        ctx.setup_lists()
+        ctx.compute0(True, True)
+        fg, peg, virg, _ = ctx.forces(sid)
+    assert rel_l2(fg, fo) < tol
+    assert abs(peg - peo) <= (1e-12 if prec == "fp64" else 1e-6) * abs(peo)
+    assert rel_l2(virg, viro) < tol
+    assert np.linalg.norm(fo.sum(axis=0)) > 1e-6 * np.abs(fo).sum()  # no Newton-3 balance
 
 
 def test_integrate1_bit_exact(specs):
@@ -179,6 +202,20 @@ def test_run_nve_crystal_fp64(specs):
         assert a["press"] == pytest.approx(b["press"], rel=1e-9, abs=1e-12)
         assert a["vol"] == b["vol"]
     po, vo, _, _ = o.state()
+    assert rel_l2(pg, po) < 1e-12
+    assert nup == o.list_updates
+
+
+def test_run_onesided_fp64(specs):
+    """Dynamics with a one-sided pair: the run takes compute1 on both sides."""
+    spec = dict(specs["alloy_fixed"])
+    spec["control"] = dict(spec["control"], out_steps=10)
+    o, ro, rg, (pg, _, _, _), nup = _run_both(spec, 100)
+    assert [r["step"] for r in rg] == [r["step"] for r in ro]
+    for a, b in zip(rg, ro):
+        assert a["pe"] == pytest.approx(b["pe"], rel=1e-11)
+        assert a["ke"] == pytest.approx(b["ke"], rel=1e-9)
+    po, _, _, _ = o.state()
     assert rel_l2(pg, po) < 1e-12
     assert nup == o.list_updates
 
