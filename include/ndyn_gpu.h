@@ -148,6 +148,15 @@ int ndg_get_state(ndg_ctx *ctx, int sys, double *pos, double *vel, double *acc,
                   double *box);
 int ndg_set_control(ndg_ctx *ctx, int sys, const ndg_control *c);
 int ndg_get_control(ndg_ctx *ctx, int sys, ndg_control *c);
+/* Hold groups with displacement conditions, integrate1's Nhold branch
+ * (src/nd.f90:1048-1077; the Hold and Disp directives fill hold(np),
+ * bcDir and bcParm, src/read_input.f90:177-190).  hold[i] is the group
+ * (1..ngroups, 0 = none) of atom i in input order; where
+ * dir[3*(g-1)+d] != 0, an atom of group g moves by du[3*(g-1)+d]
+ * (fractional units) along axis d every step instead of by its velocity.
+ * hold == NULL or ngroups == 0 removes the system's holds. */
+int ndg_set_holds(ndg_ctx *ctx, int sys, const int *hold, int ngroups, const int *dir,
+                  const double *du);
 void ndg_default_control(ndg_control *c);
 
 /* ---- the reference routines, one call each (all systems of ctx) -------- */

@@ -26,6 +26,7 @@ SIGNATURES = [
     ("ndg_load_state", i, [vp, i, vp, vp, vp, vp]),
     ("ndg_get_state", i, [vp, i, vp, vp, vp, vp]),
     ("ndg_set_control", i, [vp, i, vp]),
+    ("ndg_set_holds", i, [vp, i, vp, i, vp, vp]),
     ("ndg_get_control", i, [vp, i, vp]),
     ("ndg_default_control", None, [vp]),
     ("ndg_setup_lists", i, [vp]),

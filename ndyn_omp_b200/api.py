@@ -187,6 +187,19 @@ class Context:
                 setattr(c, k, v)
         _ok(self.L.ndg_set_control(self._c, sys, ctypes.byref(c)), "set_control")
 
+    def set_holds(self, sys, hold=None, dirs=None, du=None):
+        """Hold groups with displacement conditions (Hold/Disp directives,
+        integrate1's Nhold branch): hold[i] in 0..G per atom in input order,
+        dirs (G,3) booleans, du (G,3) fractional displacement per step.
+        hold=None removes them."""
+        if hold is None:
+            _ok(self.L.ndg_set_holds(self._c, sys, None, 0, None, None), "set_holds")
+            return
+        hold = np.ascontiguousarray(hold, np.int32)
+        dirs = np.ascontiguousarray(np.asarray(dirs, bool).reshape(-1, 3), np.int32)
+        du = np.ascontiguousarray(np.asarray(du, np.float64).reshape(-1, 3))
+        _ok(self.L.ndg_set_holds(self._c, sys, _p(hold), len(du), _p(dirs), _p(du)), "set_holds")
+
     def load_state(self, sys, pos, vel=None, acc=None, box=None):
         pos = np.ascontiguousarray(pos, np.float64).reshape(-1)
         vel = None if vel is None else np.ascontiguousarray(vel, np.float64).reshape(-1)

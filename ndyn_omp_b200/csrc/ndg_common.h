@@ -82,6 +82,7 @@ struct SysParam {
   int renei, renei_freq, out_steps;
   int isokinetic, ke_freq, isobaric, p_freq, isoenergetic, e_freq, box_load;
   double ke_target, ke_parm, p_target[3], p_parm, e_parm, box_vel[3];
+  int nhold, bc_off;             // hold groups, their first entry in DevCtx::bcd
 };
 
 // Mutable per-system state, resident on the device for the whole run.

@@ -68,6 +68,7 @@ struct HostSys {
   double ptrmin = 0.25;
   std::vector<double> mass, rcpair, ppair, fpair;
   std::vector<float2> tF2, tP2;  // FP32 (k, k+1) pairs of fpair and ppair
+  std::vector<double4> bc;       // hold groups: displacement per step, w = axis mask
   std::vector<int> pairmat;
   ndg_control ctl{};
   Range atoms, cells, nbr;  // atoms/cells in elements, nbr in ints
@@ -97,7 +98,7 @@ struct ndg_ctx {
   // arenas
   Arena atoms, cells, nbrs;  // atoms in chunks, cells in cells, nbrs in ints
   int nsys_cap = 0;
-  size_t cap_pm = 0, cap_pg = 0, cap_mass = 0, cap_rc2 = 0, cap_rlist2 = 0, cap_vdr2 = 0, cap_rc2f = 0,
+  size_t cap_pm = 0, cap_pg = 0, cap_bc = 0, cap_mass = 0, cap_rc2 = 0, cap_rlist2 = 0, cap_vdr2 = 0, cap_rc2f = 0,
          cap_tabF = 0, cap_tabP = 0, cap_tabF2 = 0, cap_tabP2 = 0;
   // device buffers
   SysParam *dP = nullptr;
@@ -108,6 +109,8 @@ struct ndg_ctx {
   double *vel = nullptr, *acc = nullptr, *disp = nullptr, *force = nullptr;
   double *s_vel = nullptr, *s_acc = nullptr;
   int *gid = nullptr, *s_gid = nullptr, *s_cell = nullptr, *nnb = nullptr;
+  int *hold = nullptr;     // per atom slot, by input index: hold group
+  double4 *bcd = nullptr;  // hold groups of all systems
   int *atom_cell = nullptr, *atom_slot = nullptr, *perm = nullptr, *tmp_src = nullptr,
       *tmp_key = nullptr;
   int *cell_count = nullptr, *cell_start = nullptr;
@@ -188,6 +191,8 @@ DevCtx devctx(ndg_ctx *c) {
   d.disp = c->disp;
   d.force = c->force;
   d.gid = c->gid;
+  d.hold = c->hold;
+  d.bcd = c->bcd;
   d.nbr = c->nbr;
   d.tile_rows = c->tile_rows;
   d.nb_vcap = c->nb_vcap;
@@ -259,6 +264,7 @@ int grow_atoms(ndg_ctx *c, long long new_chunks) {
   rc |= grow(c, c->disp, 3 * old, 3 * n);
   rc |= grow(c, c->force, 3 * old, 3 * n);
   rc |= grow(c, c->gid, old, n);
+  rc |= grow(c, c->hold, old, n);
   rc |= grow(c, c->nnb, old, n);
   rc |= grow(c, c->atom_cell, old, n);
   rc |= grow(c, c->atom_slot, 0, n);
@@ -373,6 +379,7 @@ int upload_vec(ndg_ctx *c, T *&dst, size_t &cap, const std::vector<T> &v) {
 // small per-pair/per-type arrays: rebuilt for all systems on any change
 int upload_params(ndg_ctx *c) {
   std::vector<int> pm, pg;
+  std::vector<double4> bc;
   std::vector<double> mass, rc2, rlist2, tabF, tabP;
   std::vector<float> vdr2, rc2f;
   std::vector<float2> tF2, tP2;
@@ -394,6 +401,9 @@ int upload_params(ndg_ctx *c) {
     p.type_off = (int)mass.size();
     p.pm_off = (int)pm.size();
     pm.insert(pm.end(), h.pairmat.begin(), h.pairmat.end());
+    p.bc_off = (int)bc.size();
+    p.nhold = (int)h.bc.size();
+    bc.insert(bc.end(), h.bc.begin(), h.bc.end());
     for (int b = 1; b <= h.ntypes; ++b)
       for (int a = 1; a <= h.ntypes; ++a) pg.push_back(gather_entry(h.pairmat.data(), h.ntypes, a, b));
     mass.insert(mass.end(), h.mass.begin(), h.mass.end());
@@ -448,6 +458,7 @@ int upload_params(ndg_ctx *c) {
   int rc = 0;
   rc |= upload_vec(c, c->pairmat, c->cap_pm, pm);
   rc |= upload_vec(c, c->pairg, c->cap_pg, pg);
+  rc |= upload_vec(c, c->bcd, c->cap_bc, bc);
   rc |= upload_vec(c, c->mass, c->cap_mass, mass);
   rc |= upload_vec(c, c->rc2, c->cap_rc2, rc2);
   rc |= upload_vec(c, c->rlist2, c->cap_rlist2, rlist2);
@@ -857,7 +868,7 @@ int status_from_words(ndg_ctx *c) {
 ndg_ctx::~ndg_ctx() {
   drop_graphs(this);
   void *ptrs[] = {dP, dS, chunk_sys, cell_sys, pos, s_pos, pfx, vel, acc, disp, force, s_vel,
-                  s_acc, gid, s_gid, s_cell, nnb, atom_cell, atom_slot, perm, tmp_src, tmp_key,
+                  s_acc, gid, s_gid, s_cell, nnb, hold, bcd, atom_cell, atom_slot, perm, tmp_src, tmp_key,
                   cell_count, cell_start, rb_list, plan, plan_kb, plan_hdr, nbr, tile_rows, red, itop, ired, pairmat, pairg, mass, rc2, rlist2,
                   vdr2, rc2f, tabF, tabP, tabF2, tabP2, ring, ring_count};
   for (void *p : ptrs)
@@ -1143,6 +1154,31 @@ int ndg_num_systems(const ndg_ctx *c) {
   int n = 0;
   for (auto &h : c->sys) n += h.alive;
   return n;
+}
+
+int ndg_set_holds(ndg_ctx *c, int s, const int *hold, int ngroups, const int *dir,
+                  const double *du) {
+  if (!valid_sys(c, s) || ngroups < 0 || (hold && ngroups > 0 && (!dir || !du)))
+    return NDG_ERR_ARG;
+  cudaSetDevice(c->device);
+  HostSys &h = c->sys[s];
+  c->params_dirty = true;
+  if (!hold || ngroups == 0) {
+    h.bc.clear();
+    return NDG_OK;
+  }
+  for (int i = 0; i < h.n; ++i)
+    if (hold[i] < 0 || hold[i] > ngroups) return NDG_ERR_ARG;
+  // the groups are read through the atoms' input index (gid), which the
+  // list builds' reordering keeps
+  CK(c, cudaMemcpy(c->hold + (size_t)h.atoms.off * ATOM_ALIGN, hold, h.n * sizeof(int),
+                   cudaMemcpyHostToDevice));
+  h.bc.resize(ngroups);
+  for (int g = 0; g < ngroups; ++g) {
+    const int m = (dir[3 * g] ? 1 : 0) | (dir[3 * g + 1] ? 2 : 0) | (dir[3 * g + 2] ? 4 : 0);
+    h.bc[g] = make_double4(du[3 * g], du[3 * g + 1], du[3 * g + 2], (double)m);
+  }
+  return NDG_OK;
 }
 
 int ndg_load_state(ndg_ctx *c, int s, const double *pos, const double *vel, const double *acc,

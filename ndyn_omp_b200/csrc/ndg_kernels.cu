@@ -187,8 +187,9 @@ __device__ void plan_block(const DevCtx &c, int g0, int g1) {
   }
 }
 
-// integrate1, src/nd.f90:1027-1046; applies velocity scales left pending by
-// the previous step's mkIsoKE/mkIsoE first (src/nd.f90:1145-1155,1173-1180).
+// integrate1, src/nd.f90:1027-1077 (both Nhold branches); applies velocity
+// scales left pending by the previous step's mkIsoKE/mkIsoE first
+// (src/nd.f90:1145-1155,1173-1180).
 // Emits each chunk's two largest displacement measures for the next
 // CheckListUpdate.  A dynamics step's launch has one more block, which
 // plans the step's pair launches.
@@ -221,9 +222,21 @@ __global__ __launch_bounds__(BLOCK) void k_integrate1(DevCtx c, int standalone, 
           v[0] = v0; v[1] = v1; v[2] = v2;
         }
         const double a0 = a[0], a1 = a[1], a2 = a[2];
-        const double du0 = li0 * (v0 * dt + 0.5 * a0 * dt * dt);
-        const double du1 = li1 * (v1 * dt + 0.5 * a1 * dt * dt);
-        const double du2 = li2 * (v2 * dt + 0.5 * a2 * dt * dt);
+        double du0 = li0 * (v0 * dt + 0.5 * a0 * dt * dt);
+        double du1 = li1 * (v1 * dt + 0.5 * a1 * dt * dt);
+        double du2 = li2 * (v2 * dt + 0.5 * a2 * dt * dt);
+        if (P->nhold > 0) {
+          // displacement conditions of the atom's hold group replace the
+          // constrained components (src/nd.f90:1058-1066)
+          const int hg = c.hold[P->atom_off + c.gid[i]];
+          if (hg > 0) {
+            const double4 b = c.bcd[P->bc_off + hg - 1];
+            const int m = (int)b.w;
+            if (m & 1) du0 = b.x;
+            if (m & 2) du1 = b.y;
+            if (m & 4) du2 = b.z;
+          }
+        }
         const double d0 = dl[0] + du0, d1 = dl[1] + du1, d2 = dl[2] + du2;
         dl[0] = d0; dl[1] = d1; dl[2] = d2;
         double4 p = c.pos[i];

@@ -36,6 +36,8 @@ struct DevCtx {
   int4 *pfx;
   double *vel, *acc, *disp, *force;
   int *gid;
+  const int *hold;     // per atom, by input index: hold group (0 = none)
+  const double4 *bcd;  // per hold group: displacement per step (x, y, z), w = axis mask
   int *nbr;  // blocked neighbour list (128-atom tiles), atom slots
   int *nnb;
   int *tile_rows;  // per tile: rows of its list in use (L2 prefetch size)

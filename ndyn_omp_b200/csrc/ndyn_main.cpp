@@ -144,6 +144,18 @@ struct Driver {
   std::string model, model_type = "xyz";
   uint64_t seed = 123456789ULL;
   ndg_control c{};
+  // hold groups and their displacement conditions (src/read_input.f90:177-190)
+  std::vector<int> hold;  // per atom: group, 0 = none
+  std::vector<std::string> hname;
+  std::vector<int> bcdir;
+  std::vector<double> bcparm;
+  bool holds_dirty = false;
+
+  // positions as the device has them after a run (for domain selections)
+  int sync_positions() {
+    if (!ctx || sys < 0 || dirty) return NDG_OK;
+    return ndg_get_state(ctx, sys, pos.data(), vel.data(), acc.data(), box);
+  }
 
   int type_id(const std::string &t) const {
     for (size_t i = 0; i < tname.size(); ++i)
@@ -264,6 +276,13 @@ struct Driver {
     c.quirk = quirk;
     rc = ndg_set_control(ctx, sys, &c);
     if (rc) return rc;
+    if (holds_dirty) {
+      const bool any = !hname.empty();
+      rc = ndg_set_holds(ctx, sys, any ? hold.data() : nullptr, (int)hname.size(),
+                         any ? bcdir.data() : nullptr, any ? bcparm.data() : nullptr);
+      if (rc) return rc;
+      holds_dirty = false;
+    }
     rc = ndg_run(ctx, nsteps, thermo_line, nullptr);
     if (rc) return rc;
     ndg_control after{};
@@ -314,6 +333,12 @@ int main(int argc, char **argv) {
       d.model = arg(w, 1);
       if (w.size() >= 3) d.model_type = w[2];
       if (!d.read_model()) return 2;
+      // a new model holds no atoms (read_model, src/read_input.f90:294-296)
+      d.hold.assign(d.typ.size(), 0);
+      d.hname.clear();
+      d.bcdir.clear();
+      d.bcparm.clear();
+      d.holds_dirty = true;
     } else if (k == "Seed") {
       d.seed = std::strtoull(arg(w, 1).c_str(), nullptr, 10);
     } else if (k == "Velocity") {
@@ -415,6 +440,72 @@ int main(int argc, char **argv) {
       d.c.out_steps = std::atoi(arg(w, 1).c_str());
     } else if (k == "StepNumber") {
       d.c.step = std::atoi(arg(w, 1).c_str());
+    } else if (k == "Hold") {
+      // Hold NAME typ ID | Hold NAME dom rec INSIDE xmin xmax ymin ymax zmin zmax
+      // (setGroup 'h', src/nd.f90:1625-1700; rectangular domains,
+      // src/domtype.f90:299-343, compared in FP32 on fractional positions)
+      if (d.typ.empty()) {
+        std::fprintf(stderr, "Hold: no model\n");
+        return 4;
+      }
+      d.hold.resize(d.typ.size(), 0);
+      d.hname.push_back(arg(w, 1));
+      d.bcdir.insert(d.bcdir.end(), 3, 0);
+      d.bcparm.insert(d.bcparm.end(), 3, 0.0);
+      const int g = (int)d.hname.size();
+      const std::string how = arg(w, 2).substr(0, 3);
+      if (how == "typ") {
+        const int t = std::atoi(arg(w, 3).c_str());
+        for (size_t i = 0; i < d.typ.size(); ++i)
+          if (d.typ[i] == t) d.hold[i] = g;
+      } else if (how == "dom" && arg(w, 3) == "rec" && w.size() >= 11) {
+        const std::string ins = arg(w, 4);
+        const bool inside = !(ins == "F" || ins == "f" || ins == ".false." || ins == "false");
+        float lo[3], hi[3];
+        int dir[3];
+        for (int a = 0; a < 3; ++a) {
+          lo[a] = (float)std::atof(w[5 + 2 * a].c_str());
+          hi[a] = (float)std::atof(w[6 + 2 * a].c_str());
+          dir[a] = (std::fabs(hi[a]) + std::fabs(lo[a])) < 1.17549435e-38f ? 0 : 1;
+        }
+        if (d.sync_positions()) return 4;
+        for (size_t i = 0; i < d.typ.size(); ++i) {
+          bool in = true;
+          for (int a = 0; a < 3; ++a) {
+            const float x = (float)d.pos[3 * i + a];
+            if (dir[a] && !(x > lo[a] && x <= hi[a])) in = false;
+          }
+          if (in == inside) d.hold[i] = g;
+        }
+      } else {
+        std::fprintf(stderr, "Hold: only 'typ ID' and 'dom rec ...' selections are supported\n");
+        return 4;
+      }
+      d.holds_dirty = true;
+    } else if (k == "Disp") {
+      // Disp NAME dx dy dz: per axis a displacement per step (fractional), F = free
+      int g = 0;
+      for (size_t q = 0; q < d.hname.size(); ++q)
+        if (d.hname[q] == arg(w, 1)) g = (int)q + 1;
+      if (!g) {
+        std::fprintf(stderr, "Disp: unknown hold group %s\n", arg(w, 1).c_str());
+        return 4;
+      }
+      for (int a = 0; a < 3; ++a) {
+        const std::string v = arg(w, 2 + a);
+        const bool on = !v.empty() && v != "F";
+        d.bcdir[3 * (g - 1) + a] = on;
+        d.bcparm[3 * (g - 1) + a] = on ? std::atof(v.c_str()) : 0.0;
+      }
+      d.holds_dirty = true;
+    } else if (k == "ClearHolds") {
+      d.hold.assign(d.typ.size(), 0);
+      d.hname.clear();
+      d.bcdir.clear();
+      d.bcparm.clear();
+      d.holds_dirty = true;
+    } else if (k == "HoldBufferSize") {
+      // group storage grows as needed
     } else if (k == "Run") {
       const int nsteps = std::atoi(arg(w, 1).c_str());
       if (w.size() >= 3) d.c.dt = std::atof(w[2].c_str());

@@ -42,6 +42,9 @@ struct ora_sys {
   int ncell, mcell[3], neimax, nlist_updates;
   int *list, *head, *vnl;
   double *displist;
+  /* hold groups, src/mods.f90 groupStuff: hold(np), bcDir/bcParm per group */
+  int nhold, *hold, *bcdir;
+  double *bcparm;
   int lists_ready;
   int err;
 };
@@ -223,6 +226,29 @@ static void free_lists(ora_sys *s) {
   s->lists_ready = 0;
 }
 
+static void free_holds(ora_sys *s) {
+  free(s->hold); free(s->bcdir); free(s->bcparm);
+  s->hold = NULL; s->bcdir = NULL; s->bcparm = NULL;
+  s->nhold = 0;
+}
+
+/* Hold NAME ... / Disp NAME x y z, src/read_input.f90:177-190: hold[i] is the
+ * group of atom i (0 = none); group g moves by du along the axes dir marks */
+int ora_set_holds(ora_sys *s, const int *hold, int ngroups, const int *dir, const double *du) {
+  free_holds(s);
+  if (!hold || ngroups <= 0) return ORA_OK;
+  s->hold = (int *)malloc(sizeof(int) * (size_t)s->np);
+  s->bcdir = (int *)malloc(sizeof(int) * 3 * (size_t)ngroups);
+  s->bcparm = (double *)malloc(sizeof(double) * 3 * (size_t)ngroups);
+  for (int i = 0; i < s->np; ++i) {
+    if (hold[i] < 0 || hold[i] > ngroups) { free_holds(s); return ORA_ERR_ARG; }
+    s->hold[i] = hold[i];
+  }
+  for (int k = 0; k < 3 * ngroups; ++k) { s->bcdir[k] = dir[k] != 0; s->bcparm[k] = du[k]; }
+  s->nhold = ngroups;
+  return ORA_OK;
+}
+
 static void free_state(ora_sys *s) {
   free(s->typ); free(s->pos); free(s->vel); free(s->acc); free(s->force);
   s->typ = NULL;
@@ -239,7 +265,7 @@ static void free_pairs(ora_sys *s) {
 
 void ora_free(ora_sys *s) {
   if (!s) return;
-  free_lists(s); free_state(s); free_pairs(s); free(s->mass);
+  free_lists(s); free_state(s); free_pairs(s); free_holds(s); free(s->mass);
   free(s);
 }
 
@@ -352,6 +378,7 @@ int ora_set_state(ora_sys *s, int np, const int *typ, const double *pos,
   if (np < 1) return ORA_ERR_ARG;
   free_state(s);
   free_lists(s);
+  free_holds(s); /* hold groups name atoms of the previous state */
   s->np = np;
   s->typ = (int *)malloc(sizeof(int) * np);
   s->pos = (double *)malloc(sizeof(double) * 3 * np);
@@ -613,7 +640,9 @@ int ora_check_list_update(ora_sys *s) {
 }
 
 /* ------------------------------------------------------------------ */
-/* integrate1, src/nd.f90:984-1047 (Nhold == 0 branch) */
+/* integrate1, src/nd.f90:984-1077: with hold groups (Nhold > 0) a held
+ * atom's constrained components move by the group's displacement
+ * (:1048-1074) */
 void ora_integrate1(ora_sys *s) {
   const double li0 = 1.0 / s->box[0], li1 = 1.0 / s->box[1], li2 = 1.0 / s->box[2];
   const double dt = s->c.dt;
@@ -625,6 +654,16 @@ void ora_integrate1(ora_sys *s) {
     double du0 = li0 * (vel[o] * dt + 0.5 * acc[o] * dt * dt);
     double du1 = li1 * (vel[o + 1] * dt + 0.5 * acc[o + 1] * dt * dt);
     double du2 = li2 * (vel[o + 2] * dt + 0.5 * acc[o + 2] * dt * dt);
+    if (s->nhold > 0) {
+      int g = s->hold[j];
+      if (g != 0) {
+        const int *bd = s->bcdir + 3 * (g - 1);
+        const double *bp = s->bcparm + 3 * (g - 1);
+        if (bd[0]) du0 = bp[0];
+        if (bd[1]) du1 = bp[1];
+        if (bd[2]) du2 = bp[2];
+      }
+    }
     dl[o] = dl[o] + du0; dl[o + 1] = dl[o + 1] + du1; dl[o + 2] = dl[o + 2] + du2;
     pos[o] = pos[o] + du0; pos[o + 1] = pos[o + 1] + du1; pos[o + 2] = pos[o + 2] + du2;
   }

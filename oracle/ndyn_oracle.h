@@ -119,6 +119,8 @@ int ora_check_list_update(ora_sys *s); /* src/nd.f90:1447-1499; 1 if rebuilt */
 void ora_integrate1(ora_sys *s);       /* src/nd.f90:984-1080 */
 void ora_compute0(ora_sys *s, int cv, int cu); /* src/nd.f90:200-363 */
 void ora_compute1(ora_sys *s, int cv, int cu); /* src/nd.f90:364-530 */
+/* hold groups with displacement conditions, src/read_input.f90:177-190 */
+int ora_set_holds(ora_sys *s, const int *hold, int ngroups, const int *dir, const double *du);
 void ora_compute(ora_sys *s, int cv, int cu);  /* compute0 or compute1, src/nd.f90:155-163 */
 void ora_integrate2(ora_sys *s, int ck);       /* src/nd.f90:1081-1121 */
 void ora_mk_iso_ke(ora_sys *s);        /* src/nd.f90:1122-1158 */

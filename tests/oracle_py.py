@@ -81,6 +81,7 @@ def lib():
         for f in ("ora_integrate1", "ora_mk_iso_ke", "ora_mk_iso_e", "ora_mk_iso_p"):
             getattr(L, f).argtypes = [vp]
             getattr(L, f).restype = None
+        L.ora_set_holds.argtypes = [vp, vp, i, vp, vp]
         for f in ("ora_compute0", "ora_compute1", "ora_compute"):
             getattr(L, f).argtypes = [vp, i, i]
             getattr(L, f).restype = None
@@ -226,6 +227,12 @@ class Oracle:
 
     def compute0(self, cv=1, cu=1):
         self.L.ora_compute0(self.s, cv, cu)
+
+    def set_holds(self, hold, dirs, du):
+        hold = np.ascontiguousarray(hold, np.int32)
+        dirs = np.ascontiguousarray(np.asarray(dirs, bool).reshape(-1, 3), np.int32)
+        du = np.ascontiguousarray(np.asarray(du, np.float64).reshape(-1, 3))
+        assert self.L.ora_set_holds(self.s, _p(hold), len(du), _p(dirs), _p(du)) == 0
 
     def compute(self, cv=1, cu=1):
         """The force routine dynamics would call: compute1 when some pair

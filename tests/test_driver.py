@@ -101,3 +101,26 @@ def test_driver_mixed_precision(tmp_path):
     # the potential energy, pressure and volume are compared
     _check("MorseTest mixed", rows, ref, ke_rel=1e30, press_abs=1e-6, pe_rel=1e-5,
            eerr_rel=1e30, limit=10)
+
+
+def test_driver_hold_rigid_translation(tmp_path):
+    """Hold/Disp through the driver (src/read_input.f90:177-190): holding
+    every atom with a displacement on all three axes translates the crystal
+    rigidly, so the printed potential energy never changes, while a 'dom rec'
+    hold of one slab changes it."""
+    case = GOLD["MorseTest"]
+    lattice.materialise(case["model"], str(tmp_path))
+    base = [ln for ln in case["script"] if ln.split()[:1] not in (["Run"], ["END"])]
+
+    def go(extra):
+        script = base + extra + ["OutFreq 20", "Run 100 0.0001", "END"]
+        r = subprocess.run([EXE], input="START\n" + "\n".join(script) + "\n", text=True,
+                           capture_output=True, cwd=str(tmp_path), timeout=600)
+        assert r.returncode == 0, r.stderr
+        return [float(ln.split()[1]) for ln in r.stdout.splitlines()
+                if len(ln.split()) == 6 and ln.split()[0].isdigit()]
+
+    pe = go(["Hold all typ 1", "Disp all 1.0e-5 -2.0e-5 0.5e-5"])
+    assert len(pe) >= 5 and len(set(pe)) == 1
+    pe2 = go(["Hold slab dom rec T 0 0 0 0 -0.5 -0.3", "Disp slab 2.0e-4 F F"])
+    assert len(set(pe2)) > 1

@@ -220,6 +220,42 @@ def test_run_onesided_fp64(specs):
     assert nup == o.list_updates
 
 
+def _holds(spec):
+    """Two hold groups: the atoms with z in the lower quarter move by a fixed
+    x/z displacement per step, one type is held with no constrained axis."""
+    pos = np.asarray(spec["pos"], np.float64).reshape(-1, 3)
+    hold = np.zeros(len(pos), np.int32)
+    hold[pos[:, 2].astype(np.float32) <= np.float32(-0.25)] = 1
+    hold[(hold == 0) & (np.asarray(spec["typ"]) == 2)] = 2
+    return hold, [[True, False, True], [False, False, False]], [[2e-5, 0.0, -1e-5], [0, 0, 0]]
+
+
+@pytest.mark.parametrize("name", ["alloy_fixed", "cu_ref"])
+def test_run_hold_groups_fp64(specs, name):
+    """Hold groups with displacement conditions (integrate1's Nhold branch,
+    src/nd.f90:1048-1077) follow the oracle through a run."""
+    spec = dict(specs[name])
+    spec["control"] = dict(spec["control"], out_steps=10)
+    hold, dirs, du = _holds(spec)
+    o = oracle_from_spec(spec)
+    o.set_holds(hold, dirs, du)
+    rc, ro = o.run(60, spec["control"]["dt"])
+    assert rc == 0
+    with nd.Context(0, "fp64") as ctx:
+        sid = gpu_from_spec(ctx, spec)
+        ctx.set_holds(sid, hold, dirs, du)
+        rg = ctx.run(60)
+        pg, _, _, _ = ctx.state(sid)
+    po, _, _, _ = o.state()
+    assert rel_l2(pg, po) < 1e-12
+    for a, b in zip(rg, ro):
+        assert a["pe"] == pytest.approx(b["pe"], rel=1e-11)
+        assert a["ke"] == pytest.approx(b["ke"], rel=1e-9)
+    p0 = np.asarray(spec["pos"], np.float64).reshape(-1, 3)
+    g1 = hold == 1
+    assert np.allclose(pg[g1, 0] - p0[g1, 0], 60 * 2e-5, rtol=0, atol=1e-13)  # 60 roundings
+
+
 def test_run_nvt_liquid_fixed_rebuilds(specs):
     """LJ liquid with the fixed rebuild criterion: lists are rebuilt on the
     same steps as the oracle and the thermostat trajectory follows it."""
