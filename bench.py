@@ -41,7 +41,7 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=50)
-    ap.add_argument("--config", default="c4", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--config", default="c4", choices=["c1", "c2", "c3", "c4", "c5", "c5batch"])
     ap.add_argument("--requests", type=int, default=128, help="c5: requests in the stream")
     ap.add_argument("--rate", type=float, default=200.0, help="c5: Poisson arrivals per s")
     ap.add_argument("--steps-scale", type=float, default=0.05,
@@ -62,6 +62,10 @@ def workload(cfg, scale_cells=None):
     from ndyn_omp_b200 import workloads as W
     if cfg == "c5":
         return [], "mixed"
+    if cfg == "c5batch":
+        # the first 64 requests of the c5 stream, resident together as one batch
+        reqs = W.serving_requests(64, 200.0, seed=5)
+        return [W.build_request(r) for r in reqs], "mixed"
     if cfg == "c1":
         return [W.cu_crystal(scale_cells or 10, 300.0, seed=1, quirk="ref")], "fp64"
     if cfg == "c2":
@@ -81,6 +85,8 @@ WORKLOAD_TEXT = {
           "skin 1.6, thermostat 600 K + barostat P=0 (Pparm 10)",
     "c4": "512 replicas (half Cu Morse crystals, half LJ Ar liquids), N log-uniform "
           "[500,20000] in whole FCC cells, T uniform [100,1500] K, own thermostats",
+    "c5batch": "the first 64 requests of the c5 stream (Morse/LJ/Buckingham, 1e3-2e5 atoms, "
+               "NVE/NVT/NPT, 2.35 M atoms) resident together as one batch",
     "c5": "serving: Poisson stream of MD requests (Morse/LJ/Buckingham, N log-uniform "
           "[1e3,2e5], steps log-uniform [1e3,5e4] x steps-scale, T uniform [100,1500] K, "
           "NVE/NVT/NPT), 150 GB HBM budget, graph blocks of 100 steps",
@@ -450,13 +456,14 @@ def main():
     # stated force error of this precision against the FP64 path (the FP64
     # path itself matches the CPU oracle to 1e-12, tests/test_gpu_parity.py)
     force_err = None
-    if prec == "mixed" and args.config != "c4" and not args.bare:
+    batch = args.config in ("c4", "c5batch")
+    if prec == "mixed" and not batch and not args.bare:
         force_err, _ = force_error(specs[:1], [None], local)
 
     ctx = nd.Context(local, prec)
     ids = [W.add_to_context(ctx, s) for s in specs]
     ctx.set_tuning(args.tpa, args.graph_steps)
-    if args.config == "c4" and not args.bare:
+    if batch and not args.bare:
         ctx.autotune(10)
     # warm-up (includes the dynamics prologue: cell + Verlet list build), then
     # one block of the timed region's size so that its CUDA graph is captured
@@ -495,9 +502,9 @@ def main():
         return
 
     extra = {}
-    if args.config == "c4":
-        # the mixed path's force error on the thermalised replicas, and the
-        # plain single-system FP64 path on every 8th replica in sequence
+    if batch:
+        # the mixed path's force error on the thermalised systems, and the
+        # plain single-system FP64 path on every 8th system in sequence
         states = [ctx.state(i) for i in ids]
         if prec == "mixed":
             ea, em = force_error(specs, states, local)
@@ -506,7 +513,7 @@ def main():
         prate, pn = plain_fp64_rate(specs, local, 200, 8)
         extra["plain_fp64"] = {
             "value": prate, "unit": "atom-steps/s",
-            "sample": f"{pn} of 512 replicas (every 8th), each alone in an FP64 context, "
+            "sample": f"{pn} of {len(specs)} systems (every 8th), each alone in an FP64 context, "
                       f"200 steps, CUDA-graph blocks of 100",
             "batched_over_plain": (value / ws) / prate}
 
