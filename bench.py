@@ -532,7 +532,9 @@ def main():
         tr = traffic_per_atom(args.config)
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": (tr * N if tr else None),
-                "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+                "peak_kind": ("measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                              else "fallback: no MEASURED_PEAKS.json; 6.65 TB/s B200 copy "
+                                   "bandwidth"),
                 "alg_bytes_per_atom": alg_atom, "n_half": nb_half,
                 "pair_ms": prof["pair_ms"], "integrate_ms": prof["integrate_ms"],
                 "rebuild_ms_per_step": prof["rebuild_ms"]}

@@ -350,7 +350,8 @@ int grow_sys(ndg_ctx *c, int n) {
 long long arena_take(ndg_ctx *c, Arena &a, long long len, int which) {
   long long off = a.find(len);
   if (off < 0) {
-    long long want = std::max(a.end_used() + len, a.cap + a.cap / 2);
+    long long want = std::max(a.end_used() + len, 2 * a.cap);  // each growth copies and
+                                                                 // re-captures: double
     int rc = which == 0 ? grow_atoms(c, want) : which == 1 ? grow_cells(c, want) : grow_nbr(c, want);
     if (rc) return -1;
     off = a.find(len);
@@ -910,6 +911,15 @@ int flush_system(ndg_ctx *c, int sys) {
 }
 
 int graph_captures(ndg_ctx *c) { return c ? c->captures : 0; }
+
+int reserve_atoms(ndg_ctx *c, long long atoms) {
+  if (!c || atoms < 0) return NDG_ERR_ARG;
+  // every system's range is padded to whole chunks
+  const long long need = c->atoms.end_used() + (atoms + ATOM_ALIGN - 1) / ATOM_ALIGN;
+  if (need <= c->atoms.cap) return NDG_OK;
+  cudaSetDevice(c->device);
+  return grow_atoms(c, std::max(need, 2 * c->atoms.cap));
+}
 
 int take_system_error(ndg_ctx *c, int sys, int *err) {
   if (!valid_sys(c, sys) || !err) return NDG_ERR_ARG;

@@ -21,5 +21,8 @@ int flush_system(ndg_ctx *c, int sys);
 int graph_captures(ndg_ctx *c);
 // error bits recorded on one system (E_* of ndg_common.h), then cleared
 int take_system_error(ndg_ctx *c, int sys, int *err);
+// room at the end of the atom arena for `atoms` more atoms of systems about
+// to be added (one growth for a whole admission batch)
+int reserve_atoms(ndg_ctx *c, long long atoms);
 
 }  // namespace ndg_internal

@@ -223,6 +223,13 @@ int ndg_server_step(ndg_server *s, int *completed) {
   std::deque<long long> waiting;
   std::vector<int> fresh;
   std::vector<long long> fresh_t;
+  {
+    // room for the whole batch at once (a system's atoms are padded to 256)
+    long long atoms = 0;
+    for (size_t k = 0; k < s->queue.size(); ++k)
+      if (admit[k]) atoms += (s->reqs[s->queue[k]].np + 255) / 256 * 256;
+    if (atoms) ndg_internal::reserve_atoms(s->ctx, atoms);  // a failure shows in the adds
+  }
   for (size_t k = 0; k < s->queue.size(); ++k) {
     const long long t = s->queue[k];
     if (!admit[k]) {
