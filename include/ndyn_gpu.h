@@ -157,6 +157,19 @@ int ndg_get_control(ndg_ctx *ctx, int sys, ndg_control *c);
  * hold == NULL or ngroups == 0 removes the system's holds. */
 int ndg_set_holds(ndg_ctx *ctx, int sys, const int *hold, int ngroups, const int *dir,
                   const double *du);
+/* Spring pairs (compute2/compute3, src/nd.f90:531-933): where spring[k] != 0
+ * pair k+1 is a 'spring' line with PairParams params[4k..4k+3] = rc, D0, sc,
+ * Vol (src/read_input.f90:136, :271).  Such a pair acts through its strain
+ * against the initial positions, s = r/r0 - 1, with force -D0*s*Vol^2 along
+ * the pair and energy D0*s^2*Vol^2*r0/2, and not at all while s > sc.
+ * spring == NULL removes them.  Until ndg_set_initial_positions is called,
+ * the first run's prologue takes the positions it starts from
+ * (src/nd.f90:104). */
+int ndg_set_springs(ndg_ctx *ctx, int sys, const int *spring, const double *params);
+/* InitPos (initPositionSet, src/nd.f90:1731-1762): the initial positions
+ * (3 x np fractional, input order) and box of the spring strains; NULL takes
+ * the system's current positions or box. */
+int ndg_set_initial_positions(ndg_ctx *ctx, int sys, const double *ipos, const double *ibox);
 void ndg_default_control(ndg_control *c);
 
 /* ---- the reference routines, one call each (all systems of ctx) -------- */

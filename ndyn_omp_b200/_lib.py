@@ -27,6 +27,8 @@ SIGNATURES = [
     ("ndg_get_state", i, [vp, i, vp, vp, vp, vp]),
     ("ndg_set_control", i, [vp, i, vp]),
     ("ndg_set_holds", i, [vp, i, vp, i, vp, vp]),
+    ("ndg_set_springs", i, [vp, i, vp, vp]),
+    ("ndg_set_initial_positions", i, [vp, i, vp, vp]),
     ("ndg_get_control", i, [vp, i, vp]),
     ("ndg_default_control", None, [vp]),
     ("ndg_setup_lists", i, [vp]),

@@ -164,7 +164,22 @@ class Context:
                                   _p(masses), _p(pm), _p(rcp), _p(pp), _p(fp), _p(typ), _p(pos),
                                   _p(vel), _p(acc), _p(box), ctypes.byref(sid)), "add_system")
         self.systems[sid.value] = len(typ)
+        if any(p[3] == "spring" for p in pairs):
+            # PairParams(1:4) of each spring line: rc, D0, sc, Vol
+            flags = np.array([1 if p[3] == "spring" else 0 for p in pairs], np.int32)
+            prm = np.zeros((len(pairs), 4))
+            for k, p in enumerate(pairs):
+                prm[k, :len(p[4])] = p[4][:4]
+            _ok(self.L.ndg_set_springs(self._c, sid.value, _p(flags), _p(prm)), "set_springs")
         return sid.value
+
+    def set_initial_positions(self, sys, ipos=None, ibox=None):
+        """InitPos: the spring strains' initial positions (np,3) fractional
+        and box; None takes the current ones."""
+        ipos = None if ipos is None else np.ascontiguousarray(ipos, np.float64).reshape(-1)
+        ibox = None if ibox is None else np.ascontiguousarray(ibox, np.float64)
+        _ok(self.L.ndg_set_initial_positions(self._c, sys, _p(ipos), _p(ibox)),
+            "set_initial_positions")
 
     def remove_system(self, sys):
         _ok(self.L.ndg_remove_system(self._c, sys), "remove_system")

@@ -83,6 +83,8 @@ struct SysParam {
   int isokinetic, ke_freq, isobaric, p_freq, isoenergetic, e_freq, box_load;
   double ke_target, ke_parm, p_target[3], p_parm, e_parm, box_vel[3];
   int nhold, bc_off;             // hold groups, their first entry in DevCtx::bcd
+  int nspring;                   // spring pairs (their DevCtx::spr entries are set)
+  double ibox[3];                // box of the initial positions (spring strains)
 };
 
 // Mutable per-system state, resident on the device for the whole run.

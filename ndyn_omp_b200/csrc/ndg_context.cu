@@ -69,6 +69,9 @@ struct HostSys {
   std::vector<double> mass, rcpair, ppair, fpair;
   std::vector<float2> tF2, tP2;  // FP32 (k, k+1) pairs of fpair and ppair
   std::vector<double4> bc;       // hold groups: displacement per step, w = axis mask
+  std::vector<double4> spr;      // per pair: spring D0, sc, Vol, w = 1 (empty: no springs)
+  bool ipos_set = false;         // initial positions of the spring strains uploaded
+  double ibox[3] = {0, 0, 0};
   std::vector<int> pairmat;
   ndg_control ctl{};
   Range atoms, cells, nbr;  // atoms/cells in elements, nbr in ints
@@ -98,7 +101,7 @@ struct ndg_ctx {
   // arenas
   Arena atoms, cells, nbrs;  // atoms in chunks, cells in cells, nbrs in ints
   int nsys_cap = 0;
-  size_t cap_pm = 0, cap_pg = 0, cap_bc = 0, cap_mass = 0, cap_rc2 = 0, cap_rlist2 = 0, cap_vdr2 = 0, cap_rc2f = 0,
+  size_t cap_pm = 0, cap_pg = 0, cap_bc = 0, cap_spr = 0, cap_mass = 0, cap_rc2 = 0, cap_rlist2 = 0, cap_vdr2 = 0, cap_rc2f = 0,
          cap_tabF = 0, cap_tabP = 0, cap_tabF2 = 0, cap_tabP2 = 0;
   // device buffers
   SysParam *dP = nullptr;
@@ -110,6 +113,8 @@ struct ndg_ctx {
   double *s_vel = nullptr, *s_acc = nullptr;
   int *gid = nullptr, *s_gid = nullptr, *s_cell = nullptr, *nnb = nullptr;
   int *hold = nullptr;     // per atom slot, by input index: hold group
+  double4 *ipos = nullptr; // per atom slot, by input index: initial position
+  double4 *sprd = nullptr; // spring parameters per pair of all systems
   double4 *bcd = nullptr;  // hold groups of all systems
   int *atom_cell = nullptr, *atom_slot = nullptr, *perm = nullptr, *tmp_src = nullptr,
       *tmp_key = nullptr;
@@ -136,6 +141,7 @@ struct ndg_ctx {
   // tuning and graphs
   int tpa = 0, graph_steps = 100;
   int gather = 4;  // mixed pair loop gather depth (4 or 8)
+  int any_spring = 0;  // some system holds spring pairs
   int stab_smem = 0;  // staged-table bytes of the pair kernel (0: tables from global)
   int stab_lean = 0;  // the same without the energy table
   int nb_smem = 0;  // neighbour-build dynamic smem
@@ -192,11 +198,14 @@ DevCtx devctx(ndg_ctx *c) {
   d.force = c->force;
   d.gid = c->gid;
   d.hold = c->hold;
+  d.ipos = c->ipos;
+  d.spr = c->sprd;
   d.bcd = c->bcd;
   d.nbr = c->nbr;
   d.tile_rows = c->tile_rows;
   d.nb_vcap = c->nb_vcap;
   d.gather = c->gather;
+  d.any_spring = c->any_spring;
   d.nnb = c->nnb;
   d.atom_cell = c->atom_cell;
   d.atom_slot = c->atom_slot;
@@ -265,6 +274,7 @@ int grow_atoms(ndg_ctx *c, long long new_chunks) {
   rc |= grow(c, c->force, 3 * old, 3 * n);
   rc |= grow(c, c->gid, old, n);
   rc |= grow(c, c->hold, old, n);
+  rc |= grow(c, c->ipos, old, n);
   rc |= grow(c, c->nnb, old, n);
   rc |= grow(c, c->atom_cell, old, n);
   rc |= grow(c, c->atom_slot, 0, n);
@@ -380,7 +390,7 @@ int upload_vec(ndg_ctx *c, T *&dst, size_t &cap, const std::vector<T> &v) {
 // small per-pair/per-type arrays: rebuilt for all systems on any change
 int upload_params(ndg_ctx *c) {
   std::vector<int> pm, pg;
-  std::vector<double4> bc;
+  std::vector<double4> bc, spr;
   std::vector<double> mass, rc2, rlist2, tabF, tabP;
   std::vector<float> vdr2, rc2f;
   std::vector<float2> tF2, tP2;
@@ -405,6 +415,9 @@ int upload_params(ndg_ctx *c) {
     p.bc_off = (int)bc.size();
     p.nhold = (int)h.bc.size();
     bc.insert(bc.end(), h.bc.begin(), h.bc.end());
+    p.nspring = 0;
+    for (auto &q : h.spr) p.nspring += q.w != 0.0;
+    for (int d = 0; d < 3; ++d) p.ibox[d] = h.ibox[d];
     for (int b = 1; b <= h.ntypes; ++b)
       for (int a = 1; a <= h.ntypes; ++a) pg.push_back(gather_entry(h.pairmat.data(), h.ntypes, a, b));
     mass.insert(mass.end(), h.mass.begin(), h.mass.end());
@@ -413,8 +426,12 @@ int upload_params(ndg_ctx *c) {
       const double r = h.rcpair[j];
       const double prc2 = r * r;
       const double pdr2 = (prc2 - h.ptrmin) / (h.ptsize - 1);
-      rc2.push_back(prc2);
-      rc2f.push_back((float)prc2);
+      // a spring pair has no cutoff test: cutoff words of -1 keep it out of
+      // the kernels' table loops, and their spring pass applies the strain rule
+      const bool spring = !h.spr.empty() && h.spr[j].w != 0.0;
+      rc2.push_back(spring ? -1.0 : prc2);
+      rc2f.push_back(spring ? -1.0f : (float)prc2);
+      spr.push_back(h.spr.empty() ? make_double4(0, 0, 0, 0) : h.spr[j]);
       vdr2.push_back((float)(1.0 / pdr2));  // vPTdr2 = real(1.d0/PTdr2), src/nd.f90:254
       const double rl = skin + r;            // rcuts2 = skin + PairParams(1,.), :1375
       rlist2.push_back(rl * rl);
@@ -424,6 +441,14 @@ int upload_params(ndg_ctx *c) {
     tF2.insert(tF2.end(), h.tF2.begin(), h.tF2.end());
     tP2.insert(tP2.end(), h.tP2.begin(), h.tP2.end());
     prm[s] = p;
+  }
+  // contexts with spring pairs run the pair kernels' spring variant
+  int anys = 0;
+  for (auto &h : c->sys)
+    if (h.alive && !h.spr.empty()) anys = 1;
+  if (anys != c->any_spring) {
+    c->any_spring = anys;
+    drop_graphs(c);
   }
   // stage the tables in shared memory when every system's fit (B200 allows
   // 227 KB per block; keep room for two resident blocks per SM)
@@ -460,6 +485,7 @@ int upload_params(ndg_ctx *c) {
   rc |= upload_vec(c, c->pairmat, c->cap_pm, pm);
   rc |= upload_vec(c, c->pairg, c->cap_pg, pg);
   rc |= upload_vec(c, c->bcd, c->cap_bc, bc);
+  rc |= upload_vec(c, c->sprd, c->cap_spr, spr);
   rc |= upload_vec(c, c->mass, c->cap_mass, mass);
   rc |= upload_vec(c, c->rc2, c->cap_rc2, rc2);
   rc |= upload_vec(c, c->rlist2, c->cap_rlist2, rlist2);
@@ -615,10 +641,45 @@ int list_all_systems(ndg_ctx *c) { return list_systems(c, live_systems(c)); }
 // dynamics prologue, src/nd.f90:73-108, for the given systems: skin default,
 // MCELL, neighbour capacity; then one rebuild of their lists (the other
 // systems are left as they are)
+// initPositionSet (src/nd.f90:1731-1762): the spring strains' reference
+// positions (input order; nullptr = the current ones) and box (nullptr =
+// the current one)
+int init_positions(ndg_ctx *c, int s, const double *ipos, const double *ibox) {
+  HostSys &h = c->sys[s];
+  std::vector<double> cur;
+  if (!ipos) {
+    cur.resize(3 * (size_t)h.n);
+    int rc = ndg_get_state(c, s, cur.data(), nullptr, nullptr, nullptr);
+    if (rc) return rc;
+    ipos = cur.data();
+  }
+  std::vector<double4> p4(h.n);
+  for (int i = 0; i < h.n; ++i)
+    p4[i] = make_double4(ipos[3 * i], ipos[3 * i + 1], ipos[3 * i + 2], 0.0);
+  CK(c, cudaMemcpy(c->ipos + (size_t)h.atoms.off * ATOM_ALIGN, p4.data(),
+                   h.n * sizeof(double4), cudaMemcpyHostToDevice));
+  if (ibox) {
+    for (int d = 0; d < 3; ++d) h.ibox[d] = ibox[d];
+  } else {
+    SysState S;
+    int rc = get_state_dev(c, s, S);
+    if (rc) return rc;
+    for (int d = 0; d < 3; ++d) h.ibox[d] = S.box[d];
+  }
+  h.ipos_set = true;
+  c->params_dirty = true;
+  return NDG_OK;
+}
+
 int setup_lists(ndg_ctx *c, const std::vector<int> &which) {
   for (int s : which) {
     HostSys &h = c->sys[s];
     if (!h.alive) continue;
+    if (!h.spr.empty() && !h.ipos_set) {
+      // the dynamics prologue takes the current positions (src/nd.f90:104)
+      int rc = init_positions(c, s, nullptr, nullptr);
+      if (rc) return rc;
+    }
     if (h.ctl.skin < 0) h.ctl.skin = 0.2 * h.rcut;  // persists, as in the reference
     fill_control_params(h);
     SysState S;
@@ -869,7 +930,7 @@ int status_from_words(ndg_ctx *c) {
 ndg_ctx::~ndg_ctx() {
   drop_graphs(this);
   void *ptrs[] = {dP, dS, chunk_sys, cell_sys, pos, s_pos, pfx, vel, acc, disp, force, s_vel,
-                  s_acc, gid, s_gid, s_cell, nnb, hold, bcd, atom_cell, atom_slot, perm, tmp_src, tmp_key,
+                  s_acc, gid, s_gid, s_cell, nnb, hold, bcd, ipos, sprd, atom_cell, atom_slot, perm, tmp_src, tmp_key,
                   cell_count, cell_start, rb_list, plan, plan_kb, plan_hdr, nbr, tile_rows, red, itop, ired, pairmat, pairg, mass, rc2, rlist2,
                   vdr2, rc2f, tabF, tabP, tabF2, tabP2, ring, ring_count};
   for (void *p : ptrs)
@@ -1189,6 +1250,30 @@ int ndg_set_holds(ndg_ctx *c, int s, const int *hold, int ngroups, const int *di
     h.bc[g] = make_double4(du[3 * g], du[3 * g + 1], du[3 * g + 2], (double)m);
   }
   return NDG_OK;
+}
+
+int ndg_set_springs(ndg_ctx *c, int s, const int *spring, const double *params) {
+  if (!valid_sys(c, s) || (spring && !params)) return NDG_ERR_ARG;
+  cudaSetDevice(c->device);
+  HostSys &h = c->sys[s];
+  c->params_dirty = true;
+  h.spr.clear();
+  if (!spring) return NDG_OK;
+  bool any = false;
+  for (int k = 0; k < h.npairs; ++k) any |= spring[k] != 0;
+  if (!any) return NDG_OK;
+  h.spr.resize(h.npairs);
+  for (int k = 0; k < h.npairs; ++k) {
+    const double *q = params + 4 * k;  // PairParams(1:4, k): rc, D0, sc, Vol
+    h.spr[k] = spring[k] ? make_double4(q[1], q[2], q[3], 1.0) : make_double4(0, 0, 0, 0);
+  }
+  return NDG_OK;
+}
+
+int ndg_set_initial_positions(ndg_ctx *c, int s, const double *ipos, const double *ibox) {
+  if (!valid_sys(c, s)) return NDG_ERR_ARG;
+  cudaSetDevice(c->device);
+  return init_positions(c, s, ipos, ibox);
 }
 
 int ndg_load_state(ndg_ctx *c, int s, const double *pos, const double *vel, const double *acc,

@@ -1518,6 +1518,90 @@ __device__ __forceinline__ float4 pair_params(const TabView &tv, int p1) {
   return make_float4(r * (1.f - NEAR_CUT), r * (1.f + NEAR_CUT), tv.vdr2[p1], r);
 }
 
+// A spring pair (compute2/compute3, src/nd.f90:627-660, 826-859): strain
+// s = r/r0 - 1 of the pair against its initial separation (initial
+// positions ipos, box ibox, minimum image by one anint); no force while
+// s > sc; else df = -D0*s*Vol^2/r along rij and energy D0*s^2*Vol^2*r0/2.
+// Returns false where the pair is broken.
+__device__ __forceinline__ bool spring_df(const DevCtx &c, const SysParam *P, int gi, int gj,
+                                          double d2, const double4 &sp, double &df, double &dp) {
+  const double4 a = c.ipos[P->atom_off + gi], b = c.ipos[P->atom_off + gj];
+  double s0 = a.x - b.x, s1 = a.y - b.y, s2 = a.z - b.z;
+  s0 = s0 - round(s0);
+  s1 = s1 - round(s1);
+  s2 = s2 - round(s2);
+  const double x0 = P->ibox[0] * s0, x1 = P->ibox[1] * s1, x2 = P->ibox[2] * s2;
+  double d20 = x0 * x0;
+  d20 = d20 + x1 * x1;
+  d20 = d20 + x2 * x2;
+  const double r = sqrt(d2), r0 = sqrt(d20);
+  const double sij = r / r0 - 1.0;
+  if (sij > sp.y) return false;
+  const double f = sp.x * sij * sp.z * sp.z;
+  dp = 0.5 * f * sij * r0;
+  df = -f / r;
+  return true;
+}
+
+// One atom's spring pairs, its share of the list entries (k = la, la+tpa,
+// ...), in FP64: force, energy (cu) and virial (cv) of the pairs with
+// PTij = PTji.  Mixed precision takes each pair's terms in 64-bit fixed
+// point (q), so the totals do not depend on the launch shape; FP64 sums
+// them in list order (d).
+struct SpringSum {
+  long long q[10];  // fx, fy, fz, pe, virial xx yy zz xy xz yz
+  double d[10];
+};
+
+template <bool MIXED>
+__device__ __noinline__ SpringSum spring_pass(const DevCtx &c, const SysParam *P, const SysState *S,
+                                              const int *pm, int i, int ti, int ntypes,
+                                              const int *nb, int cnt, int la, int tpa, bool cu,
+                                              bool cv) {
+  SpringSum o;
+  for (int k = 0; k < 10; ++k) {
+    o.q[k] = 0;
+    o.d[k] = 0.0;
+  }
+  const double4 pid = c.pos[i];
+  const double b0 = S->box[0], b1 = S->box[1], b2 = S->box[2];
+  const int gi = c.gid[i];
+  for (int k = la; k < cnt; k += tpa) {
+    const int j = __ldg(nb + k * TILE);
+    const double4 pjd = c.pos[j];
+    const int pg = pm[(ti - 1) + (tw_type(tw_of(pjd.w)) - 1) * ntypes];
+    const int pt = pg & PT_MASK;
+    if (pt == 0) continue;
+    const double4 sp = c.spr[P->pair_off + pt - 1];
+    if (sp.w == 0.0) continue;
+    double s0 = pid.x - pjd.x, s1 = pid.y - pjd.y, s2 = pid.z - pjd.z;
+    s0 = s0 - round(s0);
+    s1 = s1 - round(s1);
+    s2 = s2 - round(s2);
+    const double x[3] = {b0 * s0, b1 * s1, b2 * s2};
+    double dd = x[0] * x[0];
+    dd = dd + x[1] * x[1];
+    dd = dd + x[2] * x[2];
+    double df, dp;
+    if (!spring_df(c, P, gi, c.gid[j], dd, sp, df, dp)) continue;
+    const bool sym = pg < PT_ASYM;
+    double t[10] = {x[0] * df, x[1] * df, x[2] * df, (cu && sym) ? dp : 0.0, 0, 0, 0, 0, 0, 0};
+    if (cv && sym) {
+      t[4] = x[0] * x[0] * df;
+      t[5] = x[1] * x[1] * df;
+      t[6] = x[2] * x[2] * df;
+      t[7] = x[0] * x[1] * df;
+      t[8] = x[0] * x[2] * df;
+      t[9] = x[1] * x[2] * df;
+    }
+    for (int q = 0; q < 10; ++q) {
+      if (MIXED) o.q[q] += __double2ll_rn(t[q] * FORCE_FX);
+      else o.d[q] = o.d[q] + t[q];
+    }
+  }
+  return o;
+}
+
 // STAB: tables staged in shared memory (else read from global memory).
 // EV: the kernel of steps that need the potential energy or the virial
 // (calcPot / calcVirial); the kernel of the other steps carries no energy
@@ -1545,7 +1629,9 @@ constexpr int pair_ctas() {
   return MIXED ? (EV ? 5 : (GATHER > 4 ? 6 : 7)) : (EV ? 4 : 5);
 }
 
-template <int TPA, bool MIXED, bool FUSE, bool STAB, bool EV, int GATHER>
+// SPRING: the variant for contexts that hold spring pairs (one thread per
+// atom, gather depth 4); the others carry no spring code at all.
+template <int TPA, bool MIXED, bool FUSE, bool STAB, bool EV, int GATHER, bool SPRING = false>
 __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 / (TILE * TPA)) > 0
                                              ? pair_ctas<MIXED, EV, GATHER>() * 128 / (TILE * TPA)
                                              : 1) void k_pair(DevCtx c, int host_flags, int ntiles,
@@ -1854,6 +1940,26 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 /
         if (one) loop(std::true_type{});
         else loop(std::false_type{});
       }
+      if (SPRING && P->nspring > 0) {
+        // spring pairs (compute2/compute3), left out of the loops above by
+        // their cutoff word (-1), out of line so that they cost the other
+        // systems nothing
+        const SpringSum sp = spring_pass<MIXED>(c, P, S, tv.pm, i, ti, ntypes, nb, cnt, la, TPA,
+                                                cu, cv);
+        if (MIXED) {
+          qx += sp.q[0];
+          qy += sp.q[1];
+          qz += sp.q[2];
+          if (EV)
+            for (int k = 0; k < 7; ++k) evq[k * NT + threadIdx.x] += (unsigned long long)sp.q[3 + k];
+        } else {
+          fx = fx + sp.d[0];
+          fy = fy + sp.d[1];
+          fz = fz + sp.d[2];
+          pe = pe + sp.d[3];
+          for (int k = 0; k < 6; ++k) vir[k] = vir[k] + sp.d[4 + k];
+        }
+      }
     }
     if (!MIXED) {
       // combine the TPA partial forces of an atom (fixed tree: deterministic)
@@ -2001,10 +2107,10 @@ static int sm_count() {
 
 // grid of a pair-kernel variant (one wave of resident blocks); with launch
 // set, also launches it
-template <int TPA, bool MIXED, bool FUSE, bool STAB, bool EV, int GATHER>
+template <int TPA, bool MIXED, bool FUSE, bool STAB, bool EV, int GATHER, bool SPRING = false>
 static int pair_launch(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh,
                        bool launch) {
-  auto kern = k_pair<TPA, MIXED, FUSE, STAB, EV, GATHER>;
+  auto kern = k_pair<TPA, MIXED, FUSE, STAB, EV, GATHER, SPRING>;
   const int smem = (STAB ? (EV ? c.stab_smem : c.stab_lean) : 0) +
                    ((MIXED && EV) ? 7 * 8 * TILE * TPA : 0);
   static int cfg_smem = -1, occ = 0;
@@ -2025,6 +2131,9 @@ static int pair_launch(const DevCtx &c, cudaStream_t st, int hf, unsigned long l
 template <int TPA, bool MIXED, bool FUSE, bool STAB, bool EV>
 static int pair_go(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh,
                    bool launch = true) {
+  if constexpr (TPA == 1) {
+    if (c.any_spring) return pair_launch<1, MIXED, FUSE, STAB, EV, 4, true>(c, st, hf, nh, launch);
+  }
   if (MIXED && TPA == 1 && c.gather > 4)
     return pair_launch<TPA, MIXED, FUSE, STAB, EV, 8>(c, st, hf, nh, launch);
   return pair_launch<TPA, MIXED, FUSE, STAB, EV, 4>(c, st, hf, nh, launch);
@@ -2070,6 +2179,7 @@ static void pair_tpa(const DevCtx &c, cudaStream_t st, int mixed, int fuse, int 
 
 static void pair_dispatch(const DevCtx &c, cudaStream_t st, int tpa, int mixed, int fuse, int hf,
                           unsigned long long next_h, int *g) {
+  if (c.any_spring) tpa = 1;  // the spring variant is built for one thread per atom
   switch (tpa) {
     case 1: pair_tpa<1>(c, st, mixed, fuse, hf, next_h, g); break;
     case 2: pair_tpa<2>(c, st, mixed, fuse, hf, next_h, g); break;

@@ -32,12 +32,15 @@ struct DevCtx {
   int nb_smem;  // neighbour build dynamic smem
   int nb_vcap;  // flat candidate-list capacity of the build
   int gather;   // mixed pair loop: neighbour gathers in flight (4 or 8)
+  int any_spring;  // some system holds spring pairs: the pair kernels' spring variant
   double4 *pos;
   int4 *pfx;
   double *vel, *acc, *disp, *force;
   int *gid;
   const int *hold;     // per atom, by input index: hold group (0 = none)
   const double4 *bcd;  // per hold group: displacement per step (x, y, z), w = axis mask
+  const double4 *ipos; // per atom, by input index: initial position (spring strains)
+  const double4 *spr;  // per pair: spring D0, sc, Vol, w = 1 for a spring pair
   int *nbr;  // blocked neighbour list (128-atom tiles), atom slots
   int *nnb;
   int *tile_rows;  // per tile: rows of its list in use (L2 prefetch size)

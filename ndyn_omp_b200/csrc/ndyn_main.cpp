@@ -150,6 +150,12 @@ struct Driver {
   std::vector<int> bcdir;
   std::vector<double> bcparm;
   bool holds_dirty = false;
+  // spring pairs (their PairParams) and InitPos (src/read_input.f90:136,165)
+  std::vector<int> spring;
+  std::vector<double> pparams;
+  bool springs_dirty = false, ipos_pending = false;
+  std::vector<double> ipos;
+  double ibox[3] = {0, 0, 0};
 
   // positions as the device has them after a run (for domain selections)
   int sync_positions() {
@@ -276,6 +282,18 @@ struct Driver {
     c.quirk = quirk;
     rc = ndg_set_control(ctx, sys, &c);
     if (rc) return rc;
+    if (springs_dirty) {
+      bool any = false;
+      for (int f : spring) any |= f != 0;
+      rc = ndg_set_springs(ctx, sys, any ? spring.data() : nullptr, any ? pparams.data() : nullptr);
+      if (rc) return rc;
+      springs_dirty = false;
+    }
+    if (ipos_pending) {
+      rc = ndg_set_initial_positions(ctx, sys, ipos.data(), ibox);
+      if (rc) return rc;
+      ipos_pending = false;
+    }
     if (holds_dirty) {
       const bool any = !hname.empty();
       rc = ndg_set_holds(ctx, sys, any ? hold.data() : nullptr, (int)hname.size(),
@@ -389,6 +407,14 @@ int main(int argc, char **argv) {
         if (sym) d.pairmat[(b - 1) + (size_t)(a - 1) * nt] = i + 1;
       }
       d.npairs = np;
+      d.spring.assign(np, 0);
+      d.pparams = par;
+      for (int i = 0; i < np; ++i) {
+        // PairParams(1,:) defaults to the global rcut where a line gives none
+        // (src/read_input.f90:123); a spring's rc, D0, sc, Vol follow
+        d.spring[i] = std::strncmp(names.data() + 8 * i, "spring  ", 8) == 0;
+      }
+      d.springs_dirty = true;
       d.ppair.assign((size_t)(d.ptsize + 1) * np, 0.0);
       d.fpair.assign((size_t)(d.ptsize + 1) * np, 0.0);
       std::vector<double> rc2(np), dr2(np);
@@ -498,6 +524,18 @@ int main(int argc, char **argv) {
         d.bcparm[3 * (g - 1) + a] = on ? std::atof(v.c_str()) : 0.0;
       }
       d.holds_dirty = true;
+    } else if (k == "InitPos") {
+      // initPositionSet, only with spring pairs (src/read_input.f90:165)
+      bool any = false;
+      for (int f : d.spring) any |= f != 0;
+      if (!any) {
+        std::printf("# WARNING: InitPos not applicable without a spring potential\n");
+      } else {
+        if (d.sync_positions()) return 4;
+        d.ipos = d.pos;
+        for (int a = 0; a < 3; ++a) d.ibox[a] = d.box[a];
+        d.ipos_pending = true;
+      }
     } else if (k == "ClearHolds") {
       d.hold.assign(d.typ.size(), 0);
       d.hname.clear();

@@ -91,6 +91,23 @@ def onesided_alloy(n_cells=8, T=300.0, seed=7, quirk="fixed", frac2=0.4):
                 control=dict(dt=0.1, skin=ONESIDED["skin"], out_steps=100, quirk=quirk))
 
 
+def spring_alloy(n_cells=8, T=300.0, seed=11, quirk="fixed", frac2=0.3, onesided=False):
+    """Two-type FCC alloy whose type-1 nearest neighbours are bonded by
+    strain springs ('spring' rc=3.0 A D0=4 eV/A sc=0.08 Vol=1, acting against
+    the initial configuration: compute2, or compute3 when the type-1/type-2
+    LJ line is one-sided); type-2 pairs are Morse."""
+    rng = np.random.default_rng(seed)
+    pos, box = lattice((n_cells,) * 3, ONESIDED["a"], FCC_BASIS)
+    typ = np.where(rng.random(len(pos)) < frac2, 2, 1).astype(np.int32)
+    vel = mb_velocities(typ, ONESIDED["masses"], T, rng)
+    pairs = [(1, 1, True, "spring", [3.0, 4.0, 0.08, 1.0]),
+             (2, 2, True, "morse", [6.0, 0.4205, 1.4199, 2.780]),
+             (1, 2, not onesided, "LJ", [6.0, 0.02, 2.4])]
+    return dict(name=f"spring_alloy{n_cells}", masses=ONESIDED["masses"], pairs=pairs,
+                typ=typ, pos=pos, box=box, vel=vel,
+                control=dict(dt=0.1, skin=0.5, out_steps=100, quirk=quirk))
+
+
 def ar_liquid(n_cells=40, T=120.0, seed=2, quirk="fixed", thermostat=True):
     """C2: LJ argon at reduced density 0.8442, +-0.05 sigma jitter, NVT."""
     rng = np.random.default_rng(seed)

@@ -32,6 +32,8 @@ struct ora_sys {
   int ntypes, npairs, ptsize;
   int *pairmat; /* ntypes x ntypes column-major, values 1..npairs or 0 */
   int asympots; /* some Pairs line is one-sided ('asym'), src/read_input.f90:131-133 */
+  int springpots; /* some pair is a 'spring', src/read_input.f90:136 */
+  double *ipos, initbox[3]; /* initial positions and box of the spring strains */
   double *mass;
   double *ptdr2, *ptrc2, *pairparams /* 4 x npairs */, *ppair, *fpair,
       *qprod;
@@ -249,6 +251,16 @@ int ora_set_holds(ora_sys *s, const int *hold, int ngroups, const int *dir, cons
   return ORA_OK;
 }
 
+/* initPositionSet, src/nd.f90:1731-1762: the spring strains' reference
+ * positions (NULL = the current ones) and box (NULL = the current one) */
+int ora_init_positions(ora_sys *s, const double *ipos, const double *ibox) {
+  if (!s->pos) return ORA_ERR_ARG;
+  if (!s->ipos) s->ipos = (double *)malloc(sizeof(double) * 3 * (size_t)s->np);
+  memcpy(s->ipos, ipos ? ipos : s->pos, sizeof(double) * 3 * (size_t)s->np);
+  memcpy(s->initbox, ibox ? ibox : s->box, sizeof(double) * 3);
+  return ORA_OK;
+}
+
 static void free_state(ora_sys *s) {
   free(s->typ); free(s->pos); free(s->vel); free(s->acc); free(s->force);
   s->typ = NULL;
@@ -265,7 +277,7 @@ static void free_pairs(ora_sys *s) {
 
 void ora_free(ora_sys *s) {
   if (!s) return;
-  free_lists(s); free_state(s); free_pairs(s); free_holds(s); free(s->mass);
+  free_lists(s); free_state(s); free_pairs(s); free_holds(s); free(s->ipos); free(s->mass);
   free(s);
 }
 
@@ -320,6 +332,7 @@ int ora_set_pairs(ora_sys *s, int npairs, double ptrmin, int ptsize,
   s->pairname = (char(*)[9])calloc(npairs, 9);
   for (int j = 0; j < npairs; ++j) s->pairparams[4 * j] = s->rcut; /* :156 */
   s->asympots = 0;
+  s->springpots = 0;
   for (int j = 0; j < npairs; ++j) {
     if (!sym[j]) s->asympots = 1;
     int a = p1[j], b = p2[j];
@@ -331,6 +344,7 @@ int ora_set_pairs(ora_sys *s, int npairs, double ptrmin, int ptsize,
     for (int k = 7; k >= 0 && (s->pairname[j][k] == ' ' || s->pairname[j][k] == 0); --k)
       s->pairname[j][k] = 0;
     if (pot_kind(s->pairname[j]) == P_NONE) return ORA_ERR_POTENTIAL;
+    if (pot_kind(s->pairname[j]) == P_SPRING) s->springpots = 1;
     for (int k = 0; k < nparams[j] && k < 4; ++k) s->pairparams[4 * j + k] = params[4 * j + k];
     s->qprod[j] = qprod ? qprod[j] : 0.0;
   }
@@ -379,6 +393,8 @@ int ora_set_state(ora_sys *s, int np, const int *typ, const double *pos,
   free_state(s);
   free_lists(s);
   free_holds(s); /* hold groups name atoms of the previous state */
+  free(s->ipos);
+  s->ipos = NULL;
   s->np = np;
   s->typ = (int *)malloc(sizeof(int) * np);
   s->pos = (double *)malloc(sizeof(double) * 3 * np);
@@ -558,6 +574,7 @@ static int compute_mcell(ora_sys *s) {
 int ora_setup_lists(ora_sys *s) {
   if (!s->pos || !s->ppair) return ORA_ERR_ARG;
   if (s->c.skin < 0.0) s->c.skin = s->rcut * 0.2;
+  if (s->springpots && !s->ipos) ora_init_positions(s, NULL, NULL); /* src/nd.f90:104 */
   int rc = compute_mcell(s);
   if (rc) return rc;
   if (s->c.neimax == 0) {
@@ -845,10 +862,136 @@ void ora_compute1(ora_sys *s, int cv, int cu) {
   free(vtmp); free(ptmp); free(vdr2);
 }
 
-/* the force routine dynamics calls, src/nd.f90:155-163 (no spring pairs) */
+/* compute2 (src/nd.f90:531-727) and compute3 (:728-933): compute0 and
+ * compute1 with 'spring' pairs, which act through their strain against the
+ * initial configuration (:627-660, :826-859): s = r/r0 - 1, no force while
+ * s > PairParams(3); df = -PairParams(2)*s*Vol^2/r with Vol = PairParams(4),
+ * energy PairParams(2)*s*Vol^2*s*r0/2; no cutoff test.  compute2 counts
+ * every pair's energy and virial and pushes both atoms; compute3 applies
+ * compute1's one-sided rules.  Table pairs as in compute0/compute1 (compute2
+ * leaves k unclamped, :666; clamped to 1 here as compute0 does). */
+static void compute_springs(ora_sys *s, int cv, int cu, int asym) {
+  const int T = s->nthreads, np = s->np, npairs = s->npairs;
+  const int stride = s->neimax + 1, tsz = s->ptsize + 1;
+  double *vtmp = (double *)calloc(6 * (size_t)T, sizeof(double));
+  double *ptmp = (double *)calloc((size_t)T, sizeof(double));
+  float *vdr2 = (float *)malloc(sizeof(float) * npairs);
+  if (cv) for (int k = 0; k < 6; ++k) s->virial[k] = 0.0;
+  if (cu) s->potential = 0.0;
+  for (int p = 0; p < npairs; ++p) vdr2[p] = (float)(1.0 / s->ptdr2[p]);
+  double *force = s->force, *ftmp = s->ftmp;
+  const double *pos = s->pos, *box = s->box, *fp = s->fpair, *pp = s->ppair;
+  const double *rc2 = s->ptrc2, *ib = s->initbox, *ip = s->ipos;
+  const double ptrmin = s->ptrmin;
+  memset(force, 0, sizeof(double) * 3 * (size_t)np);
+  memset(ftmp, 0, sizeof(double) * 3 * (size_t)np * T);
+#pragma omp parallel num_threads(T)
+  {
+    int tid = omp_get_thread_num();
+    int istart = (np / T) * tid;
+    int iend = (np / T) * (tid + 1);
+    if (iend < np && tid == T - 1) iend = np;
+    double *ft = ftmp + 3 * (size_t)np * tid;
+    double pt = 0.0, vt[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = istart; i < iend; ++i) {
+      const double *pi = pos + 3 * (size_t)i;
+      int typi = s->typ[i];
+      const int *row = s->vnl + (size_t)stride * i;
+      for (int jn = 1; jn < row[0]; ++jn) {
+        int j = row[jn];
+        int ptij = pm(s, typi, s->typ[j]), ptji = pm(s, s->typ[j], typi);
+        int p = asym ? (ptij > ptji ? ptij : ptji) : ptij;
+        int count = asym ? ptij == ptji : 1;
+        double rij[3];
+        double d2 = pair_d2(pi, pos + 3 * (size_t)j, box, rij);
+        double df, dp = 0.0;
+        if (pot_kind(s->pairname[p - 1]) == P_SPRING) {
+          double sr[3], rij0[3];
+          for (int d = 0; d < 3; ++d) {
+            sr[d] = ip[3 * (size_t)i + d] - ip[3 * (size_t)j + d];
+            sr[d] = sr[d] - round(sr[d]);
+            rij0[d] = ib[d] * sr[d];
+          }
+          double d20 = rij0[0] * rij0[0];
+          d20 = d20 + rij0[1] * rij0[1];
+          d20 = d20 + rij0[2] * rij0[2];
+          double r = sqrt(d2), r0 = sqrt(d20);
+          double sij = r / r0 - 1.0;
+          const double *prm = s->pairparams + 4 * (size_t)(p - 1);
+          if (sij > prm[2]) continue;
+          double vi = prm[3];
+          df = prm[1] * sij * vi * vi;
+          if (cu) dp = 0.5 * df * sij * r0;
+          df = -df / r;
+        } else {
+          if (d2 > rc2[p - 1]) continue;
+          float rk = (float)(d2 - ptrmin) * vdr2[p - 1] + 1.0f;
+          int k = (int)rk;
+          if (k < 1) k = 1;
+          double w = (double)rk - (double)k;
+          const double *F = fp + (size_t)tsz * (p - 1) + (k - 1);
+          df = w * F[1] + (1.0 - w) * F[0];
+          if (cu) {
+            const double *P = pp + (size_t)tsz * (p - 1) + (k - 1);
+            dp = w * P[1] + (1.0 - w) * P[0];
+          }
+          df = df / d2;
+        }
+        if (cu && count) pt = pt + dp;
+        if (!asym || ptji > 0) {
+          ft[3 * (size_t)i] += rij[0] * df;
+          ft[3 * (size_t)i + 1] += rij[1] * df;
+          ft[3 * (size_t)i + 2] += rij[2] * df;
+        }
+        if (!asym || ptij > 0) {
+          ft[3 * (size_t)j] -= rij[0] * df;
+          ft[3 * (size_t)j + 1] -= rij[1] * df;
+          ft[3 * (size_t)j + 2] -= rij[2] * df;
+        }
+        if (cv && count) {
+          vt[0] += rij[0] * rij[0] * df;
+          vt[1] += rij[1] * rij[1] * df;
+          vt[2] += rij[2] * rij[2] * df;
+          vt[3] += rij[0] * rij[1] * df;
+          vt[4] += rij[0] * rij[2] * df;
+          vt[5] += rij[1] * rij[2] * df;
+        }
+      }
+    }
+    ptmp[tid] = pt;
+    for (int k = 0; k < 6; ++k) vtmp[6 * tid + k] = vt[k];
+#pragma omp barrier
+    for (int t = 0; t < T; ++t) {
+      const double *src = ftmp + 3 * (size_t)np * t;
+      for (int i = istart; i < iend; ++i) {
+        force[3 * (size_t)i] += src[3 * (size_t)i];
+        force[3 * (size_t)i + 1] += src[3 * (size_t)i + 1];
+        force[3 * (size_t)i + 2] += src[3 * (size_t)i + 2];
+      }
+    }
+  }
+  if (cv)
+    for (int t = 0; t < T; ++t)
+      for (int k = 0; k < 6; ++k) s->virial[k] += vtmp[6 * t + k];
+  if (cu)
+    for (int t = 0; t < T; ++t) s->potential += ptmp[t];
+  free(vtmp); free(ptmp); free(vdr2);
+}
+
+void ora_compute2(ora_sys *s, int cv, int cu) { compute_springs(s, cv, cu, 0); }
+void ora_compute3(ora_sys *s, int cv, int cu) { compute_springs(s, cv, cu, 1); }
+
+/* the force routine dynamics calls, src/nd.f90:155-163 */
 void ora_compute(ora_sys *s, int cv, int cu) {
-  if (s->asympots) ora_compute1(s, cv, cu);
-  else ora_compute0(s, cv, cu);
+  if (s->springpots) {
+    if (!s->ipos) ora_init_positions(s, NULL, NULL);
+    if (s->asympots) ora_compute3(s, cv, cu);
+    else ora_compute2(s, cv, cu);
+  } else if (s->asympots) {
+    ora_compute1(s, cv, cu);
+  } else {
+    ora_compute0(s, cv, cu);
+  }
 }
 
 /* integrate2, src/nd.f90:1081-1121 */

@@ -121,7 +121,11 @@ void ora_compute0(ora_sys *s, int cv, int cu); /* src/nd.f90:200-363 */
 void ora_compute1(ora_sys *s, int cv, int cu); /* src/nd.f90:364-530 */
 /* hold groups with displacement conditions, src/read_input.f90:177-190 */
 int ora_set_holds(ora_sys *s, const int *hold, int ngroups, const int *dir, const double *du);
-void ora_compute(ora_sys *s, int cv, int cu);  /* compute0 or compute1, src/nd.f90:155-163 */
+void ora_compute2(ora_sys *s, int cv, int cu); /* springs, src/nd.f90:531-727 */
+void ora_compute3(ora_sys *s, int cv, int cu); /* springs + one-sided pairs, src/nd.f90:728-933 */
+void ora_compute(ora_sys *s, int cv, int cu);  /* the dispatch of src/nd.f90:155-163 */
+/* InitPos / initPositionSet, src/nd.f90:1731-1762 (NULL: the current state) */
+int ora_init_positions(ora_sys *s, const double *ipos, const double *ibox);
 void ora_integrate2(ora_sys *s, int ck);       /* src/nd.f90:1081-1121 */
 void ora_mk_iso_ke(ora_sys *s);        /* src/nd.f90:1122-1158 */
 void ora_mk_iso_e(ora_sys *s);         /* src/nd.f90:1159-1182 */

@@ -82,6 +82,10 @@ def lib():
             getattr(L, f).argtypes = [vp]
             getattr(L, f).restype = None
         L.ora_set_holds.argtypes = [vp, vp, i, vp, vp]
+        L.ora_init_positions.argtypes = [vp, vp, vp]
+        for f in ("ora_compute2", "ora_compute3"):
+            getattr(L, f).argtypes = [vp, i, i]
+            getattr(L, f).restype = None
         for f in ("ora_compute0", "ora_compute1", "ora_compute"):
             getattr(L, f).argtypes = [vp, i, i]
             getattr(L, f).restype = None
@@ -233,6 +237,11 @@ class Oracle:
         dirs = np.ascontiguousarray(np.asarray(dirs, bool).reshape(-1, 3), np.int32)
         du = np.ascontiguousarray(np.asarray(du, np.float64).reshape(-1, 3))
         assert self.L.ora_set_holds(self.s, _p(hold), len(du), _p(dirs), _p(du)) == 0
+
+    def init_positions(self, ipos=None, ibox=None):
+        ipos = None if ipos is None else np.ascontiguousarray(ipos, np.float64).reshape(-1)
+        ibox = None if ibox is None else np.ascontiguousarray(ibox, np.float64)
+        assert self.L.ora_init_positions(self.s, _p(ipos), _p(ibox)) == 0
 
     def compute(self, cv=1, cu=1):
         """The force routine dynamics would call: compute1 when some pair

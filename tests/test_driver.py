@@ -124,3 +124,30 @@ def test_driver_hold_rigid_translation(tmp_path):
     assert len(pe) >= 5 and len(set(pe)) == 1
     pe2 = go(["Hold slab dom rec T 0 0 0 0 -0.5 -0.3", "Disp slab 2.0e-4 F F"])
     assert len(set(pe2)) > 1
+
+
+def test_driver_springs_match_oracle(tmp_path):
+    """A 'spring' Pairs line through the driver (compute2 against the
+    configuration the first Run starts from, src/nd.f90:104) prints the same
+    thermo rows as the oracle's driver on the same script."""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    import oracle_py
+    case = GOLD["MorseTest"]
+    lattice.materialise(case["model"], str(tmp_path))
+    script = ["Model model.dump dump", "NeiMax 200", "Types 1", " Cu 63.546", "Pairs 1",
+              " Cu Cu sym spring 3.0 4.0 0.08 1.0", "Seed 99", "Velocity 0.03", "OutFreq 10",
+              "Run 60 0.1", "END"]
+    r = subprocess.run([EXE], input="START\n" + "\n".join(script) + "\n", text=True,
+                       capture_output=True, cwd=str(tmp_path), timeout=600)
+    assert r.returncode == 0, r.stderr
+    ours = [ln.split() for ln in r.stdout.splitlines()
+            if len(ln.split()) == 6 and ln.split()[0].isdigit()]
+    rc, ref, _, err = oracle_py.run_script(script, str(tmp_path))
+    assert rc == 0, err
+    assert len(ours) == len(ref) >= 6
+    for a, b in zip(ours, ref):
+        assert int(a[0]) == b["step"]
+        assert _close(float(a[1]), b["pe"], 2e-6, 1e-9), (a, b["text"])
+        assert _close(float(a[2]), b["ke"], 2e-6, 0), (a, b["text"])
+    assert float(ours[-1][1]) > 0.0  # the springs are strained by the motion

@@ -129,6 +129,50 @@ def test_onesided_pairs_compute1(specs, prec, tol):
     assert np.linalg.norm(fo.sum(axis=0)) > 1e-6 * np.abs(fo).sum()  # no Newton-3 balance
 
 
+def _spring_spec(onesided, seed):
+    spec = W.spring_alloy(6, 300.0, seed=seed, quirk="fixed", onesided=onesided)  # 864 atoms
+    ipos = np.asarray(spec["pos"], np.float64).reshape(-1, 3).copy()
+    spec["pos"] = W.jitter(spec["pos"], spec["box"], 0.08, np.random.default_rng(seed + 1))
+    return spec, ipos
+
+
+@pytest.mark.parametrize("onesided", [False, True])
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("mixed", 1e-5)])
+def test_springs_compute2_compute3(onesided, prec, tol):
+    """Spring pairs (compute2; compute3 with a one-sided line) strained
+    against the lattice: forces, energy and virial against the oracle."""
+    spec, ipos = _spring_spec(onesided, 20)
+    o = oracle_from_spec(spec)
+    o.init_positions(ipos)
+    o.setup_lists()
+    o.compute(1, 1)
+    fo, peo, viro, _ = o.forces()
+    with nd.Context(0, prec) as ctx:
+        sid = gpu_from_spec(ctx, spec)
+        ctx.set_initial_positions(sid, ipos)
+        ctx.setup_lists()
+        assert np.array_equal(pair_multiset(ctx.neighbors(sid)), pair_multiset(o.neighbors()))
+        ctx.compute0(True, True)
+        fg, peg, virg, _ = ctx.forces(sid)
+    assert rel_l2(fg, fo) < tol
+    assert abs(peg - peo) <= (1e-12 if prec == "fp64" else 1e-6) * abs(peo)
+    assert rel_l2(virg, viro) < tol
+
+
+def test_run_springs_fp64():
+    """A run with springs: the prologue takes the starting positions as the
+    initial configuration (src/nd.f90:104) on both sides."""
+    spec = W.spring_alloy(6, 600.0, seed=22, quirk="fixed")
+    spec["control"] = dict(spec["control"], out_steps=10)
+    o, ro, rg, (pg, _, _, _), nup = _run_both(spec, 80)
+    for a, b in zip(rg, ro):
+        assert a["pe"] == pytest.approx(b["pe"], rel=1e-10, abs=1e-9)
+        assert a["ke"] == pytest.approx(b["ke"], rel=1e-9)
+    po, _, _, _ = o.state()
+    assert rel_l2(pg, po) < 1e-12
+    assert nup == o.list_updates
+
+
 def test_integrate1_bit_exact(specs):
     spec = dict(specs["ar_fixed"])
     rng = np.random.default_rng(5)
