@@ -1438,8 +1438,10 @@ struct TabView {
   const float2 *tF2, *tP2;  // FP32 (k, k+1) pairs
 };
 
-// Staged layout (stab_bytes): pair matrix | rc2 (double) | packed per-pair
-// float4 | F table | P table.  The kernel without energy skips the P table.
+// Staged layout (stab_bytes_lean): pair matrix | rc2 (double) | packed
+// per-pair float4 | F table.  The P table stays in global memory (L1-cached):
+// only output steps read it, and leaving it out keeps the energy/virial
+// kernel (every step of a barostat) at the lean kernel's residency.
 template <bool MIXED, bool EV>
 __device__ void stage_tables(const DevCtx &c, const SysParam *P, unsigned char *sm, TabView &tv) {
   const int nt = P->ntypes, np = P->npairs, T = P->ptsize + 1;
@@ -1461,23 +1463,17 @@ __device__ void stage_tables(const DevCtx &c, const SysParam *P, unsigned char *
   tv.rc2f = c.rc2f + P->pair_off;
   tv.vdr2 = c.vdr2 + P->pair_off;
   if (MIXED) {
-    float2 *dF = (float2 *)(sm + off), *dP = dF + np * T;
-    const float2 *sF = c.tabF2 + P->tab_off, *sP = c.tabP2 + P->tab_off;
-    for (int k = threadIdx.x; k < np * T; k += blockDim.x) {
-      dF[k] = sF[k];
-      if (EV) dP[k] = sP[k];
-    }
+    float2 *dF = (float2 *)(sm + off);
+    const float2 *sF = c.tabF2 + P->tab_off;
+    for (int k = threadIdx.x; k < np * T; k += blockDim.x) dF[k] = sF[k];
     tv.tF2 = dF;
-    tv.tP2 = dP;
+    tv.tP2 = c.tabP2 + P->tab_off;
   } else {
-    double *dF = (double *)(sm + off), *dP = dF + np * T;
-    const double *sF = c.tabF + P->tab_off, *sP = c.tabP + P->tab_off;
-    for (int k = threadIdx.x; k < np * T; k += blockDim.x) {
-      dF[k] = sF[k];
-      if (EV) dP[k] = sP[k];
-    }
+    double *dF = (double *)(sm + off);
+    const double *sF = c.tabF + P->tab_off;
+    for (int k = threadIdx.x; k < np * T; k += blockDim.x) dF[k] = sF[k];
     tv.tF = dF;
-    tv.tP = dP;
+    tv.tP = c.tabP + P->tab_off;
   }
 }
 
@@ -1639,7 +1635,7 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 /
   constexpr int NT = TILE * TPA;
   extern __shared__ __align__(16) unsigned char dsm[];
   // mixed EV: 7 fixed-point slots (energy, virial) per thread, after the tables
-  unsigned long long *evq = (unsigned long long *)(dsm + (STAB ? c.stab_smem : 0));
+  unsigned long long *evq = (unsigned long long *)(dsm + (STAB ? c.stab_lean : 0));
   const int G = gridDim.x;
   // the block's tiles: in a dynamics step its equal share of the planned
   // cost of this launch's systems (runs of consecutive tiles, usually of
@@ -2111,8 +2107,7 @@ template <int TPA, bool MIXED, bool FUSE, bool STAB, bool EV, int GATHER, bool S
 static int pair_launch(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh,
                        bool launch) {
   auto kern = k_pair<TPA, MIXED, FUSE, STAB, EV, GATHER, SPRING>;
-  const int smem = (STAB ? (EV ? c.stab_smem : c.stab_lean) : 0) +
-                   ((MIXED && EV) ? 7 * 8 * TILE * TPA : 0);
+  const int smem = (STAB ? c.stab_lean : 0) + ((MIXED && EV) ? 7 * 8 * TILE * TPA : 0);
   static int cfg_smem = -1, occ = 0;
   if (smem != cfg_smem) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
