@@ -125,6 +125,7 @@ struct ndg_ctx {
   size_t pin_cap = 0;
   int *rb_list = nullptr;  // systems listed for a list rebuild
   PlanEnt *plan = nullptr;  // pair-launch work plan (integrate1's extra block)
+  int *build_ctr = nullptr;  // k_build's tile counter
   int *plan_kb = nullptr;
   PlanHdr *plan_hdr = nullptr;
   double *red = nullptr, *itop = nullptr, *ired = nullptr;
@@ -237,6 +238,7 @@ DevCtx devctx(ndg_ctx *c) {
   d.ring_count = c->ring_count;
   d.rb_list = c->rb_list;
   d.plan = c->plan;
+  d.build_ctr = c->build_ctr;
   d.plan_kb = c->plan_kb;
   d.plan_hdr = c->plan_hdr;
   d.ring_cap = c->ring_cap;
@@ -334,6 +336,7 @@ int grow_sys(ndg_ctx *c, int n) {
   rc |= grow(c, c->plan, 0, 2 * (size_t)n);
   if (!c->plan_kb) rc |= grow(c, c->plan_kb, 0, 2 * (size_t)PLAN_GMAX);
   if (!c->plan_hdr) rc |= grow(c, c->plan_hdr, 0, 1);
+  if (!c->build_ctr) rc |= grow(c, c->build_ctr, 0, 1);
   if (rc) return NDG_ERR_NOMEM;
   drop_graphs(c);
   std::vector<SysParam> z(n - c->nsys_cap);
@@ -931,7 +934,7 @@ ndg_ctx::~ndg_ctx() {
   drop_graphs(this);
   void *ptrs[] = {dP, dS, chunk_sys, cell_sys, pos, s_pos, pfx, vel, acc, disp, force, s_vel,
                   s_acc, gid, s_gid, s_cell, nnb, hold, bcd, ipos, sprd, atom_cell, atom_slot, perm, tmp_src, tmp_key,
-                  cell_count, cell_start, rb_list, plan, plan_kb, plan_hdr, nbr, tile_rows, red, itop, ired, pairmat, pairg, mass, rc2, rlist2,
+                  cell_count, cell_start, rb_list, plan, plan_kb, plan_hdr, build_ctr, nbr, tile_rows, red, itop, ired, pairmat, pairg, mass, rc2, rlist2,
                   vdr2, rc2f, tabF, tabP, tabF2, tabP2, ring, ring_count};
   for (void *p : ptrs)
     if (p) cudaFree(p);

@@ -759,6 +759,7 @@ __device__ void scan_system(const DevCtx &c, int s, int counting) {
 // exclusive scan of the cell counts, one listed system at a time per block
 __global__ __launch_bounds__(1024) void k_scan(DevCtx c, int counting) {
   const int nl = c.ring_count[3];
+  if (blockIdx.x == 0 && threadIdx.x == 0) *c.build_ctr = 0;  // k_build's work counter
   for (int k = blockIdx.x; k < nl; k += gridDim.x) {
     scan_system(c, c.rb_list[k], counting);
     __syncthreads();  // carry and wsum are reused by the next system
@@ -1398,13 +1399,47 @@ __device__ void build_tile(const DevCtx &c, int sys, int tile) {
   }
 }
 
+// A short rebuild list (a step's rebuilds: a few tiles per block) takes its
+// tiles from a work counter, so that blocks that draw cheap tiles take more
+// of them; a long one (a prologue build) is dealt round-robin.
 __global__ __launch_bounds__(NBT, 2) void k_build(DevCtx c) {
-  for_listed(c,
-             [&](int s, int &f, int &n) {
-               f = c.P[s].atom_off / TILE;
-               n = c.P[s].npad / TILE;
-             },
-             [&](int s, int u) { build_tile(c, s, u); });
+  const int n = c.ring_count[3];
+  if (n >= NBT) {  // (thread n writes the total below)
+    for_listed(c,
+               [&](int s, int &f, int &n) {
+                 f = c.P[s].atom_off / TILE;
+                 n = c.P[s].npad / TILE;
+               },
+               [&](int s, int u) { build_tile(c, s, u); });
+    return;
+  }
+  __shared__ int l_sys[NBT], l_first[NBT], l_pre[NBT + 1];
+  __shared__ int wsum[NBT / 32], unit_s;
+  int cnt = 0;
+  if ((int)threadIdx.x < n) {
+    const int s = c.rb_list[threadIdx.x];
+    l_sys[threadIdx.x] = s;
+    l_first[threadIdx.x] = c.P[s].atom_off / TILE;
+    cnt = c.P[s].npad / TILE;
+  }
+  const int pre = block_excl_scan(cnt, wsum);
+  if ((int)threadIdx.x <= n) l_pre[threadIdx.x] = pre;  // l_pre[n]: all tiles
+  __syncthreads();
+  const int total = l_pre[n];
+  for (;;) {
+    if (threadIdx.x == 0) unit_s = atomicAdd(c.build_ctr, 1);
+    __syncthreads();
+    const int u = unit_s;
+    __syncthreads();  // every thread has read the unit before the next draw
+    if (u >= total) break;
+    int lo = 0, hi = n - 1;  // the entry whose tiles hold unit u
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (l_pre[mid] <= u) lo = mid;
+      else hi = mid - 1;
+    }
+    build_tile(c, l_sys[lo], l_first[lo] + (u - l_pre[lo]));
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -62,6 +62,7 @@ struct DevCtx {
   int *ring_count;  // [0] records written, [1] error bits of any system,
                     // [2] largest tile candidate count, [3] systems on rb_list
   int *rb_list;     // systems whose lists the next rebuild group rebuilds
+  int *build_ctr;   // k_build's tile counter (reset by k_scan)
   PlanEnt *plan;    // 2 x nsys_cap entries
   int *plan_kb;     // 2 x PLAN_GMAX block starts
   PlanHdr *plan_hdr;
