@@ -354,6 +354,36 @@ def test_batch_equals_alone(specs):
                 assert np.array_equal(a, b), n
 
 
+def test_many_systems_round_robin_build():
+    """300 systems in one context: the prologue build deals their tiles
+    round-robin (a list of 256 or more systems), a step's few rebuilds take
+    them from the build's work counter; either way each system's lists and
+    trajectory are the same bits as alone."""
+    rng = np.random.default_rng(40)
+    many = [W.cu_crystal(5, float(T), seed=int(100 + k), quirk="fixed")
+            for k, T in enumerate(rng.uniform(300.0, 1500.0, 300))]
+    sample = [0, 137, 299]
+    alone = {}
+    for k in sample:
+        with nd.Context(0, "mixed") as ctx:
+            sid = gpu_from_spec(ctx, many[k])
+            ctx.setup_lists()
+            nb = pair_multiset(ctx.neighbors(sid))
+            ctx.run(40)
+            alone[k] = (nb, ctx.state(sid), ctx.list_updates(sid))
+    with nd.Context(0, "mixed") as ctx:
+        ids = [gpu_from_spec(ctx, sp) for sp in many]
+        ctx.setup_lists()
+        for k in sample:
+            assert np.array_equal(pair_multiset(ctx.neighbors(ids[k])), alone[k][0])
+        ctx.run(40)
+        for k in sample:
+            for a, b in zip(ctx.state(ids[k]), alone[k][1]):
+                assert np.array_equal(a, b), k
+            assert ctx.list_updates(ids[k]) == alone[k][2]
+        assert sum(ctx.list_updates(i) for i in ids) > 0  # some steps rebuilt
+
+
 def test_deterministic_repeat(specs):
     out = []
     for _ in range(2):
