@@ -307,6 +307,10 @@ typedef struct ndg_request {
   const double *box;
   ndg_control control; /* dt, skin, ensembles, OutSteps, quirk, ... */
   int nsteps;          /* steps of the run (one Run directive) */
+  /* spring pairs as ndg_set_springs takes them, or NULL: none (the run's
+   * prologue takes the positions it starts from as the initial ones) */
+  const int *spring;
+  const double *pair_params;
 } ndg_request;
 
 typedef struct ndg_server_stats {

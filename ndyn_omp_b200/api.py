@@ -368,7 +368,8 @@ class Request(ctypes.Structure):
                 ("rcpair", ctypes.c_void_p), ("ppair", ctypes.c_void_p),
                 ("fpair", ctypes.c_void_p), ("typ", ctypes.c_void_p), ("pos", ctypes.c_void_p),
                 ("vel", ctypes.c_void_p), ("box", ctypes.c_void_p), ("control", Control),
-                ("nsteps", ctypes.c_int)]
+                ("nsteps", ctypes.c_int), ("spring", ctypes.c_void_p),
+                ("pair_params", ctypes.c_void_p)]
 
 
 class ServerStats(ctypes.Structure):
@@ -450,10 +451,17 @@ class Server:
         pos = np.ascontiguousarray(pos, np.float64).reshape(-1)
         vel = None if vel is None else np.ascontiguousarray(vel, np.float64).reshape(-1)
         box = np.ascontiguousarray(box, np.float64)
+        spring = prm = None
+        if any(p[3] == "spring" for p in pairs):
+            spring = np.array([1 if p[3] == "spring" else 0 for p in pairs], np.int32)
+            prm = np.zeros((len(pairs), 4))
+            for k, p in enumerate(pairs):
+                prm[k, :len(p[4])] = p[4][:4]
         r = Request(np=len(typ), ntypes=nt, npairs=len(pairs), ptsize=int(ptsize),
                     ptrmin=float(ptrmin), mass=_p(masses), pairmat=_p(pm), rcpair=_p(rcp),
                     ppair=_p(pp), fpair=_p(fp), typ=_p(typ), pos=_p(pos), vel=_p(vel),
-                    box=_p(box), control=make_control(**control), nsteps=int(nsteps))
+                    box=_p(box), control=make_control(**control), nsteps=int(nsteps),
+                    spring=_p(spring), pair_params=_p(prm))
         t = ctypes.c_longlong()
         _ok(self.L.ndg_server_submit(self._s, ctypes.byref(r), ctypes.byref(t)), "server_submit")
         # write_thermo rows: every OutSteps-th step and the run's first

@@ -37,6 +37,8 @@ struct Request {
   double ptrmin = 0.25;
   std::vector<double> mass, rcpair, ppair, fpair, pos, vel;
   std::vector<int> pairmat, typ;
+  std::vector<int> spring;         // spring pairs (empty: none)
+  std::vector<double> pair_params;  // their PairParams, 4 per pair
   double box[3] = {0, 0, 0};
   ndg_control ctl{};
   int nsteps = 0, left = 0;
@@ -199,6 +201,11 @@ int ndg_server_submit(ndg_server *s, const ndg_request *q, long long *ticket) {
   r.typ.assign(q->typ, q->typ + q->np);
   r.pos.assign(q->pos, q->pos + 3 * (size_t)q->np);
   if (q->vel) r.vel.assign(q->vel, q->vel + 3 * (size_t)q->np);
+  if (q->spring) {
+    if (!q->pair_params) return NDG_ERR_ARG;
+    r.spring.assign(q->spring, q->spring + q->npairs);
+    r.pair_params.assign(q->pair_params, q->pair_params + 4 * (size_t)q->npairs);
+  }
   for (int d = 0; d < 3; ++d) r.box[d] = q->box[d];
   r.ctl = q->control;
   r.nsteps = r.left = q->nsteps;
@@ -243,6 +250,8 @@ int ndg_server_step(ndg_server *s, int *completed) {
                             r.typ.data(), r.pos.data(), r.vel.empty() ? nullptr : r.vel.data(),
                             nullptr, r.box, &sys);
     if (!rc) rc = ndg_set_control(s->ctx, sys, &r.ctl);
+    if (!rc && !r.spring.empty())
+      rc = ndg_set_springs(s->ctx, sys, r.spring.data(), r.pair_params.data());
     if (rc) {
       if (sys >= 0) ndg_remove_system(s->ctx, sys);
       r.status = rc;

@@ -89,6 +89,27 @@ def test_serving_result_same_alone_and_in_mix():
 
 
 @pytest.mark.gpu
+def test_serving_springs_same_alone_and_in_mix():
+    """A served run with spring pairs (the context switches to the spring
+    variant of the pair kernels for every resident run) gives the same bits
+    alone and beside runs without springs, and so do they."""
+    spr = W.spring_alloy(6, 500.0, seed=45, quirk="fixed")  # 864 atoms, compute2
+    spr["control"] = dict(spr["control"], out_steps=20)
+    reqs = _requests()[:2] + [(spr, 120)]
+    alone = [_alone_run(s, n) for s, n in reqs]
+    with nd.Server(0, "mixed", hbm_budget=8e9, block_steps=40) as srv:
+        t = [W.submit_to_server(srv, s, n) for s, n in reqs]
+        for _ in range(40):
+            srv.step()
+            if all(srv.status(x) == 2 for x in t):
+                break
+        assert all(srv.status(x) == 2 for x in t)
+        for k, x in enumerate(t):
+            pos, vel, acc, box, rows = srv.result(x)
+            _same(((pos, vel, acc, box), rows), alone[k])
+
+
+@pytest.mark.gpu
 def test_serving_admission_waits_for_budget():
     """With room for one run at a time the second is admitted only when the
     first retires; both results equal the runs alone."""
