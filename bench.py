@@ -184,7 +184,7 @@ def cpu_rate(spec, target_s, threads=None, fixed_steps=None):
         t0 = time.perf_counter()
         rc, _ = o.run(1, dt, loop_only=True)
         t1 = time.perf_counter() - t0
-        steps = int(max(2, min(200, target_s / max(t1, 1e-6))))
+        steps = int(max(2, min(1000000, target_s / max(t1, 1e-6))))
     else:
         steps = fixed_steps
     t0 = time.perf_counter()
@@ -193,6 +193,38 @@ def cpu_rate(spec, target_s, threads=None, fixed_steps=None):
     assert rc == 0, rc
     n = len(spec["typ"])
     return n * steps / el, steps, el, threads
+
+
+def spread_sample(specs, atom_budget):
+    """Systems spread evenly over the list (sizes and materials as they
+    come), as many as the atom budget allows (at least one)."""
+    n = len(specs)
+    for k in range(n, 0, -1):
+        pick = [specs[(j * n) // k] for j in range(k)]
+        if sum(len(s["typ"]) for s in pick) <= atom_budget or k == 1:
+            return pick, [(j * n) // k for j in range(k)]
+    return specs[:1], [0]
+
+
+def cpu_rate_systems(specs, steps, warmup, threads):
+    """The oracle on each system in turn (the reference runs one system at
+    a time): warm-up and timed steps per system; returns (atom-steps/s,
+    seconds of timed work)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import oracle_from_spec
+    work = el = 0.0
+    for sp in specs:
+        o = oracle_from_spec(sp, threads=threads)
+        assert o.setup_lists() == 0
+        dt = sp["control"]["dt"]
+        if warmup:
+            o.run(warmup, dt, loop_only=True)
+        t0 = time.perf_counter()
+        rc, _ = o.run(steps, dt, loop_only=True)
+        el += time.perf_counter() - t0
+        assert rc == 0, rc
+        work += len(sp["typ"]) * steps
+    return work / el, el
 
 
 def n_atoms(specs):
@@ -311,10 +343,27 @@ def run_reference(args, ws, rank):
         n = int(min(64, max(6, round((want_atoms / 8) ** (1 / 3)))))
         sample = workload("c3", (n, n, n))[0][0]
         sample_txt = f"{len(sample['typ'])} atoms ({n}^3 rocksalt cells)"
-    elif args.config == "c4":
-        # c4: replicas run one after another (the plain path in sequence)
-        sample = specs[1]
-        sample_txt = f"replica 1 of 512 ({len(sample['typ'])} atoms)"
+    elif args.config in ("c4", "c5batch"):
+        # the systems run one after another (the reference runs one system at
+        # a time): a spread of them, as many as fit the budget at K+W steps
+        r, _, _, _ = cpu_rate(specs[1], 1.0, threads)
+        pick, idx = spread_sample(specs, r * budget / max(args.steps + args.warmup, 1))
+        v, el = cpu_rate_systems(pick, args.steps, args.warmup, threads)
+        sample_txt = (f"{len(pick)} of {len(specs)} systems spread evenly over the list "
+                      f"({n_atoms(pick)} atoms), one after another")
+        line = {
+            "impl": "reference", "metric": "atom-steps/s", "value": v, "unit": "atom-steps/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD_TEXT[args.config], "sample": sample_txt},
+            "cpu_baseline": {"value": v, "unit": "atom-steps/s", "cores": threads, "kind": "port",
+                             "sample": sample_txt + f", {args.steps} steps each"},
+            "e2e": {"value": v, "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+        return
     else:
         # c5: the stream's first request system
         from ndyn_omp_b200 import workloads as W
@@ -568,13 +617,24 @@ def main():
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        sample = specs[0] if args.config != "c4" else specs[1]
-        if args.config == "c3":
-            sample = workload("c3", (24, 24, 24))[0][0]
-        r, st, el, th = cpu_rate(sample, 15.0)
-        cpu = {"value": r, "unit": "atom-steps/s", "cores": th, "kind": "port",
-               "sample": f"{len(sample['typ'])} atoms x {st} steps ({el:.1f} s), "
-                         f"oracle restatement of the reference OpenMP FP64 loop"}
+        if batch:
+            # the systems one after another, as the reference runs them: a
+            # spread of them sized for ~15 s at 100 steps each
+            r0, _, _, th = cpu_rate(specs[1], 1.0)
+            pick, _ = spread_sample(specs, r0 * 15.0 / 100)
+            r, el = cpu_rate_systems(pick, 100, 10, th)
+            cpu = {"value": r, "unit": "atom-steps/s", "cores": th, "kind": "port",
+                   "sample": f"{len(pick)} of {len(specs)} systems spread over the list "
+                             f"({n_atoms(pick)} atoms) x 100 steps each ({el:.1f} s), one after "
+                             f"another; oracle restatement of the reference OpenMP FP64 loop"}
+        else:
+            sample = specs[0]
+            if args.config == "c3":
+                sample = workload("c3", (24, 24, 24))[0][0]
+            r, st, el, th = cpu_rate(sample, 15.0)
+            cpu = {"value": r, "unit": "atom-steps/s", "cores": th, "kind": "port",
+                   "sample": f"{len(sample['typ'])} atoms x {st} steps ({el:.1f} s), "
+                             f"oracle restatement of the reference OpenMP FP64 loop"}
 
     touched = N * (4.0 * 2 * (nb_half or 40) + 200.0)
     line = {
