@@ -870,8 +870,8 @@ __global__ __launch_bounds__(BLOCK) void k_copyback(DevCtx c, int mixed) {
 //      margin take the reference's exact FP64 test, so membership is
 //      bit-identical to buildVerletList (src/nd.f90:1356-1383 for the cell
 //      itself, :1403-1426 for the neighbour cells).
-//   3. Hits are compacted with __ballot_sync/__popc into 16-bit tile-local
-//      candidate indices and written to the blocked list row by row.
+//   3. Hits are compacted with __ballot_sync/__popc straight into the own
+//      atom's column of the blocked list (atom slots).
 // A tile whose cells or candidates do not fit the shared buffers takes
 // build_tile_direct (same test, same list order, no staging).
 constexpr int TC_MAX = 256;    // link cells a tile may stage
