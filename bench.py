@@ -588,32 +588,32 @@ def main():
                 "pair_ms": prof["pair_ms"], "integrate_ms": prof["integrate_ms"],
                 "rebuild_ms_per_step": prof["rebuild_ms"]}
 
-    # end to end through the C ABI with host buffers: load state, run, read
-    # state back (what a caller of ndg_load_state/ndg_run/ndg_get_state pays)
-    # end to end through the C ABI with host buffers: load every system's
-    # state from pinned host memory, run K steps (prologue list build
-    # included), read every state back
-    host = []
-    for i in ids:
-        pos0, vel0, acc0, box0 = ctx.state(i)
-        host.append([torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
-                     for a in (pos0, vel0, acc0)] + [box0])
+    # end to end through the C ABI with host buffers: every system's state
+    # loaded from pinned host memory in one call (ndg_load_state, sys = -1),
+    # K steps (the prologue list build included), every state read back into
+    # pinned host memory in one call (ndg_get_state, sys = -1)
+    p0, v0, a0, b0 = ctx.states()
+
+    def pinned(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+
+    hp, hv, ha = pinned(p0), pinned(v0), pinned(a0)
+    out = (pinned(np.zeros_like(p0)), pinned(np.zeros_like(v0)), pinned(np.zeros_like(a0)),
+           np.zeros_like(b0))
     barrier(ws)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for i, hs in zip(ids, host):
-        ctx.load_state(i, hs[0], hs[1], hs[2], hs[3])
+    ctx.load_states(hp, hv, ha, b0)
     rows = ctx.run(args.steps)
-    for i in ids:
-        ctx.state(i)
+    ctx.states(out=out)
     torch.cuda.synchronize()
     el = allmax(time.perf_counter() - t0, ws)
-    h2d = N * (32 + 24 * 3 + 4)            # pos(+type) double4, vel, acc, disp, gid
-    d2h = N * (36 + 4 + 32 + 24 * 2) + 120 * len(rows)  # types for load, gid, pos, vel, acc, thermo
+    h2d = N * 3 * 8 * 3 + b0.size * 8                 # pos, vel, acc (3,np) each, boxes
+    d2h = N * 3 * 8 * 3 + b0.size * 8 + 120 * len(rows)  # the same back, thermo records
     e2e = {"value": N * args.steps * ws / el, "unit": "atom-steps/s",
            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
-           "what": "ndg_load_state + ndg_run(K) (incl. list build) + ndg_get_state, "
-                   "every system"}
+           "what": "ndg_load_state(all systems) + ndg_run(K) (incl. list build) + "
+                   "ndg_get_state(all systems), host buffers page-locked"}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:

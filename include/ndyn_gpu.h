@@ -141,7 +141,13 @@ int ndg_add_system(ndg_ctx *ctx, int np, int ntypes, int npairs, int ptsize,
 int ndg_remove_system(ndg_ctx *ctx, int sys);
 int ndg_num_systems(const ndg_ctx *ctx);
 
-/* replace positions/velocities/accelerations/box of a system */
+/* replace (load) or read (get) positions/velocities/accelerations/box of a
+ * system; vel/acc/box may be NULL (load: zero velocities/accelerations, box
+ * kept).  sys = -1 moves every live system at once: the arrays hold the
+ * systems one after another in ascending id order (3*np doubles each, in
+ * the reference's layout) and box holds 3 doubles per system.  That form
+ * copies each array in one transfer, straight from or into the caller's
+ * buffers (page-locked ones move by DMA), and waits once for all systems. */
 int ndg_load_state(ndg_ctx *ctx, int sys, const double *pos, const double *vel,
                    const double *acc, const double *box);
 int ndg_get_state(ndg_ctx *ctx, int sys, double *pos, double *vel, double *acc,
@@ -228,18 +234,22 @@ int ndg_get_neighbor_count(ndg_ctx *ctx, int sys, long long *entries);
  *
  * The same forces, potential energy and virial as ndg_compute (compute0,
  * FP64) for one system, for callers that cannot allocate device memory:
- * code that launches work while a CUDA stream is being captured into a
- * graph (cudaMalloc is not allowed there), host applications that hand all
- * of a GPU's memory to their own pool and only lend out buffers, and
- * latency-bound loops that must not stall on the driver's allocator.
+ * host applications that hand all of a GPU's memory to their own pool (a
+ * framework's caching allocator, a Fortran code that sizes everything at
+ * start-up) and only lend out buffers, so that a cudaMalloc of ours would
+ * fail or fragment their pool; and loops that must not stall on
+ * cudaMalloc/cudaFree, which can synchronise the whole device.
  *
  * The caller owns every buffer: pos_d (3*np, fractional, reference layout),
  * typ_d (np), the tables fpair_d/ppair_d ((ptsize+1)*npairs, column-major)
  * and the output force_d (3*np) are device pointers; pairmat (ntypes^2,
  * column-major), rcpair (npairs) and box (3) are host arrays; skin and quirk
- * select the link-cell grid as ndg_setup_lists does (skin >= 0).  potential
- * and virial (6) are written on the host; the call returns when they are.
- * stream is a cudaStream_t (NULL: the legacy default stream).
+ * select the link-cell grid as ndg_setup_lists does (skin >= 0,
+ * rcut + skin > 0).  Every typ_d entry must lie in 1..ntypes: an atom of
+ * another type is left out of the sums and the call returns NDG_ERR_ARG.
+ * potential and virial (6) are written on the host: the call waits for its
+ * stream (cudaStreamSynchronize) and returns when they are.  stream is a
+ * cudaStream_t (NULL: the legacy default stream).
  *
  * Scratch lives in one static device array of about 0.8 MB that every GPU
  * loading the library keeps until the process exits.  Limits: 32768 atoms,

@@ -228,6 +228,31 @@ class Context:
         _ok(self.L.ndg_get_state(self._c, sys, _p(pos), _p(vel), _p(acc), _p(box)), "get_state")
         return pos.reshape(n, 3), vel.reshape(n, 3), acc.reshape(n, 3), box
 
+    def load_states(self, pos, vel=None, acc=None, boxes=None):
+        """Every live system at once (ndg_load_state with sys = -1): pos,
+        vel, acc are (sum of np, 3) arrays holding the systems one after
+        another in ascending id order, boxes (nsys, 3).  Page-locked arrays
+        (e.g. from torch's pin_memory) move by DMA."""
+        pos = np.ascontiguousarray(pos, np.float64).reshape(-1)
+        vel = None if vel is None else np.ascontiguousarray(vel, np.float64).reshape(-1)
+        acc = None if acc is None else np.ascontiguousarray(acc, np.float64).reshape(-1)
+        boxes = None if boxes is None else np.ascontiguousarray(boxes, np.float64).reshape(-1)
+        _ok(self.L.ndg_load_state(self._c, -1, _p(pos), _p(vel), _p(acc), _p(boxes)),
+            "load_state(all)")
+
+    def states(self, out=None):
+        """Every live system's (pos, vel, acc) as (sum of np, 3) arrays in
+        ascending id order, and boxes (nsys, 3) (ndg_get_state with sys = -1).
+        out = (pos, vel, acc, boxes) writes into the caller's arrays."""
+        total = sum(self.systems.values())
+        if out is None:
+            out = (np.zeros((total, 3)), np.zeros((total, 3)), np.zeros((total, 3)),
+                   np.zeros((len(self.systems), 3)))
+        pos, vel, acc, boxes = out
+        _ok(self.L.ndg_get_state(self._c, -1, _p(pos), _p(vel), _p(acc), _p(boxes)),
+            "get_state(all)")
+        return pos, vel, acc, boxes
+
     def forces(self, sys=0):
         n = self.systems[sys]
         f = np.zeros(3 * n)

@@ -123,6 +123,9 @@ struct ndg_ctx {
   int *tile_rows = nullptr;
   char *pin = nullptr;  // pinned host staging of atom copies (reused)
   size_t pin_cap = 0;
+  int *pin_words = nullptr;  // pinned copy of the status words (ring_count[0..1])
+  long long *xoff = nullptr;  // bulk state transfer: each system's first atom in the
+  size_t cap_xoff = 0;        // caller's concatenated arrays (-1: not a live system)
   int *rb_list = nullptr;  // systems listed for a list rebuild
   PlanEnt *plan = nullptr;  // pair-launch work plan (integrate1's extra block)
   int *build_ctr = nullptr;  // k_build's tile counter
@@ -508,6 +511,17 @@ int upload_params(ndg_ctx *c) {
 // needs them, so that adding many systems stays linear in their number
 int ensure_params(ndg_ctx *c) { return c->params_dirty ? upload_params(c) : NDG_OK; }
 
+// the per-system records alone, when only ranges, grids or list capacities
+// changed (their table offsets are those of the last full upload)
+int upload_sysparams(ndg_ctx *c) {
+  std::vector<SysParam> prm(c->nsys_cap);
+  memset(prm.data(), 0, prm.size() * sizeof(SysParam));
+  for (size_t s = 0; s < c->sys.size(); ++s)
+    if (c->sys[s].alive) prm[s] = c->sys[s].prm;
+  CK(c, cudaMemcpy(c->dP, prm.data(), prm.size() * sizeof(SysParam), cudaMemcpyHostToDevice));
+  return NDG_OK;
+}
+
 void fill_control_params(HostSys &h) {
   SysParam &p = h.prm;
   const ndg_control &q = h.ctl;
@@ -675,6 +689,11 @@ int init_positions(ndg_ctx *c, int s, const double *ipos, const double *ibox) {
 }
 
 int setup_lists(ndg_ctx *c, const std::vector<int> &which) {
+  // every system's state record read and written once (not one round trip
+  // per system), and the cell owners uploaded once
+  std::vector<SysState> Sall(c->nsys_cap);
+  CK(c, cudaMemcpy(Sall.data(), c->dS, Sall.size() * sizeof(SysState), cudaMemcpyDeviceToHost));
+  bool cells_moved = false;
   for (int s : which) {
     HostSys &h = c->sys[s];
     if (!h.alive) continue;
@@ -685,9 +704,8 @@ int setup_lists(ndg_ctx *c, const std::vector<int> &which) {
     }
     if (h.ctl.skin < 0) h.ctl.skin = 0.2 * h.rcut;  // persists, as in the reference
     fill_control_params(h);
-    SysState S;
-    int rc = get_state_dev(c, (int)s, S);
-    if (rc) return rc;
+    SysState &S = Sall[s];
+    int rc = 0;
     int nc = 1;
     for (int d = 0; d < 3; ++d) {
       h.mcell0[d] = (int)(S.box[d] / (h.rcut + h.prm.skin));
@@ -733,8 +751,7 @@ int setup_lists(ndg_ctx *c, const std::vector<int> &which) {
       h.cells.len = nc + 1;
       h.ncell_cap = nc + 1;
       for (long long q = off; q < off + nc; ++q) c->cell_sys_h[q] = (int)s;
-      CK(c, cudaMemcpy(c->cell_sys, c->cell_sys_h.data(), c->cells.cap * sizeof(int),
-                       cudaMemcpyHostToDevice));
+      cells_moved = true;
     }
     h.prm.atom_off = (int)(h.atoms.off * ATOM_ALIGN);
     h.prm.n = h.n;
@@ -748,10 +765,14 @@ int setup_lists(ndg_ctx *c, const std::vector<int> &which) {
     S.err = 0;
     S.pend = 0;
     for (int d = 0; d < 3; ++d) S.box_build[d] = S.box[d];
-    rc = put_state_dev(c, (int)s, S);
-    if (rc) return rc;
   }
-  int rc = upload_params(c);
+  if (cells_moved)
+    CK(c, cudaMemcpy(c->cell_sys, c->cell_sys_h.data(), c->cells.cap * sizeof(int),
+                     cudaMemcpyHostToDevice));
+  CK(c, cudaMemcpy(c->dS, Sall.data(), Sall.size() * sizeof(SysState), cudaMemcpyHostToDevice));
+  // the prologue changes only the systems' ranges and grids: the tables go
+  // up again only when something else changed them
+  int rc = c->params_dirty ? upload_params(c) : upload_sysparams(c);
   if (rc) return rc;
   CK(c, cudaMemset(c->ring_count, 0, 4 * sizeof(int)));
   rc = list_systems(c, which);
@@ -806,8 +827,11 @@ void enqueue_steps(ndg_ctx *c, int nsteps) {
 }
 
 int check_words(ndg_ctx *c, int *count) {
-  int words[2];
-  CK(c, cudaMemcpyAsync(words, c->ring_count, sizeof(words), cudaMemcpyDeviceToHost, c->st));
+  // read through pinned memory: a copy into pageable memory goes through
+  // the driver's staging and wakes the host late
+  int local[2];
+  int *words = c->pin_words ? c->pin_words : local;
+  CK(c, cudaMemcpyAsync(words, c->ring_count, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->st));
   CK(c, cudaStreamSynchronize(c->st));
   *count = words[0];
   if (words[1] & E_NEIMAX) return NDG_ERR_NEIMAX;
@@ -881,7 +905,7 @@ int capture_block(ndg_ctx *c, int g, cudaGraphExec_t *out) {
 // Run nsteps as blocks of up to graph_steps: each block's head gives every
 // armed system its share of the block (k_begin_block), then the block runs
 // as one captured graph (or as eager launches when graph_steps is 1).
-int run_blocks(ndg_ctx *c, int nsteps, ndg_thermo_cb cb, void *user) {
+int run_blocks(ndg_ctx *c, int nsteps, ndg_thermo_cb cb, void *user, bool flush_end = false) {
   int left = nsteps;
   while (left > 0) {
     const int g = std::min(left, std::max(c->graph_steps, 1));
@@ -904,6 +928,12 @@ int run_blocks(ndg_ctx *c, int nsteps, ndg_thermo_cb cb, void *user) {
     } else {
       enqueue_steps(c, g);
       CK(c, cudaGetLastError());
+    }
+    if (flush_end && left == g) {
+      // the run's last block: its pending velocity scales are applied in
+      // the same stream batch, so one host wait covers both
+      DevCtx d = devctx(c);
+      launch_flush(d, c->st, c->nsys_cap, -1);
     }
     int count = 0;
     int rc = check_words(c, &count);
@@ -939,6 +969,8 @@ ndg_ctx::~ndg_ctx() {
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (pin) cudaFreeHost(pin);
+  if (pin_words) cudaFreeHost(pin_words);
+  if (xoff) cudaFree(xoff);
   if (st) cudaStreamDestroy(st);
   if (st2) cudaStreamDestroy(st2);
 }
@@ -1064,6 +1096,10 @@ int ndg_create(ndg_ctx **out, int device, int precision) {
     return NDG_ERR_NOMEM;
   }
   cudaMemset(c->ring_count, 0, 4 * sizeof(int));
+  if (cudaHostAlloc((void **)&c->pin_words, 4 * sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    c->pin_words = nullptr;  // check_words falls back to a pageable copy
+  }
   int rc = grow_sys(c, 4);
   if (!rc) rc = grow_atoms(c, 16);
   if (!rc) rc = grow_cells(c, 1024);
@@ -1279,8 +1315,122 @@ int ndg_set_initial_positions(ndg_ctx *c, int s, const double *ipos, const doubl
   return init_positions(c, s, ipos, ibox);
 }
 
+// ---------------------------------------------------------------------------
+// Bulk state transfer (sys = -1): every live system at once, the caller's
+// arrays holding them one after another in ascending id order.  The host
+// data moves in one copy per array (straight from the caller's buffers, so
+// pinned ones go by DMA) through the rebuild's scratch arrays, and one
+// kernel puts each atom in place; the boxes move with one copy of the state
+// records.  One host wait per call, however many systems.
+
+// each live system's first atom in the concatenated arrays, on the device;
+// *total = all atoms, *nlive = live systems
+static int xfer_offsets(ndg_ctx *c, long long *total, int *nlive) {
+  std::vector<long long> xo(std::max(c->nsys_cap, 1), -1);
+  long long t = 0;
+  int m = 0;
+  for (size_t s = 0; s < c->sys.size(); ++s)
+    if (c->sys[s].alive) {
+      xo[s] = t;
+      t += c->sys[s].n;
+      ++m;
+    }
+  if (!c->xoff || c->cap_xoff < xo.size()) {
+    if (c->xoff) cudaFree(c->xoff);
+    c->xoff = dalloc<long long>(xo.size());
+    c->cap_xoff = c->xoff ? xo.size() : 0;
+    if (!c->xoff) return NDG_ERR_NOMEM;
+  }
+  CK(c, cudaMemcpyAsync(c->xoff, xo.data(), xo.size() * sizeof(long long),
+                        cudaMemcpyHostToDevice, c->st));
+  CK(c, cudaStreamSynchronize(c->st));  // xo is a local
+  *total = t;
+  *nlive = m;
+  return NDG_OK;
+}
+
+static int load_all(ndg_ctx *c, const double *pos, const double *vel, const double *acc,
+                    const double *box) {
+  int rc = ensure_params(c);
+  if (rc) return rc;
+  long long t = 0;
+  int m = 0;
+  rc = xfer_offsets(c, &t, &m);
+  if (rc || m == 0) return rc;
+  const size_t b3 = 3 * (size_t)t * sizeof(double);
+  cudaStream_t st = c->st;
+  double *xp = (double *)c->s_pos, *xv = vel ? c->s_vel : nullptr, *xa = acc ? c->s_acc : nullptr;
+  CK(c, cudaMemcpyAsync(xp, pos, b3, cudaMemcpyHostToDevice, st));
+  if (vel) CK(c, cudaMemcpyAsync(xv, vel, b3, cudaMemcpyHostToDevice, st));
+  if (acc) CK(c, cudaMemcpyAsync(xa, acc, b3, cudaMemcpyHostToDevice, st));
+  DevCtx d = devctx(c);
+  launch_load_all(d, st, c->xoff, xp, xv, xa);
+  CK(c, cudaGetLastError());
+  if (box) {
+    std::vector<SysState> S(c->nsys_cap);
+    CK(c, cudaMemcpyAsync(S.data(), c->dS, S.size() * sizeof(SysState), cudaMemcpyDeviceToHost,
+                          st));
+    CK(c, cudaStreamSynchronize(st));
+    int k = 0;
+    for (size_t s = 0; s < c->sys.size(); ++s)
+      if (c->sys[s].alive) {
+        for (int q = 0; q < 3; ++q) {
+          S[s].box[q] = box[3 * k + q];
+          S[s].li[q] = 1.0 / box[3 * k + q];
+        }
+        ++k;
+      }
+    CK(c, cudaMemcpyAsync(c->dS, S.data(), S.size() * sizeof(SysState), cudaMemcpyHostToDevice,
+                          st));
+    CK(c, cudaStreamSynchronize(st));  // S is a local
+  }
+  if (c->precision == NDG_PREC_MIXED) launch_refresh_pfx(d, st);
+  CK(c, cudaGetLastError());
+  CK(c, cudaStreamSynchronize(st));
+  for (auto &h : c->sys)
+    if (h.alive) h.lists_valid = false;
+  return NDG_OK;
+}
+
+static int get_all(ndg_ctx *c, double *pos, double *vel, double *acc, double *box) {
+  int rc = ensure_params(c);
+  if (rc) return rc;
+  long long t = 0;
+  int m = 0;
+  rc = xfer_offsets(c, &t, &m);
+  if (rc || m == 0) return rc;
+  const size_t b3 = 3 * (size_t)t * sizeof(double);
+  cudaStream_t st = c->st;
+  double *xp = pos ? (double *)c->s_pos : nullptr, *xv = vel ? c->s_vel : nullptr,
+         *xa = acc ? c->s_acc : nullptr;
+  DevCtx d = devctx(c);
+  launch_store_all(d, st, c->xoff, xp, xv, xa);
+  CK(c, cudaGetLastError());
+  if (pos) CK(c, cudaMemcpyAsync(pos, xp, b3, cudaMemcpyDeviceToHost, st));
+  if (vel) CK(c, cudaMemcpyAsync(vel, xv, b3, cudaMemcpyDeviceToHost, st));
+  if (acc) CK(c, cudaMemcpyAsync(acc, xa, b3, cudaMemcpyDeviceToHost, st));
+  std::vector<SysState> S(box ? c->nsys_cap : 0);
+  if (box)
+    CK(c, cudaMemcpyAsync(S.data(), c->dS, S.size() * sizeof(SysState), cudaMemcpyDeviceToHost,
+                          st));
+  CK(c, cudaStreamSynchronize(st));
+  if (box) {
+    int k = 0;
+    for (size_t s = 0; s < c->sys.size(); ++s)
+      if (c->sys[s].alive) {
+        for (int q = 0; q < 3; ++q) box[3 * k + q] = S[s].box[q];
+        ++k;
+      }
+  }
+  return NDG_OK;
+}
+
 int ndg_load_state(ndg_ctx *c, int s, const double *pos, const double *vel, const double *acc,
                    const double *box) {
+  if (c && s == -1 && pos) {
+    cudaSetDevice(c->device);
+    return load_all(c, pos, vel, acc, box);
+  }
   if (!valid_sys(c, s) || !pos) return NDG_ERR_ARG;
   cudaSetDevice(c->device);
   int rc = ensure_params(c);
@@ -1307,6 +1457,10 @@ int ndg_load_state(ndg_ctx *c, int s, const double *pos, const double *vel, cons
 }
 
 int ndg_get_state(ndg_ctx *c, int s, double *pos, double *vel, double *acc, double *box) {
+  if (c && s == -1) {
+    cudaSetDevice(c->device);
+    return get_all(c, pos, vel, acc, box);
+  }
   if (!valid_sys(c, s)) return NDG_ERR_ARG;
   cudaSetDevice(c->device);
   HostSys &h = c->sys[s];
@@ -1564,18 +1718,24 @@ static int run_impl(ndg_ctx *c, int nsteps, ndg_thermo_cb cb, void *user, int co
     if (rc) return rc;
     cont = 0;
   }
-  // controls may have changed between runs
+  // controls may have changed between runs; the parameters go up again only
+  // when some system's did (an upload re-packs every system's tables, about
+  // 10 ms for 512 systems, which a short run would otherwise pay each time)
   for (auto &h : c->sys)
-    if (h.alive) fill_control_params(h);
-  rc = upload_params(c);
+    if (h.alive) {
+      const SysParam before = h.prm;
+      fill_control_params(h);
+      if (memcmp(&before, &h.prm, sizeof(SysParam)) != 0) c->params_dirty = true;
+    }
+  rc = ensure_params(c);
   if (rc) return rc;
   CK(c, cudaMemset(c->ring_count, 0, 4 * sizeof(int)));
   DevCtx d = devctx(c);
   launch_arm(d, c->st, c->nsys_cap, -1, nsteps, cont ? START_NEW : START_BUILT);
   CK(c, cudaGetLastError());
-  rc = run_blocks(c, nsteps, cb, user);
-  int rf = flush_pending(c);
-  return rc ? rc : rf;
+  rc = run_blocks(c, nsteps, cb, user, true);
+  if (rc) flush_pending(c);  // a failed block left the last flush unlaunched
+  return rc;
 }
 
 int ndg_run(ndg_ctx *c, int nsteps, ndg_thermo_cb cb, void *user) {

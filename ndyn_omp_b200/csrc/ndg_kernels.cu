@@ -2112,6 +2112,89 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 /
 }
 
 // ---------------------------------------------------------------------------
+// Bulk state transfer of every system at once (ndg_load_state and
+// ndg_get_state with sys = -1).  The caller's arrays hold the systems one
+// after another in id order, unpadded, each in the reference's (3,np) input
+// order; xoff[s] is system s's first atom there (-1: not transferred).  The
+// device staging blocks xp, xv, xa have the same (3,total) layout.
+
+// the type word of every atom by input index (tw[atom_off + gid]), read
+// before a load replaces the layout
+__global__ __launch_bounds__(BLOCK) void k_type_words(DevCtx c, int *tw) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  const int sys = c.chunk_sys[i / ATOM_ALIGN];
+  if (sys < 0) return;
+  const SysParam &P = c.P[sys];
+  if (i - P.atom_off >= P.n) return;
+  const int g = c.gid[i];
+  if (g < 0 || g >= P.n) return;
+  tw[P.atom_off + g] = tw_of(c.pos[i].w);
+}
+
+// load: slot atom_off + l takes input atom l (identity order, as a
+// per-system load leaves it); the lists are rebuilt before the next step
+__global__ __launch_bounds__(BLOCK) void k_load_all(DevCtx c, const long long *xoff, const int *tw,
+                                                    const double *xp, const double *xv,
+                                                    const double *xa) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  const int sys = c.chunk_sys[i / ATOM_ALIGN];
+  if (sys < 0) return;
+  const SysParam &P = c.P[sys];
+  const int l = i - P.atom_off;
+  const long long o = xoff[sys];
+  if (l >= P.n || o < 0) return;
+  const size_t src = 3 * (size_t)(o + l), dst = 3 * (size_t)i;
+  const long long w = (long long)(unsigned)tw[i];
+  c.pos[i] = make_double4(xp[src], xp[src + 1], xp[src + 2], __longlong_as_double(w));
+  c.gid[i] = l;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    c.vel[dst + d] = xv ? xv[src + d] : 0.0;
+    c.acc[dst + d] = xa ? xa[src + d] : 0.0;
+    c.disp[dst + d] = 0.0;
+  }
+}
+
+// store: the atom of slot i (input index gid[i]) goes to its place in the
+// caller's layout
+__global__ __launch_bounds__(BLOCK) void k_store_all(DevCtx c, const long long *xoff, double *xp,
+                                                     double *xv, double *xa) {
+  const int i = blockIdx.x * BLOCK + threadIdx.x;
+  const int sys = c.chunk_sys[i / ATOM_ALIGN];
+  if (sys < 0) return;
+  const SysParam &P = c.P[sys];
+  const long long o = xoff[sys];
+  if (i - P.atom_off >= P.n || o < 0) return;
+  const int g = c.gid[i];
+  if (g < 0 || g >= P.n) return;
+  const size_t dst = 3 * (size_t)(o + g), src = 3 * (size_t)i;
+  const double4 p = c.pos[i];
+  if (xp) {
+    xp[dst] = p.x;
+    xp[dst + 1] = p.y;
+    xp[dst + 2] = p.z;
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    if (xv) xv[dst + d] = c.vel[src + d];
+    if (xa) xa[dst + d] = c.acc[src + d];
+  }
+}
+
+void launch_load_all(const DevCtx &c, cudaStream_t st, const long long *xoff, const double *xp,
+                     const double *xv, const double *xa) {
+  // type words go through tmp_key (rebuild scratch; the lists are rebuilt
+  // after a load anyway)
+  k_type_words<<<c.nchunks * (ATOM_ALIGN / BLOCK), BLOCK, 0, st>>>(c, c.tmp_key);
+  k_load_all<<<c.nchunks * (ATOM_ALIGN / BLOCK), BLOCK, 0, st>>>(c, xoff, c.tmp_key, xp, xv, xa);
+}
+
+void launch_store_all(const DevCtx &c, cudaStream_t st, const long long *xoff, double *xp,
+                      double *xv, double *xa) {
+  k_store_all<<<c.nchunks * (ATOM_ALIGN / BLOCK), BLOCK, 0, st>>>(c, xoff, xp, xv, xa);
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 static void pair_grids(const DevCtx &c, int tpa, int mixed, int *g);
 

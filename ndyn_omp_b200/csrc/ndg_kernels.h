@@ -86,6 +86,13 @@ void launch_flush(const DevCtx &c, cudaStream_t st, int nsys_cap, int sys);
 void launch_check(const DevCtx &c, cudaStream_t st, int nsys_cap);
 void launch_scale_vel(const DevCtx &c, cudaStream_t st, int sys, double lam);
 void launch_refresh_pfx(const DevCtx &c, cudaStream_t st);
+// every system's state in one pass: xoff[s] = system s's first atom in the
+// caller's concatenated (3,total) arrays, -1 to skip it; the staging blocks
+// xp/xv/xa (device, that layout) may be null where an array is not moved
+void launch_load_all(const DevCtx &c, cudaStream_t st, const long long *xoff, const double *xp,
+                     const double *xv, const double *xa);
+void launch_store_all(const DevCtx &c, cudaStream_t st, const long long *xoff, double *xp,
+                      double *xv, double *xa);
 
 // bytes of shared memory a system's tables need in the staged layout of the
 // pair kernel: pair matrix, per-pair cutoffs/scales, then the F and P tables

@@ -5,10 +5,11 @@
 // pair arithmetic as the context path (ndg_compute), but it allocates
 // nothing: every scratch array it needs (link-cell counts and offsets, the
 // cell-sorted atom order, per-block partial sums, the per-pair constants)
-// lives in the file-scope array g_static_scratch below, which the driver
-// reserves in every GPU's memory when the library is loaded and keeps until
-// the process exits.  The caller passes its own device buffers for the
-// inputs and the force output.
+// lives in the file-scope array g_static_scratch below, which the CUDA
+// driver reserves on every GPU that loads the library's device code and
+// keeps until the process exits.  The caller passes its own device buffers
+// for the inputs and the force output.  The call waits for its stream and
+// returns the potential energy and virial on the host.
 //
 // Limits: STATIC_MAX_ATOMS atoms, STATIC_MAX_CELLS link cells,
 // STATIC_MAX_TYPES types, STATIC_MAX_PAIRS pair potentials.
@@ -18,6 +19,7 @@
 // scratch.  Calls must be ordered, e.g. issued on one stream.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -48,6 +50,13 @@ struct StaticParams {
   float vdr2[STATIC_MAX_PAIRS];
 };
 
+// what the host reads back after the kernels
+struct StaticOut {
+  double result[7];  // potential, virial(6)
+  int bad_type;      // set when some typ[i] lies outside 1..ntypes
+  int pad;
+};
+
 struct StaticScratch {
   StaticParams prm;
   int cell_count[STATIC_MAX_CELLS];
@@ -57,7 +66,7 @@ struct StaticScratch {
   int unsorted[STATIC_MAX_ATOMS];
   int order[STATIC_MAX_ATOMS];
   double partial[STATIC_MAX_BLOCKS * 7];
-  double result[7];  // potential, virial(6)
+  StaticOut out;
 };
 
 // The scratch.  In host code this name is only a stand-in for the symbol,
@@ -66,10 +75,12 @@ struct StaticScratch {
 static __device__ __align__(256) unsigned char g_static_scratch[sizeof(StaticScratch)];
 
 // link cell of each atom (src/nd.f90:1237-1248) and its slot in the cell
-__global__ void ks_bin(StaticScratch *s, const double *pos) {
+__global__ void ks_bin(StaticScratch *s, const double *pos, const int *typ) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const StaticParams &p = s->prm;
   if (i >= p.np) return;
+  const int t = typ[i];
+  if (t < 1 || t > p.ntypes) s->out.bad_type = 1;  // the force kernel skips the atom
   int ix[3];
   for (int d = 0; d < 3; ++d) {
     const double q = pos[3 * (size_t)i + d];
@@ -146,7 +157,7 @@ __global__ __launch_bounds__(SB) void ks_force(StaticScratch *s, const double *p
   const StaticParams &p = s->prm;
   const int i = blockIdx.x * SB + threadIdx.x;
   double fx = 0, fy = 0, fz = 0, pe = 0, vir[6] = {0, 0, 0, 0, 0, 0};
-  if (i < p.np) {
+  if (i < p.np && typ[i] >= 1 && typ[i] <= p.ntypes) {
     const double xi = pos[3 * (size_t)i], yi = pos[3 * (size_t)i + 1], zi = pos[3 * (size_t)i + 2];
     const int ti = typ[i];
     const int cl = s->cellof[i];
@@ -163,7 +174,9 @@ __global__ __launch_bounds__(SB) void ks_force(StaticScratch *s, const double *p
       for (int q = s->cell_start[nc]; q < s->cell_start[nc + 1]; ++q) {
         const int j = s->order[q];
         if (j == i) continue;
-        const int pg = p.pairmat[(ti - 1) + (typ[j] - 1) * p.ntypes];  // gather matrix
+        const int tj = typ[j];
+        if (tj < 1 || tj > p.ntypes) continue;
+        const int pg = p.pairmat[(ti - 1) + (tj - 1) * p.ntypes];  // gather matrix
         const int pt = pg & PT_MASK;
         if (pt <= 0) continue;
         const double ev = pg < PT_ASYM ? 1.0 : 0.0;  // one-sided pairs: force only
@@ -199,6 +212,8 @@ __global__ __launch_bounds__(SB) void ks_force(StaticScratch *s, const double *p
         }
       }
     }
+  }
+  if (i < p.np) {
     force[3 * (size_t)i] = fx;
     force[3 * (size_t)i + 1] = fy;
     force[3 * (size_t)i + 2] = fz;
@@ -223,7 +238,7 @@ __global__ void ks_reduce(StaticScratch *s, int nblk) {
   for (int k = threadIdx.x; k < 7; k += blockDim.x) {
     double a = 0.0;
     for (int b = 0; b < nblk; ++b) a += s->partial[7 * b + k];
-    s->result[k] = 0.5 * a;
+    s->out.result[k] = 0.5 * a;
   }
 }
 
@@ -284,19 +299,30 @@ extern "C" int ndg_compute0_static(int np, int ntypes, int npairs, int ptsize, d
   p.ptrmin = ptrmin;
   double rcut = rcpair[0];
   for (int j = 1; j < npairs; ++j) rcut = rcpair[j] > rcut ? rcpair[j] : rcut;
-  int ncell = 1;
+  // the cell grid: MCELL = int(box/(rcut+skin)), src/nd.f90:80-83, worked
+  // out in double and bounded before any cast, so no size can wrap
+  const double rl = rcut + skin;
+  if (!(skin >= 0.0) || !(rl > 0.0) || !std::isfinite(rl)) return NDG_ERR_ARG;
+  long long ncell = 1;
   for (int d = 0; d < 3; ++d) {
+    if (!(box[d] > 0.0) || !std::isfinite(box[d])) return NDG_ERR_ARG;
+    const double m = std::floor(box[d] / rl);
+    if (m < 2.0) return NDG_ERR_CELLS;
+    if (m > (double)STATIC_MAX_CELLS) {
+      std::fprintf(stderr, "ndg_compute0_static: %.0f link cells along axis %d exceed the static "
+                   "limit of %d\n", m, d + 1, STATIC_MAX_CELLS);
+      return NDG_ERR_ARG;
+    }
     p.box[d] = box[d];
-    p.mcell[d] = (int)(box[d] / (rcut + skin));  // src/nd.f90:80-83
-    if (p.mcell[d] < 2) return NDG_ERR_CELLS;
+    p.mcell[d] = (int)m;
     ncell *= p.mcell[d];
   }
   if (ncell > STATIC_MAX_CELLS) {
-    std::fprintf(stderr, "ndg_compute0_static: %d link cells exceed the static limit of %d\n",
+    std::fprintf(stderr, "ndg_compute0_static: %lld link cells exceed the static limit of %d\n",
                  ncell, STATIC_MAX_CELLS);
     return NDG_ERR_ARG;
   }
-  p.ncell = ncell;
+  p.ncell = (int)ncell;
   for (int k = 0; k < ntypes * ntypes; ++k)
     if (pairmat[k] < 0 || pairmat[k] > npairs) return NDG_ERR_ARG;
   for (int b = 1; b <= ntypes; ++b)
@@ -308,24 +334,30 @@ extern "C" int ndg_compute0_static(int np, int ntypes, int npairs, int ptsize, d
   }
   p.nstencil = make_stencil(p.mcell, quirk, p.stencil);
   cudaError_t e = cudaMemcpyAsync(&s->prm, &p, sizeof(p), cudaMemcpyHostToDevice, st);
-  // the cell counts accumulate with atomics: they must start at zero, and
-  // the array still holds the previous call's counts
-  if (e == cudaSuccess) e = cudaMemsetAsync(s->cell_count, 0, ncell * sizeof(int), st);
+  // the cell counts accumulate with atomics and the type check only ever
+  // sets its flag: both must start at zero, and the array still holds the
+  // previous call's values
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->cell_count, 0, (size_t)ncell * sizeof(int), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(&s->out.bad_type, 0, sizeof(int), st);
   if (e != cudaSuccess) return NDG_ERR_CUDA;
   const int nb = (np + SB - 1) / SB;
-  ks_bin<<<nb, SB, 0, st>>>(s, pos_d);
+  ks_bin<<<nb, SB, 0, st>>>(s, pos_d, typ_d);
   ks_scan<<<1, 1024, 0, st>>>(s);
   ks_scatter<<<nb, SB, 0, st>>>(s);
-  ks_order<<<(ncell + 7) / 8, 256, 0, st>>>(s);
+  ks_order<<<(p.ncell + 7) / 8, 256, 0, st>>>(s);
   ks_force<<<nb, SB, 0, st>>>(s, pos_d, typ_d, fpair_d, ppair_d, force_d);
   ks_reduce<<<1, 32, 0, st>>>(s, nb);
-  double res[7];
+  StaticOut res;
   e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaMemcpyAsync(res, s->result, sizeof(res), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&res, &s->out, sizeof(res), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return NDG_ERR_CUDA;
-  if (potential) *potential = res[0];
+  if (res.bad_type) {
+    std::fprintf(stderr, "ndg_compute0_static: an atom type lies outside 1..%d\n", ntypes);
+    return NDG_ERR_ARG;
+  }
+  if (potential) *potential = res.result[0];
   if (virial)
-    for (int k = 0; k < 6; ++k) virial[k] = res[1 + k];
+    for (int k = 0; k < 6; ++k) virial[k] = res.result[1 + k];
   return NDG_OK;
 }
