@@ -169,6 +169,13 @@ def traffic_per_atom(cfg):
 
 
 # ---------------------------------------------------------------------------
+# the CPU legs time the oracle's reference-flags build (libndyn_oracle_fast:
+# -Ofast -march=x86-64-v4 -funsafe-math-optimizations -fopenmp, the release
+# flags of the reference's src/Makefile with a portable -march)
+CPU_BUILD = "oracle restatement of the reference OpenMP FP64 loop, built with the reference's " \
+            "release flags (-Ofast -funsafe-math-optimizations -fopenmp, -march=x86-64-v4)"
+
+
 def cpu_rate(spec, target_s, threads=None, fixed_steps=None):
     """Oracle (the reference's FP64 OpenMP path restated) on the host cores:
     setup untimed, then the step loop timed.  Returns (atom-steps/s, steps,
@@ -177,7 +184,7 @@ def cpu_rate(spec, target_s, threads=None, fixed_steps=None):
     import oracle_py
     from helpers import oracle_from_spec
     threads = threads or os.cpu_count()
-    o = oracle_from_spec(spec, threads=threads)
+    o = oracle_from_spec(spec, threads=threads, fast=True)
     assert o.setup_lists() == 0
     dt = spec["control"]["dt"]
     if fixed_steps is None:
@@ -214,7 +221,7 @@ def cpu_rate_systems(specs, steps, warmup, threads):
     from helpers import oracle_from_spec
     work = el = 0.0
     for sp in specs:
-        o = oracle_from_spec(sp, threads=threads)
+        o = oracle_from_spec(sp, threads=threads, fast=True)
         assert o.setup_lists() == 0
         dt = sp["control"]["dt"]
         if warmup:
@@ -358,7 +365,7 @@ def run_reference(args, ws, rank):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD_TEXT[args.config], "sample": sample_txt},
             "cpu_baseline": {"value": v, "unit": "atom-steps/s", "cores": threads, "kind": "port",
-                             "sample": sample_txt + f", {args.steps} steps each"},
+                             "sample": sample_txt + f", {args.steps} steps each; " + CPU_BUILD},
             "e2e": {"value": v, "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
         }
@@ -371,7 +378,7 @@ def run_reference(args, ws, rank):
         sample_txt = f"request 0 of the stream ({len(sample['typ'])} atoms)"
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from helpers import oracle_from_spec
-    o = oracle_from_spec(sample, threads=threads)
+    o = oracle_from_spec(sample, threads=threads, fast=True)
     assert o.setup_lists() == 0
     dt = sample["control"]["dt"]
     if args.warmup:
@@ -389,7 +396,7 @@ def run_reference(args, ws, rank):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD_TEXT[args.config], "sample": sample_txt},
         "cpu_baseline": {"value": v, "unit": "atom-steps/s", "cores": threads, "kind": "port",
-                         "sample": sample_txt + f", {args.steps} steps"},
+                         "sample": sample_txt + f", {args.steps} steps; " + CPU_BUILD},
         "e2e": {"value": v, "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -626,7 +633,7 @@ def main():
             cpu = {"value": r, "unit": "atom-steps/s", "cores": th, "kind": "port",
                    "sample": f"{len(pick)} of {len(specs)} systems spread over the list "
                              f"({n_atoms(pick)} atoms) x 100 steps each ({el:.1f} s), one after "
-                             f"another; oracle restatement of the reference OpenMP FP64 loop"}
+                             f"another; " + CPU_BUILD}
         else:
             sample = specs[0]
             if args.config == "c3":
@@ -634,7 +641,7 @@ def main():
             r, st, el, th = cpu_rate(sample, 15.0)
             cpu = {"value": r, "unit": "atom-steps/s", "cores": th, "kind": "port",
                    "sample": f"{len(sample['typ'])} atoms x {st} steps ({el:.1f} s), "
-                             f"oracle restatement of the reference OpenMP FP64 loop"}
+                             + CPU_BUILD}
 
     touched = N * (4.0 * 2 * (nb_half or 40) + 200.0)
     line = {

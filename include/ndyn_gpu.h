@@ -208,7 +208,12 @@ int ndg_get_forces(ndg_ctx *ctx, int sys, double *force, double *potential,
  * Lists are rebuilt at the start (as dynamics does).  cb (may be NULL)
  * receives every write_thermo record in step order. */
 int ndg_run(ndg_ctx *ctx, int nsteps, ndg_thermo_cb cb, void *user);
-/* Same loop without the prologue list build: continues a run. */
+/* Continues the last run by nsteps more steps, without the prologue list
+ * build: the step count within the run, e0 and the list decision carry on,
+ * so ndg_run(n) followed by ndg_run_continue(m) gives the same states and
+ * write_thermo records as ndg_run(n + m).  A caller that writes the model
+ * every ConfOutFreq steps (write_model, src/nd.f90:172) runs the steps in
+ * such pieces and reads the state in between. */
 int ndg_run_continue(ndg_ctx *ctx, int nsteps, ndg_thermo_cb cb, void *user);
 /* thermo scalars of the last completed step of a system */
 int ndg_get_thermo(ndg_ctx *ctx, int sys, ndg_thermo *t);

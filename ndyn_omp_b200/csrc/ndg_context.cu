@@ -1731,7 +1731,9 @@ static int run_impl(ndg_ctx *c, int nsteps, ndg_thermo_cb cb, void *user, int co
   if (rc) return rc;
   CK(c, cudaMemset(c->ring_count, 0, 4 * sizeof(int)));
   DevCtx d = devctx(c);
-  launch_arm(d, c->st, c->nsys_cap, -1, nsteps, cont ? START_NEW : START_BUILT);
+  // a continued run carries on from the last step (its counter tt, e0 and
+  // list decision), as if the two calls were one Run
+  launch_arm(d, c->st, c->nsys_cap, -1, nsteps, cont ? START_CONTINUE : START_BUILT);
   CK(c, cudaGetLastError());
   rc = run_blocks(c, nsteps, cb, user, true);
   if (rc) flush_pending(c);  // a failed block left the last flush unlaunched

@@ -7,10 +7,11 @@ import oracle_py
 QUIRK = {"ref": oracle_py.MODE_REF, "fixed": oracle_py.MODE_FIXED}
 
 
-def oracle_from_spec(spec, threads=None):
+def oracle_from_spec(spec, threads=None, fast=False):
+    """fast=True: the reference-flags build, for timing only"""
     ctl = dict(spec["control"])
     mode = QUIRK[ctl.pop("quirk", "ref")]
-    o = oracle_py.Oracle(threads=threads, mode=mode)
+    o = oracle_py.Oracle(threads=threads, mode=mode, fast=fast)
     o.set_types(spec["masses"])
     o.set_pairs(spec["pairs"])
     o.set_state(spec["typ"], spec["pos"], spec["box"], vel=spec.get("vel"), acc=spec.get("acc"))

@@ -12,6 +12,9 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ODIR = os.path.join(ROOT, "oracle")
 LIB = os.path.join(ODIR, "_build", "libndyn_oracle.so")
+# the same restatement built with the reference's release flags (-Ofast
+# etc.): the timed CPU baseline only, never the parity checker
+LIB_FAST = os.path.join(ODIR, "_build", "libndyn_oracle_fast.so")
 EXE = os.path.join(ODIR, "_build", "ndyn_oracle")
 
 MODE_REF, MODE_FIXED = 0, 1
@@ -19,7 +22,7 @@ MODE_REF, MODE_FIXED = 0, 1
 
 def ensure_built():
     srcs = [os.path.join(ODIR, f) for f in ("ndyn_oracle.c", "ndyn_oracle.h", "ora_main.c")]
-    if not (os.path.exists(LIB) and os.path.exists(EXE)) or any(
+    if not (os.path.exists(LIB) and os.path.exists(EXE) and os.path.exists(LIB_FAST)) or any(
             os.path.getmtime(s) > os.path.getmtime(LIB) for s in srcs if os.path.exists(s)):
         subprocess.run(["make", "-s", "-C", ODIR], check=True)
 
@@ -46,14 +49,14 @@ class Thermo(ctypes.Structure):
 
 
 THERMO_CB = ctypes.CFUNCTYPE(None, ctypes.POINTER(Thermo), ctypes.c_void_p)
-_lib = None
+_libs = {}
 
 
-def lib():
-    global _lib
-    if _lib is None:
+def lib(fast=False):
+    """The parity build, or with fast=True the reference-flags build."""
+    if fast not in _libs:
         ensure_built()
-        L = ctypes.CDLL(LIB)
+        L = ctypes.CDLL(LIB_FAST if fast else LIB)
         vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
         L.ora_new.restype = vp
         L.ora_free.argtypes = [vp]
@@ -103,8 +106,8 @@ def lib():
         L.ora_velocity.restype = None
         L.ora_fmt_thermo.argtypes = [ctypes.POINTER(Thermo), ctypes.c_char_p]
         L.ora_fmt_thermo.restype = None
-        _lib = L
-    return _lib
+        _libs[fast] = L
+    return _libs[fast]
 
 
 def _p(a):
@@ -128,8 +131,8 @@ def dpot(name, r, params, qprd=0.0, rcut=None):
 class Oracle:
     """One reference-semantics system (module globals of src/mods.f90)."""
 
-    def __init__(self, threads=None, mode=MODE_REF):
-        self.L = lib()
+    def __init__(self, threads=None, mode=MODE_REF, fast=False):
+        self.L = lib(fast)
         self.s = ctypes.c_void_p(self.L.ora_new())
         if threads:
             self.L.ora_set_threads(self.s, int(threads))

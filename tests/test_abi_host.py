@@ -82,3 +82,10 @@ def test_pair_matrix_layout():
     pm = pair_matrix([(1, 1, True, "a", [1]), (2, 2, True, "b", [1]), (1, 2, True, "c", [1])], 2)
     # column-major PairMat(a,b) at (a-1)+(b-1)*ntypes
     assert list(pm) == [1, 3, 3, 2]
+
+
+def test_bench_script_compiles():
+    """bench.py (run by the driver on the GPU host) is valid Python"""
+    import ast
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    ast.parse(open(os.path.join(root, "bench.py")).read())

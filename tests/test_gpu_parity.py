@@ -384,6 +384,28 @@ def test_many_systems_round_robin_build():
         assert sum(ctx.list_updates(i) for i in ids) > 0  # some steps rebuilt
 
 
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_run_continue_equals_one_run(specs, prec):
+    """ndg_run(n) then ndg_run_continue(m) is the same run as ndg_run(n + m):
+    the same states and write_thermo records (e0 and the step counter carry
+    on), which lets a caller stop every ConfOutFreq steps to write the
+    model."""
+    spec = dict(specs["nacl_fixed"])
+    spec["control"] = dict(spec["control"], out_steps=7)
+    out = []
+    for pieces in ((60,), (25, 10, 25)):
+        with nd.Context(0, prec) as ctx:
+            sid = gpu_from_spec(ctx, spec)
+            rows = ctx.run(pieces[0])
+            for m in pieces[1:]:
+                rows += ctx.run(m, cont=True)
+            out.append((ctx.state(sid), rows, ctx.list_updates(sid)))
+    for a, b in zip(out[0][0], out[1][0]):
+        assert np.array_equal(a, b)
+    assert out[0][1] == out[1][1]
+    assert out[0][2] == out[1][2]
+
+
 def test_deterministic_repeat(specs):
     out = []
     for _ in range(2):
