@@ -277,12 +277,14 @@ def force_error(specs, states, local, warm=0):
 def plain_fp64_rate(specs, local, steps, stride):
     """The plain path: each sampled replica alone in an FP64 context (its own
     list build and graphs, untimed), `steps` steps timed with CUDA events on
-    the library's stream; returns summed atom-steps / summed time."""
+    the library's stream; returns summed atom-steps / summed time, the
+    number of systems, and the FP64 force kernel's algorithmic bytes and
+    mean launch time summed over them (eager launches with events)."""
     import torch
 
     import ndyn_omp_b200 as nd
     from ndyn_omp_b200 import workloads as W
-    tot_as, tot_s, n = 0.0, 0.0, 0
+    tot_as, tot_s, n, alg_bytes, pair_s = 0.0, 0.0, 0, 0.0, 0.0
     for sp in specs[::stride]:
         with nd.Context(local, "fp64") as cx:
             sid = W.add_to_context(cx, sp)
@@ -295,9 +297,14 @@ def plain_fp64_rate(specs, local, steps, stride):
             e1.record(st)
             torch.cuda.synchronize()
             tot_s += e0.elapsed_time(e1) / 1e3
-            tot_as += len(sp["typ"]) * steps
+            na = len(sp["typ"])
+            tot_as += na * steps
             n += 1
-    return tot_as / tot_s, n
+            nb_half = cx.neighbor_count(sid) / (2.0 * na)
+            prof = cx.profile_run(20)
+            alg_bytes += na * (4.0 * nb_half + 148.0)
+            pair_s += prof["pair_ms"] / 1e3
+    return tot_as / tot_s, n, alg_bytes, pair_s
 
 
 # ---------------------------------------------------------------------------
@@ -403,63 +410,95 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
-def run_serving(args, ws, rank, local):
-    """c5: the request loop.  Requests arrive on a seeded Poisson clock (wall
-    time); between blocks every arrived request is submitted, and each
+def serve_stream(local, ws, rank, nreq, rate, steps_scale, seed=5):
+    """The request loop over one seeded Poisson stream: requests arrive on a
+    wall clock; between blocks every arrived request is submitted, and each
     server step admits what fits the HBM budget and advances every resident
-    run by one block.  Latency = completion - arrival, wall clock; value =
-    all atom-steps / (last completion - first arrival)."""
+    run by one block.  Latency = completion - arrival (wall clock).  Returns
+    the stream's specs, latencies (s), makespan (s, max over ranks),
+    failures and the server's stats."""
     import torch
 
     import ndyn_omp_b200 as nd
     from ndyn_omp_b200 import workloads as W
-    torch.cuda.set_device(local)
-    reqs = W.serving_requests(args.requests, args.rate, seed=5 + rank)
+    reqs = W.serving_requests(nreq, rate, seed=seed + rank)
     specs = []
     for r in reqs:
         sp = W.build_request(r)
-        sp["steps"] = max(1, int(round(sp["steps"] * args.steps_scale)))
+        sp["steps"] = max(1, int(round(sp["steps"] * steps_scale)))
         specs.append(sp)
-    total = float(sum(len(sp["typ"]) * sp["steps"] for sp in specs))
-    # the stated force error: mixed vs FP64 on the first requests' systems
-    probe = [sp for sp in specs[:8] if len(sp["typ"]) <= 60000][:4] or specs[:1]
-    ea, em = force_error(probe, [None] * len(probe), local, warm=100)
     srv = nd.Server(local, "mixed", hbm_budget=150e9, block_steps=100)
     arrival, lat, which, failed = {}, {}, {}, []
     barrier(ws)
     torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        t0 = time.perf_counter()
-        k = 0
-        while len(lat) < len(specs):
-            now = time.perf_counter() - t0
-            while k < len(specs) and reqs[k]["arrival"] <= now:
-                t = W.submit_to_server(srv, specs[k])
-                arrival[t] = reqs[k]["arrival"]
-                which[t] = k
-                k += 1
-            st = srv.stats()
-            if st["resident"] + st["queued"] == 0:
-                if k < len(specs):
-                    time.sleep(max(0.0, min(0.01, reqs[k]["arrival"] - now)))
-                continue
-            srv.step()
-            tn = time.perf_counter() - t0
-            for t in srv.poll():
-                lat[t] = tn - arrival[t]
-                if srv.status(t) == 2:
-                    srv.result(t)
-                else:
-                    r = reqs[which[t]]
-                    failed.append({"request": which[t], "status": srv.status(t),
-                                   "pot": r["pot"], "atoms": len(specs[which[t]]["typ"]),
-                                   "ensemble": r["ensemble"], "T": round(r["T"], 1),
-                                   "steps": specs[which[t]]["steps"]})
-        t_end = max(arrival[t] + lat[t] for t in lat)
+    t0 = time.perf_counter()
+    k = 0
+    while len(lat) < len(specs):
+        now = time.perf_counter() - t0
+        while k < len(specs) and reqs[k]["arrival"] <= now:
+            t = W.submit_to_server(srv, specs[k])
+            arrival[t] = reqs[k]["arrival"]
+            which[t] = k
+            k += 1
+        st = srv.stats()
+        if st["resident"] + st["queued"] == 0:
+            if k < len(specs):
+                time.sleep(max(0.0, min(0.01, reqs[k]["arrival"] - now)))
+            continue
+        srv.step()
+        tn = time.perf_counter() - t0
+        for t in srv.poll():
+            lat[t] = tn - arrival[t]
+            if srv.status(t) == 2:
+                srv.result(t)
+            else:
+                r = reqs[which[t]]
+                failed.append({"request": which[t], "status": srv.status(t),
+                               "pot": r["pot"], "atoms": len(specs[which[t]]["typ"]),
+                               "ensemble": r["ensemble"], "T": round(r["T"], 1),
+                               "steps": specs[which[t]]["steps"]})
+    t_end = max(arrival[t] + lat[t] for t in lat)
     makespan = allmax(t_end - reqs[0]["arrival"], ws)
     st = srv.stats()
     srv.close()
-    lv = np.array(sorted(lat.values())) * 1e3
+    return specs, np.array(sorted(lat.values())), makespan, failed, st
+
+
+def serving_summary(local, ws, rank, nreq=64, steps_scale=0.02, rates=(50.0, 200.0, 800.0)):
+    """p50/p99 completion latency and aggregate atom-steps/s of a scaled
+    serving stream at each arrival rate (the default bench line's serving
+    record)."""
+    out = {"requests": nreq, "steps_scale": steps_scale, "hbm_budget_gb": 150,
+           "block_steps": 100, "rates": []}
+    for rate in rates:
+        specs, lat, makespan, failed, st = serve_stream(local, ws, rank, nreq, rate, steps_scale)
+        total = float(sum(len(sp["typ"]) * sp["steps"] for sp in specs))
+        lv = lat * 1e3
+        out["rates"].append({"rate_per_s": rate, "p50_ms": float(np.percentile(lv, 50)),
+                             "p99_ms": float(np.percentile(lv, 99)),
+                             "atom_steps_per_s": total * ws / makespan, "failed": len(failed)})
+    return out
+
+
+def run_serving(args, ws, rank, local):
+    """c5: the request loop (serve_stream) on the configured stream."""
+    import torch
+    torch.cuda.set_device(local)
+    from ndyn_omp_b200 import workloads as W
+    reqs = W.serving_requests(args.requests, args.rate, seed=5 + rank)
+    probe_specs = []
+    for r in reqs[:8]:
+        sp = W.build_request(r)
+        if len(sp["typ"]) <= 60000:
+            probe_specs.append(sp)
+    probe = probe_specs[:4] or [W.build_request(reqs[0])]
+    # the stated force error: mixed vs FP64 on the first requests' systems
+    ea, em = force_error(probe, [None] * len(probe), local, warm=100)
+    with ClockSampler(local) as clk:
+        specs, lat, makespan, failed, st = serve_stream(local, ws, rank, args.requests, args.rate,
+                                                        args.steps_scale)
+    total = float(sum(len(sp["typ"]) * sp["steps"] for sp in specs))
+    lv = lat * 1e3
     # each rank serves its own stream: aggregate work over the slowest rank
     value_all = total * ws / makespan
     line = {
@@ -542,6 +581,21 @@ def main():
     ms = e0.elapsed_time(e1)
     rebuilds = sum(ctx.list_updates(i) for i in ids) - nup0
     ms = allmax(ms, ws)
+    steady = None
+    if batch and not args.bare:
+        # the same run further on, once the replicas' rebuilds no longer all
+        # date from the run's first list build: 300 more steps untimed, then
+        # 100 timed (a long run's steady state)
+        ctx.run(300, cont=True)
+        torch.cuda.synchronize()
+        e0.record(s)
+        ctx.run(100, cont=True)
+        e1.record(s)
+        torch.cuda.synchronize()
+        ms_ss = allmax(e0.elapsed_time(e1), ws) / 100
+        steady = {"ms_per_step": ms_ss, "value": N * ws / (ms_ss / 1e3),
+                  "after_steps": max(args.warmup, 3) + min(args.graph_steps, args.steps) +
+                  args.steps + 300, "steps": 100}
     value = N * args.steps * ws / (ms / 1e3)
     clocks = clk.summary()
     if args.bare:
@@ -566,12 +620,19 @@ def main():
             ea, em = force_error(specs, states, local)
             force_err = ea
             extra["force_rel_err_max_replica"] = em
-        prate, pn = plain_fp64_rate(specs, local, 200, 8)
+        prate, pn, palg, ppair = plain_fp64_rate(specs, local, 200, 8)
+        peak0, _ = hbm_peak()
         extra["plain_fp64"] = {
             "value": prate, "unit": "atom-steps/s",
             "sample": f"{pn} of {len(specs)} systems (every 8th), each alone in an FP64 context, "
                       f"200 steps, CUDA-graph blocks of 100",
-            "batched_over_plain": (value / ws) / prate}
+            "batched_over_plain": (value / ws) / prate,
+            # the FP64 force kernel on the same systems: algorithmic bytes
+            # (4 n_half + 148 per atom, each system's own n_half) over its
+            # mean launch time, summed over the systems
+            "roofline": {"bound": "hbm", "achieved": palg / ppair / 1e9, "peak": peak0,
+                         "unit": "GB/s", "frac": palg / ppair / 1e9 / peak0,
+                         "pair_ms_summed": ppair * 1e3}}
 
     # per-kernel mean launch time over the same kind of steps (eager launches
     # with CUDA events on the library's stream)
@@ -643,6 +704,11 @@ def main():
                    "sample": f"{len(sample['typ'])} atoms x {st} steps ({el:.1f} s), "
                              + CPU_BUILD}
 
+    serving = None
+    if batch and not args.bare and args.config == "c4":
+        # the serving loop on a scaled c5 stream at the three arrival rates
+        serving = serving_summary(local, ws, rank)
+
     touched = N * (4.0 * 2 * (nb_half or 40) + 200.0)
     line = {
         "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": ws,
@@ -662,6 +728,8 @@ def main():
                                       "stated force error; p50/p99"},
         "force_rel_err_vs_fp64": force_err,
         **extra,
+        "steady_state": steady,
+        "serving": serving,
         "list_rebuilds_in_timed_region": rebuilds,
         # per step integrate1 (with the work plan) and the two pair kernels; per
         # graph block k_begin_block and k_decide; the 7 rebuild kernels on

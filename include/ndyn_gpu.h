@@ -283,6 +283,20 @@ int ndg_get_gather_depth(ndg_ctx *ctx, int *depth);
  * thread per atom in mixed precision) on the current systems for a few
  * steps and keep the fastest (state is restored afterwards) */
 int ndg_autotune(ndg_ctx *ctx, int steps_per_trial);
+/* The rebuild-interval autotuner: choose each fixed-semantics system's list
+ * skin (so its rebuild interval).  A trial of `steps` steps from freshly
+ * built lists measures the pair kernel's cost per list row, the rebuild
+ * cost per rebuilt tile and each system's rebuild count; a model proposes a
+ * skin in [0.5, 2] x the current one per system, and a second trial with
+ * the proposed skins must run at least 2% faster than the first, or every
+ * skin stays.  Both trials are undone (state restored); the fixed systems'
+ * lists are rebuilt (with the new skins, where kept), and the skins read
+ * back through ndg_get_control.  Forces do not depend on the skin in the
+ * fixed semantics; systems in the reference semantics keep theirs.
+ * *changed (may be NULL) = systems whose skin changed.  No counterpart in the
+ * reference (its Skin is an input, src/read_input.f90:95; its default
+ * 0.2*rcut, src/nd.f90:77-79). */
+int ndg_autotune_skin(ndg_ctx *ctx, int steps, int *changed);
 /* device bytes the context holds, and the bytes one more system of np
  * atoms with ntypes/npairs/ptsize would need */
 int ndg_device_bytes(const ndg_ctx *ctx, long long *bytes);

@@ -54,6 +54,7 @@ SIGNATURES = [
     ("ndg_set_gather_depth", i, [vp, i]),
     ("ndg_get_gather_depth", i, [vp, vp]),
     ("ndg_autotune", i, [vp, i]),
+    ("ndg_autotune_skin", i, [vp, i, vp]),
     ("ndg_device_bytes", i, [vp, vp]),
     ("ndg_system_bytes", ll, [i, i, i, i, d, d, i]),
     ("ndg_get_kernel_times", i, [vp, vp, vp, vp, vp]),

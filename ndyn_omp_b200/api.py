@@ -381,6 +381,14 @@ class Context:
         _ok(self.L.ndg_autotune(self._c, int(steps)), "autotune")
         return self.tuning()
 
+    def autotune_skin(self, steps=60):
+        """The rebuild-interval autotuner (ndg_autotune_skin): a list skin
+        per fixed-semantics system from a trial of `steps` steps, which is
+        undone; returns the number of systems whose skin changed."""
+        n = ctypes.c_int()
+        _ok(self.L.ndg_autotune_skin(self._c, int(steps), ctypes.byref(n)), "autotune_skin")
+        return n.value
+
     def set_precision(self, precision):
         _ok(self.L.ndg_set_precision(self._c, PREC[precision]), "set_precision")
 

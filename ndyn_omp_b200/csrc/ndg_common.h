@@ -12,10 +12,13 @@
 //           fractions of the box (2^32 = one box length; integer wrap-around
 //           is the periodic minimum image), w as in pos.
 //   * vel, acc, disp, force: (3,np) FP64, the reference's own layout.
-//   * nbr   full neighbour list, blocked SoA per system: tiles of 32 atoms,
-//           nbr[nbr_off + (local_i/32)*maxnb*32 + k*32 + local_i%32],
-//           k < maxnb; nnb[i] = count.  A tile's list is one contiguous
-//           region, so the pair kernel streams it with dense DRAM access.
+//   * nbr   full neighbour list, blocked SoA per system: tiles of 128 atoms,
+//           entry k of atom t of a tile at word k*128 + t of the tile's
+//           block (nbr_off + (local_i/128)*maxnb*128), k < maxnb; nnb[i] =
+//           count.  Packed lists (SysParam::nb16) hold 16-bit offsets from
+//           the system's first atom, entries 2w and 2w+1 in the low and high
+//           half of word w*128 + t.  A tile's list is one contiguous region,
+//           so the pair kernel streams it with dense DRAM access.
 //   * atoms are kept sorted by link cell (cell-major, original id inside a
 //     cell); gid[i] maps back to the caller's order.
 #pragma once
@@ -73,6 +76,10 @@ struct SysParam {
   int mcell0[3];                 // link cells at run start
   long long nbr_off;
   int maxnb;
+  int nb16;                      // list entries packed as 16-bit offsets from atom_off,
+                                 // two per 32-bit word (list_entry, ndg_kernels.cu)
+  int neimax_stop;               // reference semantics: NeiMax, the longest half list
+                                 // an atom may have (else 'too many neighbours'); 0 = none
   int tab_off;                   // table entry of pair 1, entry 1
   int pair_off, type_off, pm_off;
   int ntypes, npairs, ptsize;

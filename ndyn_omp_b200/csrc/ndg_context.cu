@@ -146,6 +146,7 @@ struct ndg_ctx {
   int tpa = 0, graph_steps = 100;
   int gather = 4;  // mixed pair loop gather depth (4 or 8)
   int any_spring = 0;  // some system holds spring pairs
+  int any_neimax = 0;  // some system checks the reference's NeiMax at list builds
   int stab_smem = 0;  // staged-table bytes of the pair kernel (0: tables from global)
   int stab_lean = 0;  // the same without the energy table
   int nb_smem = 0;  // neighbour-build dynamic smem
@@ -210,6 +211,7 @@ DevCtx devctx(ndg_ctx *c) {
   d.nb_vcap = c->nb_vcap;
   d.gather = c->gather;
   d.any_spring = c->any_spring;
+  d.any_neimax = c->any_neimax;
   d.nnb = c->nnb;
   d.atom_cell = c->atom_cell;
   d.atom_slot = c->atom_slot;
@@ -393,6 +395,17 @@ int upload_vec(ndg_ctx *c, T *&dst, size_t &cap, const std::vector<T> &v) {
   return NDG_OK;
 }
 
+// the rebuild group runs the NeiMax check while some system needs it
+void note_neimax(ndg_ctx *c) {
+  int any = 0;
+  for (auto &h : c->sys)
+    if (h.alive && h.prm.neimax_stop > 0) any = 1;
+  if (any != c->any_neimax) {
+    c->any_neimax = any;
+    drop_graphs(c);
+  }
+}
+
 // small per-pair/per-type arrays: rebuilt for all systems on any change
 int upload_params(ndg_ctx *c) {
   std::vector<int> pm, pg;
@@ -456,6 +469,7 @@ int upload_params(ndg_ctx *c) {
     c->any_spring = anys;
     drop_graphs(c);
   }
+  note_neimax(c);
   // stage the tables in shared memory when every system's fit (B200 allows
   // 227 KB per block; keep room for two resident blocks per SM)
   int stab = 0, lean = 0;
@@ -514,6 +528,7 @@ int ensure_params(ndg_ctx *c) { return c->params_dirty ? upload_params(c) : NDG_
 // the per-system records alone, when only ranges, grids or list capacities
 // changed (their table offsets are those of the last full upload)
 int upload_sysparams(ndg_ctx *c) {
+  note_neimax(c);
   std::vector<SysParam> prm(c->nsys_cap);
   memset(prm.data(), 0, prm.size() * sizeof(SysParam));
   for (size_t s = 0; s < c->sys.size(); ++s)
@@ -720,6 +735,17 @@ int setup_lists(ndg_ctx *c, const std::vector<int> &which) {
     // sphere, src/nd.f90:84-88), doubled where the reference stencil repeats
     // pairs (a cell count of 2 in ref semantics)
     const double vol = S.box[0] * S.box[1] * S.box[2];
+    if (h.ctl.quirk == NDG_QUIRK_REF && h.ctl.neimax == 0) {
+      // NeiMax = int(4./3.*PI*((rcut+skin)*1.1)**3*np/(box(1)*box(2)*box(3))),
+      // src/nd.f90:84-88, with 4./3. and 1.1 default (single precision) reals;
+      // the value persists, as the reference's module variable does
+      const double f43 = (double)(4.0f / 3.0f), rr = (h.rcut + h.prm.skin) * (double)1.1f;
+      h.ctl.neimax = (int)(f43 * 3.141592653589793 * (rr * rr * rr) * (double)h.n / vol);
+    }
+    // the reference semantics stop where a half list outgrows NeiMax
+    // (k_neimax); the fixed semantics size the lists and only stop where
+    // the device capacity itself runs out
+    h.prm.neimax_stop = h.ctl.quirk == NDG_QUIRK_REF ? std::max(h.ctl.neimax, 0) : 0;
     const double r = (h.rcut + h.prm.skin) * 1.1;
     double est = 4.0 / 3.0 * 3.141592653589793 * r * r * r * h.n / vol;
     if (h.ctl.quirk == NDG_QUIRK_REF &&
@@ -760,6 +786,9 @@ int setup_lists(ndg_ctx *c, const std::vector<int> &which) {
     h.prm.ncell_cap = h.ncell_cap;
     h.prm.nbr_off = h.nbr.off;
     h.prm.maxnb = h.maxnb;
+    // mixed precision lists of systems under 65,536 atom slots are packed as
+    // 16-bit offsets, two per word: half the list bytes to write and stream
+    h.prm.nb16 = (c->precision == NDG_PREC_MIXED && npad <= 65536) ? 1 : 0;
     S.nlist_updates = 0;
     S.rebuild = 0;
     S.err = 0;
@@ -1804,10 +1833,21 @@ int ndg_get_neighbors(ndg_ctx *c, int s, int *pairs, long long cap, long long *n
   CK(c, cudaMemcpy(nb.data(), c->nbr + h.nbr.off, nb.size() * sizeof(int),
                    cudaMemcpyDeviceToHost));
   long long m = 0;
+  const bool nb16 = h.prm.nb16 != 0;
   for (int i = 0; i < n; ++i) {
     const int k1 = std::min(cnt[i], h.maxnb);
+    const size_t col = (size_t)(i / 128) * h.maxnb * 128 + (i % 128);
     for (int k = 0; k < k1; ++k) {
-      const int j = nb[(size_t)(i / 128) * h.maxnb * 128 + (size_t)k * 128 + (i % 128)] - (int)off;
+      int j;
+      if (nb16) {
+        // entry k: half k&1 of word (k>>1)*128 of the column, an offset from
+        // the system's first atom (little-endian: the low half comes first)
+        unsigned short e[2];
+        memcpy(e, &nb[col + (size_t)(k >> 1) * 128], sizeof(e));
+        j = e[k & 1];
+      } else {
+        j = nb[col + (size_t)k * 128] - (int)off;
+      }
       const int gi = g[i], gj = g[j];
       if (gi < gj) {
         if (pairs && m < cap) {
@@ -1903,6 +1943,49 @@ long long ndg_system_bytes(int np, int ntypes, int npairs, int ptsize, double de
 // launch shape (threads per atom) runs `steps` real graph steps on the
 // current systems, timed with CUDA events on the library's stream, the state
 // is restored after each trial, and the fastest shape is kept.
+namespace {
+// A device copy of every mutable array of a context (positions, lists,
+// state records, ...), so that trial steps can be undone.
+struct Snapshot {
+  struct Buf {
+    void *p;
+    size_t bytes;
+  };
+  ndg_ctx *c;
+  std::vector<Buf> bufs;
+  char *snap = nullptr;
+  explicit Snapshot(ndg_ctx *ctx) : c(ctx) {
+    const size_t A = (size_t)c->atoms.cap * ATOM_ALIGN, T = 2 * (size_t)c->atoms.cap;
+    bufs = {{c->pos, A * sizeof(double4)},       {c->pfx, A * sizeof(int4)},
+            {c->vel, 3 * A * sizeof(double)},    {c->acc, 3 * A * sizeof(double)},
+            {c->disp, 3 * A * sizeof(double)},   {c->gid, A * sizeof(int)},
+            {c->nnb, A * sizeof(int)},           {c->atom_cell, A * sizeof(int)},
+            {c->itop, 2 * (size_t)c->atoms.cap * sizeof(double)},
+            {c->tile_rows, T * sizeof(int)},
+            {c->cell_start, (size_t)c->cells.cap * sizeof(int)},
+            {c->nbr, (size_t)c->nbrs.cap * sizeof(int)},
+            {c->dS, (size_t)c->nsys_cap * sizeof(SysState)}};
+    size_t total = 0;
+    for (auto &b : bufs) total += b.bytes;
+    snap = dalloc<char>(total);
+  }
+  ~Snapshot() {
+    if (snap) cudaFree(snap);
+  }
+  bool ok() const { return snap != nullptr; }
+  cudaError_t copy(bool save) {
+    size_t off = 0;
+    for (auto &b : bufs) {
+      cudaError_t e = save ? cudaMemcpyAsync(snap + off, b.p, b.bytes, cudaMemcpyDeviceToDevice, c->st)
+                           : cudaMemcpyAsync(b.p, snap + off, b.bytes, cudaMemcpyDeviceToDevice, c->st);
+      if (e != cudaSuccess) return e;
+      off += b.bytes;
+    }
+    return cudaStreamSynchronize(c->st);
+  }
+};
+}  // namespace
+
 int ndg_autotune(ndg_ctx *c, int steps) {
   if (!c || steps < 1) return NDG_ERR_ARG;
   cudaSetDevice(c->device);
@@ -1913,35 +1996,9 @@ int ndg_autotune(ndg_ctx *c, int steps) {
   }
   rc = ensure_params(c);
   if (rc) return rc;
-  const size_t A = (size_t)c->atoms.cap * ATOM_ALIGN, T = 2 * (size_t)c->atoms.cap;
-  struct Buf {
-    void *p;
-    size_t bytes;
-  };
-  const std::vector<Buf> bufs = {
-      {c->pos, A * sizeof(double4)},       {c->pfx, A * sizeof(int4)},
-      {c->vel, 3 * A * sizeof(double)},    {c->acc, 3 * A * sizeof(double)},
-      {c->disp, 3 * A * sizeof(double)},   {c->gid, A * sizeof(int)},
-      {c->nnb, A * sizeof(int)},           {c->atom_cell, A * sizeof(int)},
-      {c->itop, 2 * (size_t)c->atoms.cap * sizeof(double)},
-      {c->tile_rows, T * sizeof(int)},
-      {c->cell_start, (size_t)c->cells.cap * sizeof(int)},
-      {c->nbr, (size_t)c->nbrs.cap * sizeof(int)},
-      {c->dS, (size_t)c->nsys_cap * sizeof(SysState)}};
-  size_t total = 0;
-  for (auto &b : bufs) total += b.bytes;
-  char *snap = dalloc<char>(total);
-  if (!snap) return NDG_ERR_NOMEM;
-  auto copy = [&](bool save) -> cudaError_t {
-    size_t off = 0;
-    for (auto &b : bufs) {
-      cudaError_t e = save ? cudaMemcpyAsync(snap + off, b.p, b.bytes, cudaMemcpyDeviceToDevice, c->st)
-                           : cudaMemcpyAsync(b.p, snap + off, b.bytes, cudaMemcpyDeviceToDevice, c->st);
-      if (e != cudaSuccess) return e;
-      off += b.bytes;
-    }
-    return cudaStreamSynchronize(c->st);
-  };
+  Snapshot sn(c);
+  if (!sn.ok()) return NDG_ERR_NOMEM;
+  auto copy = [&](bool save) { return sn.copy(save); };
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -1979,13 +2036,134 @@ int ndg_autotune(ndg_ctx *c, int steps) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  cudaFree(snap);
   CK(c, cudaMemset(c->ring_count, 0, 4 * sizeof(int)));
   c->tpa = best ? best : keep_tpa;
   c->gather = best ? best_g : keep_gather;
   drop_graphs(c);
   if (ce != cudaSuccess) return cuda_fail(c, ce, "autotune snapshot");
   return rc;
+}
+
+// The rebuild-interval autotuner: a list skin per system (fixed semantics).
+//
+// A larger skin makes every list longer, and the pair kernel's work per step
+// grows with the list (as (rcut+skin)^3); a smaller one makes the fixed
+// rebuild test (the two largest displacements since the last build against
+// the skin) fire sooner.  From lists built afresh, a trial of `steps` eager
+// steps measures the two costs on this batch: the pair kernel's time per
+// unit of the work plan's tile cost (rows + 16 per tile), the rebuild
+// group's time per rebuilt tile, and each system's rebuild count.  With the
+// rebuild interval taken as proportional to the skin (displacements grow
+// about linearly over the few tens of steps between builds), each system
+// gets the skin of the grid f * skin, f in [0.5, 2], with the lowest
+// modelled cost per step, if that beats its current skin by 2%.  A second
+// trial from the same state with the new skins' lists must then run at
+// least 2% faster than the first, or every skin goes back: the model only
+// proposes, the clock decides.  Forces do not depend on the skin in these
+// semantics (every pair within the cutoff is in the list at every step).
+// The trials are undone.  Systems in the reference semantics keep their
+// skin: their rebuild test is the reference's, and their list contents
+// depend on it.
+namespace {
+// one trial from the current state, undone afterwards: the mean time per
+// step of the step's kernels, and the state records after the trial
+int skin_trial(ndg_ctx *c, int steps, double *ms, std::vector<SysState> &after) {
+  Snapshot sn(c);
+  if (!sn.ok()) return NDG_ERR_NOMEM;
+  cudaError_t ce = sn.copy(true);
+  if (ce != cudaSuccess) return cuda_fail(c, ce, "autotune_skin snapshot");
+  int rc = ndg_profile_run(c, steps);
+  if (rc == NDG_OK) {
+    *ms = c->t_int + c->t_pair + c->t_reb;
+    CK(c, cudaMemcpy(after.data(), c->dS, after.size() * sizeof(SysState),
+                     cudaMemcpyDeviceToHost));
+  }
+  ce = sn.copy(false);
+  if (ce != cudaSuccess) return cuda_fail(c, ce, "autotune_skin restore");
+  CK(c, cudaMemset(c->ring_count, 0, 4 * sizeof(int)));
+  return rc;
+}
+}  // namespace
+
+int ndg_autotune_skin(ndg_ctx *c, int steps, int *changed) {
+  if (changed) *changed = 0;
+  if (!c || steps < 4) return NDG_ERR_ARG;
+  cudaSetDevice(c->device);
+  std::vector<int> fixed;
+  for (size_t s = 0; s < c->sys.size(); ++s)
+    if (c->sys[s].alive && c->sys[s].ctl.quirk == NDG_QUIRK_FIXED) fixed.push_back((int)s);
+  if (fixed.empty()) return NDG_OK;
+  int rc = lists_ready(c) ? ensure_params(c) : setup_lists(c);
+  if (rc) return rc;
+  rc = setup_lists(c, fixed);  // fresh lists: both trials start alike
+  if (rc) return rc;
+  std::vector<SysState> S0(c->nsys_cap), S1(c->nsys_cap), S2(c->nsys_cap);
+  CK(c, cudaMemcpy(S0.data(), c->dS, S0.size() * sizeof(SysState), cudaMemcpyDeviceToHost));
+  double msA = 0.0, msB = 0.0;
+  rc = skin_trial(c, steps, &msA, S1);
+  if (rc) return rc;
+  const double t_pair = c->t_pair * steps, t_reb = c->t_reb * steps;  // ms over the trial
+  double units = 0.0, rebuilt_tiles = 0.0;
+  for (int s : fixed) {
+    const double tiles = (double)c->sys[s].prm.npad / 128.0;
+    units += tiles * 16.0 + (double)S0[s].rows;
+    rebuilt_tiles += tiles * (double)(S1[s].nlist_updates - S0[s].nlist_updates);
+  }
+  if (units <= 0.0 || rebuilt_tiles <= 0.0 || t_pair <= 0.0 || t_reb <= 0.0)
+    return NDG_OK;  // nothing rebuilt in the trial: no measure of a rebuild's cost
+  const double alpha = t_pair / steps / units;  // ms per tile-cost unit per step
+  const double beta = t_reb / rebuilt_tiles;    // ms per rebuilt tile
+  static const double grid[] = {0.5, 0.625, 0.75, 0.875, 1.0, 1.25, 1.5, 1.75, 2.0};
+  std::vector<int> ids;
+  std::vector<double> old_skin;
+  for (int s : fixed) {
+    HostSys &h = c->sys[s];
+    const double skin0 = h.prm.skin, rl0 = h.rcut + skin0;
+    if (!(skin0 > 0.0)) continue;
+    const double tiles = (double)h.prm.npad / 128.0;
+    const double rows = (double)S0[s].rows / tiles;  // mean list rows of a tile
+    const int nup = std::max(S1[s].nlist_updates - S0[s].nlist_updates, 1);
+    const double bmin = std::min(S0[s].box[0], std::min(S0[s].box[1], S0[s].box[2]));
+    auto cost = [&](double skin) {
+      const double g = (h.rcut + skin) / rl0;
+      return alpha * tiles * (rows * g * g * g + 16.0) +
+             beta * tiles * ((double)nup / steps) * (skin0 / skin);
+    };
+    const double c0 = cost(skin0);
+    double best = skin0, bc = c0;
+    for (double f : grid) {
+      const double skin = f * skin0;
+      if ((int)(bmin / (h.rcut + skin)) < 3) continue;  // keep three link cells per axis
+      const double cf = cost(skin);
+      if (cf < bc) {
+        bc = cf;
+        best = skin;
+      }
+    }
+    if (best != skin0 && bc < 0.98 * c0) {
+      ids.push_back(s);
+      old_skin.push_back(h.ctl.skin);
+      h.ctl.skin = best;
+      fill_control_params(h);
+    }
+  }
+  if (ids.empty()) return NDG_OK;
+  c->params_dirty = true;
+  rc = setup_lists(c, ids);  // the proposed skins' lists
+  if (!rc) rc = skin_trial(c, steps, &msB, S2);
+  if (rc || !(msB < 0.98 * msA)) {
+    // the clock does not confirm the model: every skin goes back
+    for (size_t k = 0; k < ids.size(); ++k) {
+      HostSys &h = c->sys[ids[k]];
+      h.ctl.skin = old_skin[k];
+      fill_control_params(h);
+    }
+    c->params_dirty = true;
+    const int rr = setup_lists(c, ids);
+    return rc ? rc : rr;
+  }
+  if (changed) *changed = (int)ids.size();
+  return NDG_OK;
 }
 
 int ndg_get_stream(ndg_ctx *c, void **stream) {
@@ -1997,13 +2175,15 @@ int ndg_get_stream(ndg_ctx *c, void **stream) {
 int ndg_profile_run(ndg_ctx *c, int nsteps) {
   if (!c || nsteps < 1 || !lists_ready(c)) return NDG_ERR_ARG;
   cudaSetDevice(c->device);
-  int rc = upload_params(c);
+  int rc = ensure_params(c);
   if (rc) return rc;
   CK(c, cudaMemset(c->ring_count, 0, 4 * sizeof(int)));
   DevCtx d = devctx(c);
   const int mixed = c->precision == NDG_PREC_MIXED;
   const int tpa = choose_tpa(c);
-  launch_arm(d, c->st, c->nsys_cap, -1, nsteps, START_NEW);
+  // the steps continue the last run (no first-step energy output), as the
+  // step blocks of a run do
+  launch_arm(d, c->st, c->nsys_cap, -1, nsteps, START_CONTINUE);
   launch_begin_block(d, c->st, c->nsys_cap, nsteps);
   std::vector<cudaEvent_t> ev(4 * (size_t)nsteps);
   for (auto &e : ev) CK(c, cudaEventCreate(&e));

@@ -19,6 +19,7 @@
 #include <cstdio>
 
 #include <algorithm>
+#include <climits>
 #include <type_traits>
 
 #include "ndg_kernels.h"
@@ -28,6 +29,28 @@ namespace ndg {
 constexpr int TILE = 128;  // atoms per tile of the neighbour list and the pair kernel
 
 __device__ __forceinline__ int tw_of(double w) { return (int)__double_as_longlong(w); }
+
+// Entry k of an atom's neighbour list; col points at the atom's column of
+// its tile's list block (block start + the atom's index in the tile).  A
+// plain list holds atom slots, one per 32-bit word, entry k in word k*TILE;
+// a packed list (SysParam::nb16: mixed precision, systems under 65,536
+// atoms) holds 16-bit offsets from the system's first atom, entry k in half
+// k&1 of word (k>>1)*TILE, so one 32-bit load brings two entries.
+__device__ __forceinline__ int list_entry(const int *col, int nb16, int atom_off, int k) {
+  if (nb16)
+    return atom_off + (int)__ldg((const unsigned short *)(col + (k >> 1) * TILE) + (k & 1));
+  return __ldg(col + k * TILE);
+}
+
+__device__ __forceinline__ void list_store(int *col, int nb16, int atom_off, int k, int j) {
+  if (nb16) ((unsigned short *)(col + (k >> 1) * TILE))[k & 1] = (unsigned short)(j - atom_off);
+  else col[k * TILE] = j;
+}
+
+// 32-bit words a tile's list of `rows` rows occupies
+__device__ __forceinline__ int list_words(int rows, int nb16) {
+  return nb16 ? (rows + 1) >> 1 : rows;
+}
 
 // record an error on the system and in the context-wide error word
 __device__ __forceinline__ void set_err(const DevCtx &c, SysState *S, int bits) {
@@ -701,6 +724,7 @@ __device__ void bin_chunk(const DevCtx &c, int sys, int chunk) {
 }
 
 __global__ __launch_bounds__(BLOCK) void k_bin(DevCtx c) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) c.ring_count[2] = 0;  // k_scan counts the cells
   for_listed(c, [&](int s, int &f, int &n) { chunk_range(c, s, f, n); },
              [&](int s, int u) { bin_chunk(c, s, u); });
 }
@@ -753,6 +777,7 @@ __device__ void scan_system(const DevCtx &c, int s, int counting) {
     S->nstencil = make_stencil(S->mcell, P->quirk, S->stencil);
     for (int d = 0; d < 3; ++d) S->box_build[d] = S->box[d];
     if (counting) S->nlist_updates += 1;  // NlistUpdates, src/nd.f90:1495
+    atomicAdd(c.ring_count + 2, ncell);  // the build chooses its form by the cells listed
   }
 }
 
@@ -877,6 +902,15 @@ __global__ __launch_bounds__(BLOCK) void k_copyback(DevCtx c, int mixed) {
 constexpr int TC_MAX = 256;    // link cells a tile may stage
 constexpr int HSLOTS = 1024;   // shared hash slots for the tile's cell set
 constexpr float NB_MARGIN = 1e-5f;
+// The list build takes one of two forms.  By tile (k_build): a CTA per
+// 128-atom tile, a warp per own atom testing 32 staged candidates at a time
+// (plenty of parallelism however few atoms are rebuilt: a step's few
+// replicas).  By cell (k_build_cells): a warp per link cell, a lane per own
+// atom, the cell's candidates broadcast one at a time (far fewer
+// instructions, but a long serial chain per warp, which only pays when every
+// warp has several cells: a prologue, a large system).  Both give every
+// atom the same list in the same order.
+constexpr int CELL_BUILD_MIN = 16384;  // listed cells from which the cell form builds
 constexpr int BUILD_CAP = 3072;  // candidates the build stages per tile
 constexpr int NBT = 256;         // threads of the build CTA (8 warps)
 
@@ -1009,7 +1043,7 @@ __device__ __noinline__ void build_tile_direct(const DevCtx &c, int sys, int til
         const unsigned bal = __ballot_sync(0xffffffffu, hit);
         if (hit) {
           const int k = cnt + __popc(bal & ((1u << lane) - 1u));
-          if (k < maxnb) dst[k * TILE + t] = j;
+          if (k < maxnb) list_store(dst + t, P->nb16, P->atom_off, k, j);
         }
         cnt += __popc(bal);
       }
@@ -1176,7 +1210,6 @@ __device__ void build_tile(const DevCtx &c, int sys, int tile) {
     return;
   }
   const int U = nu, C = coff[nu];
-  if (threadIdx.x == 0) atomicMax(c.ring_count + 2, C);
   // 2. stage the candidates
   for (int u = threadIdx.x >> 5; u < U; u += NBT / 32) {
     const int q0 = coff[u], len = coff[u + 1] - q0;
@@ -1280,6 +1313,7 @@ __device__ void build_tile(const DevCtx &c, int sys, int tile) {
   const bool one = nt == 1 && npr == 1 && pm[0] == 1;
   const float2 band1 = one ? rlb_s[0] : make_float2(0.f, 0.f);
   int *dst = c.nbr + P->nbr_off + (long long)(local0 / TILE) * maxnb * TILE;
+  const int nb16 = P->nb16, aoff = P->atom_off;
   for (int rb = 0; rb < nruns;) {
     // the runs whose lists fit the buffer together
     __shared__ int re_s;
@@ -1367,7 +1401,7 @@ __device__ void build_tile(const DevCtx &c, int sys, int tile) {
         const unsigned bal = __ballot_sync(0xffffffffu, hit);
         if (hit) {
           const int k = cnt + __popc(bal & ((1u << lane) - 1u));
-          if (k < maxnb) dst[k * TILE + t] = cgid[q];
+          if (k < maxnb) list_store(dst + t, nb16, aoff, k, cgid[q]);
         }
         cnt += __popc(bal);
       }
@@ -1399,10 +1433,223 @@ __device__ void build_tile(const DevCtx &c, int sys, int tile) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Neighbour build by link cell (buildVerletList, src/nd.f90:1328-1446): one
+// warp per cell of a listed system, one lane per atom of the cell (32 at a
+// time).  The candidates of the cell's stencil entries pass the warp one
+// after another, in stencil order and, within a cell, in cell order; every
+// lane tests each against its own atom and appends the hits to its own
+// column of the blocked list.  Each list thus has the order of the
+// reference's cell walk (stencil entry, then cell order), and the candidate
+// test is the tile build's: FP32 on the fixed-point positions outside a
+// 1e-5 band around the list radius and PTrMin, the reference's FP64 test
+// inside it.  A candidate costs the warp one broadcast load and one test
+// for all 32 atoms of the cell at once.
+constexpr int CB_THREADS = 256;
+
+__device__ __forceinline__ int wrap_step(int x, int d, int M) {
+  const int y = x + d;  // d in {-1, 0, 1}, x in [0, M)
+  return y < 0 ? y + M : (y >= M ? y - M : y);
+}
+
+__device__ __forceinline__ void build_cell(const DevCtx &c, int sys, int cell, int lane) {
+  const SysParam *__restrict__ P = c.P + sys;
+  SysState *S = c.S + sys;
+  const int *cst = c.cell_start + P->cell_off;
+  const int o0 = cst[cell], o1 = cst[cell + 1];
+  if (o0 >= o1) return;
+  const int M0 = S->mcell[0], M1 = S->mcell[1], M2 = S->mcell[2];
+  const int ne = S->nstencil;
+  // lane e < ne holds stencil entry e: its cell's candidate range and
+  // whether it is the own cell
+  int e_q0 = 0, e_q1 = 0, e_center = 0;
+  if (lane < ne) {
+    const int cx = cell % M0, cy = (cell / M0) % M1, cz = cell / (M0 * M1);
+    const int st = S->stencil[lane];
+    const int nc = wrap_step(cx, (st & 15) - 1, M0) +
+                   (wrap_step(cy, ((st >> 4) & 15) - 1, M1) +
+                    wrap_step(cz, ((st >> 8) & 15) - 1, M2) * M1) * M0;
+    e_q0 = cst[nc];
+    e_q1 = cst[nc + 1];
+    e_center = (st >> 12) & 1;
+  }
+  const int aoff = P->atom_off, nt = P->ntypes, maxnb = P->maxnb, nb16 = P->nb16;
+  const int *pm = c.pairmat + P->pm_off;
+  const double *rl2 = c.rlist2 + P->pair_off;
+  const float sb0 = (float)(S->box[0] * (1.0 / FX_ONE)), sb1 = (float)(S->box[1] * (1.0 / FX_ONE)),
+              sb2 = (float)(S->box[2] * (1.0 / FX_ONE));
+  const float ptrlo = (float)P->ptrmin * (1.f - NB_MARGIN),
+              ptrhi = (float)P->ptrmin * (1.f + NB_MARGIN);
+  const bool one = nt == 1 && P->npairs == 1 && pm[0] == 1;
+  const float rf1 = (float)rl2[0];
+  const float2 band1 = make_float2(rf1 * (1.f - NB_MARGIN), rf1 * (1.f + NB_MARGIN));
+  // a candidate farther than the list radius from the box of the warp's own
+  // atoms cannot be a neighbour of any of them; the box is kept as offsets
+  // from the first own atom, whose wrap-around differences are minimum
+  // images on grids of five or more cells per axis
+  const bool prune = M0 >= 5 && M1 >= 5 && M2 >= 5;
+  const float rlbox = (float)(P->rlist * P->rlist) * (1.f + 4.f * NB_MARGIN);
+  for (int g0 = o0; g0 < o1; g0 += 32) {
+    const int li = g0 + lane;  // the lane's own atom (local slot)
+    const bool own = li < o1;
+    const int i = aoff + (own ? li : o0);
+    const int4 pi = c.pfx[i];
+    const int ti = tw_type(pi.w);
+    const int ax = __shfl_sync(0xffffffffu, pi.x, 0), ay = __shfl_sync(0xffffffffu, pi.y, 0),
+              az = __shfl_sync(0xffffffffu, pi.z, 0);
+    const int ox = (int)((unsigned)pi.x - (unsigned)ax), oy = (int)((unsigned)pi.y - (unsigned)ay),
+              oz = (int)((unsigned)pi.z - (unsigned)az);
+    const int lx = __reduce_min_sync(0xffffffffu, own ? ox : INT_MAX),
+              hx = __reduce_max_sync(0xffffffffu, own ? ox : INT_MIN),
+              ly = __reduce_min_sync(0xffffffffu, own ? oy : INT_MAX),
+              hy = __reduce_max_sync(0xffffffffu, own ? oy : INT_MIN),
+              lz = __reduce_min_sync(0xffffffffu, own ? oz : INT_MAX),
+              hz = __reduce_max_sync(0xffffffffu, own ? oz : INT_MIN);
+    int *col = c.nbr + P->nbr_off + (long long)(li / TILE) * maxnb * TILE + (li % TILE);
+    int cnt = 0;
+    for (int e = 0; e < ne; ++e) {
+      const bool center = __shfl_sync(0xffffffffu, e_center, e) != 0;
+      const int q1 = __shfl_sync(0xffffffffu, e_q1, e);
+      for (int qb = __shfl_sync(0xffffffffu, e_q0, e); qb < q1; qb += 32) {
+        // 32 candidates at once, one per lane; the lanes test their own
+        // candidate against the own atoms' box, then the kept ones pass
+        // the warp in cell order
+        const int qq = qb + lane;
+        const bool have = qq < q1;
+        const int4 pc = c.pfx[aoff + (have ? qq : qb)];
+        bool keep = have;
+        if (prune && keep) {
+          const int dx = (int)((unsigned)pc.x - (unsigned)ax), dy = (int)((unsigned)pc.y - (unsigned)ay),
+                    dz = (int)((unsigned)pc.z - (unsigned)az);
+          const float gx = dx < lx ? (float)lx - (float)dx : (dx > hx ? (float)dx - (float)hx : 0.f);
+          const float gy = dy < ly ? (float)ly - (float)dy : (dy > hy ? (float)dy - (float)hy : 0.f);
+          const float gz = dz < lz ? (float)lz - (float)dz : (dz > hz ? (float)dz - (float)hz : 0.f);
+          const float d2b = (gx * sb0) * (gx * sb0) + (gy * sb1) * (gy * sb1) + (gz * sb2) * (gz * sb2);
+          keep = d2b <= rlbox;
+        }
+        unsigned m = __ballot_sync(0xffffffffu, keep);
+        while (m) {
+          const int k = __ffs(m) - 1;
+          m &= m - 1;
+          const int4 pj = make_int4(__shfl_sync(0xffffffffu, pc.x, k), __shfl_sync(0xffffffffu, pc.y, k),
+                                    __shfl_sync(0xffffffffu, pc.z, k), __shfl_sync(0xffffffffu, pc.w, k));
+          const int j = aoff + qb + k;
+          int mx = 1;
+          if (!one) {
+            const int tj = tw_type(pj.w);
+            const int a = pm[(ti - 1) + (tj - 1) * nt], b = pm[(tj - 1) + (ti - 1) * nt];
+            mx = a > b ? a : b;
+          }
+          const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * sb0;
+          const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * sb1;
+          const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * sb2;
+          const float d2f = r0 * r0 + r1 * r1 + r2 * r2;
+          const bool live = own && j != i && mx > 0;
+          float2 band = band1;
+          if (!one && live) {
+            const float rf = (float)rl2[mx - 1];
+            band = make_float2(rf * (1.f - NB_MARGIN), rf * (1.f + NB_MARGIN));
+          }
+          // outside both margins FP32 decides; inside either, FP64 does
+          bool hit = live && d2f < band.x && !(center && d2f < ptrhi);
+          const bool unsure = live && ((d2f >= band.x && d2f <= band.y) ||
+                                       (center && d2f >= ptrlo && d2f <= ptrhi));
+          if (unsure) {
+            // the reference's FP64 test (src/nd.f90:1362-1377, 1419-1420),
+            // its operands read again on this rare path
+            const double4 pid = c.pos[i], pjd = c.pos[j];
+            double s0 = pid.x - pjd.x, s1 = pid.y - pjd.y, s2 = pid.z - pjd.z;
+            s0 = s0 - round(s0);
+            s1 = s1 - round(s1);
+            s2 = s2 - round(s2);
+            const double x0 = S->box[0] * s0, x1 = S->box[1] * s1, x2 = S->box[2] * s2;
+            double d2 = x0 * x0;
+            d2 = d2 + x1 * x1;
+            d2 = d2 + x2 * x2;
+            hit = !(center && d2 < P->ptrmin) && !(d2 > rl2[mx - 1]);
+          }
+          if (hit) {
+            if (cnt < maxnb) list_store(col, nb16, aoff, cnt, j);
+            ++cnt;
+          }
+        }
+      }
+    }
+    if (own) {
+      c.nnb[aoff + li] = cnt;
+      if (cnt > maxnb) set_err(c, S, E_NEIMAX);
+    }
+  }
+}
+
+// the listed systems' cells, dealt round-robin to every warp of the grid
+__global__ __launch_bounds__(CB_THREADS, 3) void k_build_cells(DevCtx c) {
+  __shared__ int l_sys[LIST_STAGE], l_pre[LIST_STAGE + 1];
+  __shared__ int wsum[CB_THREADS / 32];
+  static_assert(CB_THREADS == LIST_STAGE, "one listed system per thread when staging");
+  if (c.ring_count[2] < CELL_BUILD_MIN) return;  // few cells: the tile build takes them
+  const int n = c.ring_count[3];
+  const int lane = threadIdx.x & 31;
+  const int nw = gridDim.x * (CB_THREADS / 32);
+  const int gw = blockIdx.x * (CB_THREADS / 32) + (threadIdx.x >> 5);
+  for (int k0 = 0; k0 < n; k0 += LIST_STAGE) {
+    const int m = min(LIST_STAGE, n - k0);
+    __syncthreads();  // the previous group's entries are no longer read
+    int cnt = 0;
+    if ((int)threadIdx.x < m) {
+      const int s = c.rb_list[k0 + threadIdx.x];
+      l_sys[threadIdx.x] = s;
+      cnt = c.S[s].ncell;
+    }
+    const int pre = block_excl_scan(cnt, wsum);
+    if ((int)threadIdx.x < m) l_pre[threadIdx.x] = pre;
+    if ((int)threadIdx.x == m - 1) l_pre[m] = pre + cnt;
+    __syncthreads();
+    const int total = l_pre[m];
+    for (int u = gw; u < total; u += nw) {
+      int lo = 0, hi = m - 1;  // the listed system whose cells hold unit u
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (l_pre[mid] <= u) lo = mid;
+        else hi = mid - 1;
+      }
+      build_cell(c, l_sys[lo], u - l_pre[lo], lane);
+    }
+  }
+}
+
+// each rebuilt tile's row count (its longest list, for the pair kernel's L2
+// prefetch) and the system's sum of them (the work plan's tile cost)
+__global__ __launch_bounds__(TILE) void k_tile_rows(DevCtx c) {
+  __shared__ int wmax[TILE / 32];
+  if (c.ring_count[2] < CELL_BUILD_MIN) return;  // the tile build counted its own rows
+  for_listed(c,
+             [&](int s, int &f, int &n) {
+               f = c.P[s].atom_off / TILE;
+               n = c.P[s].npad / TILE;
+             },
+             [&](int s, int tile) {
+               const SysParam *P = c.P + s;
+               const int i = tile * TILE + threadIdx.x;
+               int r = i - P->atom_off < P->n ? min(c.nnb[i], P->maxnb) : 0;
+               r = __reduce_max_sync(0xffffffffu, r);
+               if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = r;
+               __syncthreads();
+               if (threadIdx.x == 0) {
+                 int rows = 0;
+                 for (int w = 0; w < TILE / 32; ++w) rows = max(rows, wmax[w]);
+                 c.tile_rows[tile] = rows;
+                 atomicAdd(&c.S[s].rows, (unsigned long long)rows);
+               }
+               __syncthreads();
+             });
+}
+
 // A short rebuild list (a step's rebuilds: a few tiles per block) takes its
 // tiles from a work counter, so that blocks that draw cheap tiles take more
 // of them; a long one (a prologue build) is dealt round-robin.
 __global__ __launch_bounds__(NBT, 2) void k_build(DevCtx c) {
+  if (c.ring_count[2] >= CELL_BUILD_MIN) return;  // many cells: the cell build takes them
   const int n = c.ring_count[3];
   if (n >= NBT) {  // (thread n writes the total below)
     for_listed(c,
@@ -1598,7 +1845,7 @@ __device__ __noinline__ SpringSum spring_pass(const DevCtx &c, const SysParam *P
   const double b0 = S->box[0], b1 = S->box[1], b2 = S->box[2];
   const int gi = c.gid[i];
   for (int k = la; k < cnt; k += tpa) {
-    const int j = __ldg(nb + k * TILE);
+    const int j = list_entry(nb, P->nb16, P->atom_off, k);
     const double4 pjd = c.pos[j];
     const int pg = pm[(ti - 1) + (tw_type(tw_of(pjd.w)) - 1) * ntypes];
     const int pt = pg & PT_MASK;
@@ -1743,7 +1990,7 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 /
       const int ns = c.chunk_sys[nt_ * TILE / ATOM_ALIGN];
       if (ns >= 0) {
         const SysParam *Pn = c.P + ns;
-        const int rows = min(c.tile_rows[nt_], Pn->maxnb);
+        const int rows = list_words(min(c.tile_rows[nt_], Pn->maxnb), Pn->nb16);
         const int *src = c.nbr + Pn->nbr_off + (long long)((nt_ * TILE - Pn->atom_off) / TILE) *
                                                    Pn->maxnb * TILE;
         if (rows > 0) {
@@ -1772,6 +2019,7 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 /
           c.nbr + P->nbr_off + (long long)(local / TILE) * P->maxnb * TILE + g;
       int cnt = c.nnb[i];
       cnt = cnt < P->maxnb ? cnt : P->maxnb;
+      const int nb16 = P->nb16, aoff = P->atom_off;
       if (!MIXED) {
         const double4 pi = c.pos[i];
         ti = tw_type(tw_of(pi.w));
@@ -1786,7 +2034,7 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 /
 #pragma unroll
             for (int q = 0; q < UNR_D; ++q) {
               const int k = k0 + q * TPA;
-              qq[q] = k < cnt ? __ldg(nb + k * TILE) : -1;
+              qq[q] = k < cnt ? list_entry(nb, nb16, aoff, k) : -1;
             }
 #pragma unroll
             for (int q = 0; q < UNR_D; ++q) pj[q] = c.pos[qq[q] >= 0 ? qq[q] : i];
@@ -1846,9 +2094,19 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 /
           for (int m = la; m < nch; m += TPA) {
             const int kb = m * CHUNK;
             int qq[CHUNK];
+            if (nb16) {
+              // two 16-bit entries per word (CHUNK and kb are even)
 #pragma unroll
-            for (int q = 0; q < CHUNK; ++q)
-              qq[q] = kb + q < cnt ? ld_stream(nb + (kb + q) * TILE, lpol) : -1;
+              for (int q = 0; q < CHUNK; q += 2) {
+                const int w = kb + q < cnt ? ld_stream(nb + ((kb + q) >> 1) * TILE, lpol) : 0;
+                qq[q] = kb + q < cnt ? aoff + (w & 0xffff) : -1;
+                qq[q + 1] = kb + q + 1 < cnt ? aoff + (int)((unsigned)w >> 16) : -1;
+              }
+            } else {
+#pragma unroll
+              for (int q = 0; q < CHUNK; ++q)
+                qq[q] = kb + q < cnt ? ld_stream(nb + (kb + q) * TILE, lpol) : -1;
+            }
             float ax = 0.f, ay = 0.f, az = 0.f, ape = 0.f;
             float av0 = 0.f, av1 = 0.f, av2 = 0.f, av3 = 0.f, av4 = 0.f, av5 = 0.f;
             unsigned nm = 0;  // entries of this chunk within FP32 rounding of the cutoff
@@ -1908,7 +2166,7 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 /
               while (nm) {
                 const int q = __ffs(nm) - 1;
                 nm &= nm - 1;
-                const int j = __ldg(nb + (kb + q) * TILE);
+                const int j = list_entry(nb, nb16, aoff, kb + q);
                 const int4 pj = c.pfx[j];
                 const int pg = ONE ? 1 : pmr[(tw_type(pj.w) - 1) * ntypes];
                 const bool sym = ONE || pg < PT_ASYM;
@@ -2330,6 +2588,71 @@ void launch_integrate2(const DevCtx &c, cudaStream_t st, int ck) {
 }
 
 
+// The reference's NeiMax check (buildVerletList, src/nd.f90:1378,1421: STOP
+// 'too many neighbours in list'), for systems in the reference semantics:
+// each atom's half list as the reference builds it, the atoms of its own
+// cell with a larger index (input order, :1358) plus those of the 13
+// forward cells of getJcellNP (:1268-1300, folded periodically, so a grid
+// of two cells visits a cell more than once), counted with the reference's
+// FP64 test (:1362-1377, 1405-1420), must not exceed NeiMax.  The lists the
+// pair kernels use are the full ones k_build makes; this pass only counts.
+__device__ void neimax_chunk(const DevCtx &c, int sys, int chunk) {
+  const SysParam *__restrict__ P = c.P + sys;
+  if (P->neimax_stop <= 0) return;
+  SysState *S = c.S + sys;
+  const int i = chunk * ATOM_ALIGN + threadIdx.x;
+  if (i - P->atom_off >= P->n) return;
+  // the forward offsets of getJcellNP cases 2..14
+  const int fwd[13][3] = {{0, 0, 1}, {0, 1, 0},  {0, 1, -1},  {0, 1, 1},  {1, 0, 0},
+                          {1, 0, -1}, {1, 0, 1}, {1, 1, 0},   {1, 1, -1}, {1, 1, 1},
+                          {1, -1, 0}, {1, -1, -1}, {1, -1, 1}};
+  const int M0 = S->mcell[0], M1 = S->mcell[1], M2 = S->mcell[2];
+  const int cl = c.atom_cell[i];
+  const int cx = cl % M0, cy = (cl / M0) % M1, cz = cl / (M0 * M1);
+  const int *cst = c.cell_start + P->cell_off;
+  const int *pm = c.pairmat + P->pm_off;
+  const int nt = P->ntypes, gi = c.gid[i];
+  const double4 pi = c.pos[i];
+  const int ti = tw_type(tw_of(pi.w));
+  const double b0 = S->box[0], b1 = S->box[1], b2 = S->box[2], ptrmin = P->ptrmin;
+  int count = 0;
+  for (int k = -1; k < 13; ++k) {
+    const bool same = k < 0;
+    int nc = cl;
+    if (!same) {
+      const int nx = (cx + fwd[k][0] + M0) % M0, ny = (cy + fwd[k][1] + M1) % M1,
+                nz = (cz + fwd[k][2] + M2) % M2;
+      nc = nx + ny * M0 + nz * M0 * M1;
+    }
+    for (int q = cst[nc]; q < cst[nc + 1]; ++q) {
+      const int j = P->atom_off + q;
+      if (same && c.gid[j] <= gi) continue;
+      const double4 pj = c.pos[j];
+      const int tj = tw_type(tw_of(pj.w));
+      const int a = pm[(ti - 1) + (tj - 1) * nt], b = pm[(tj - 1) + (ti - 1) * nt];
+      const int mx = a > b ? a : b;
+      if (mx <= 0) continue;
+      double s0 = pi.x - pj.x, s1 = pi.y - pj.y, s2 = pi.z - pj.z;
+      s0 = s0 - round(s0);
+      s1 = s1 - round(s1);
+      s2 = s2 - round(s2);
+      const double x0 = b0 * s0, x1 = b1 * s1, x2 = b2 * s2;
+      double d2 = x0 * x0;
+      d2 = d2 + x1 * x1;
+      d2 = d2 + x2 * x2;
+      if (same && d2 < ptrmin) continue;
+      if (d2 > c.rlist2[P->pair_off + mx - 1]) continue;
+      ++count;
+    }
+  }
+  if (count > P->neimax_stop) set_err(c, S, E_NEIMAX);
+}
+
+__global__ __launch_bounds__(BLOCK) void k_neimax(DevCtx c) {
+  for_listed(c, [&](int s, int &f, int &n) { chunk_range(c, s, f, n); },
+             [&](int s, int u) { neimax_chunk(c, s, u); });
+}
+
 // the rebuild group over the systems on the rebuild list; `counting` adds
 // the rebuild to each system's NlistUpdates (not for the setup builds)
 void launch_rebuild(const DevCtx &c, cudaStream_t st, int counting, int mixed) {
@@ -2343,12 +2666,23 @@ void launch_rebuild(const DevCtx &c, cudaStream_t st, int counting, int mixed) {
   k_order<<<gcell, BLOCK, 0, st>>>(c);
   k_permute<<<gchunk, BLOCK, 0, st>>>(c);
   k_copyback<<<gchunk, BLOCK, 0, st>>>(c, mixed);
+  // the two forms of the list build; each returns at once unless the
+  // number of listed cells (counted by k_scan) selects it
   static int cfg = -1;
   if (c.nb_smem > cfg) {
     cudaFuncSetAttribute(k_build, cudaFuncAttributeMaxDynamicSharedMemorySize, c.nb_smem);
     cfg = c.nb_smem;
   }
   k_build<<<gtile, NBT, c.nb_smem, st>>>(c);
+  static int gcb = 0;
+  if (!gcb) {
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_build_cells, CB_THREADS, 0);
+    gcb = nsm * (occ > 0 ? occ : 1);
+  }
+  k_build_cells<<<gcb, CB_THREADS, 0, st>>>(c);
+  k_tile_rows<<<std::min(c.nchunks * (ATOM_ALIGN / TILE), nsm * 8), TILE, 0, st>>>(c);
+  if (c.any_neimax) k_neimax<<<gchunk, BLOCK, 0, st>>>(c);
 }
 
 void launch_arm(const DevCtx &c, cudaStream_t st, int nsys_cap, int sys, int nsteps, int start) {

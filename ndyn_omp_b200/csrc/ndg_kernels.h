@@ -33,6 +33,7 @@ struct DevCtx {
   int nb_vcap;  // flat candidate-list capacity of the build
   int gather;   // mixed pair loop: neighbour gathers in flight (4 or 8)
   int any_spring;  // some system holds spring pairs: the pair kernels' spring variant
+  int any_neimax;  // some system checks the reference's NeiMax after its list builds
   double4 *pos;
   int4 *pfx;
   double *vel, *acc, *disp, *force;

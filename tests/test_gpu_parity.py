@@ -406,6 +406,48 @@ def test_run_continue_equals_one_run(specs, prec):
     assert out[0][2] == out[1][2]
 
 
+@pytest.mark.parametrize("quirk", ["ref", "fixed"])
+def test_cell_build_equals_tile_build(quirk):
+    """The list build's two forms give every atom the same list in the same
+    order.  400 systems with 2, 3, 4 and 5 link cells per axis (22,400 cells)
+    take the cell form in their shared prologue; each alone takes the tile
+    form.  The sampled systems' pair multisets are equal, and so are their
+    mixed-precision states after a short run, whose fixed-point sums follow
+    the list order."""
+    rng = np.random.default_rng(81)
+    makers = [lambda k: W.cu_crystal(5, 900.0, seed=1000 + k, quirk=quirk),   # 2 cells per axis
+              lambda k: W.cu_crystal(6, 600.0, seed=2000 + k, quirk=quirk),   # 3
+              lambda k: W.cu_crystal(8, 300.0, seed=3000 + k, quirk=quirk),   # 4
+              lambda k: W.ar_liquid(9, 120.0, seed=4000 + k, quirk=quirk)]    # 5
+    many = []
+    for k in range(100):
+        for mk in makers:
+            sp = mk(k)
+            sp["pos"] = W.jitter(sp["pos"], sp["box"], 0.05, rng)
+            # the reference's own NeiMax estimate does not allow for the
+            # repeated cells of a 2-cell grid: a caller's NeiMax does
+            sp["control"] = dict(sp["control"], neimax=300)
+            many.append(sp)
+    sample = [0, 1, 2, 3, 201, 398, 399]
+    alone = {}
+    for k in sample:
+        with nd.Context(0, "mixed") as ctx:
+            sid = gpu_from_spec(ctx, many[k])
+            ctx.setup_lists()
+            alone[k] = (pair_multiset(ctx.neighbors(sid)), None)
+            ctx.run(5)
+            alone[k] = (alone[k][0], ctx.state(sid))
+    with nd.Context(0, "mixed") as ctx:
+        ids = [gpu_from_spec(ctx, sp) for sp in many]
+        ctx.setup_lists()
+        for k in sample:
+            assert np.array_equal(pair_multiset(ctx.neighbors(ids[k])), alone[k][0]), k
+        ctx.run(5)
+        for k in sample:
+            for a, b in zip(ctx.state(ids[k]), alone[k][1]):
+                assert np.array_equal(a, b), k
+
+
 def test_deterministic_repeat(specs):
     out = []
     for _ in range(2):
@@ -475,6 +517,44 @@ def test_autotune_restores_state(specs):
         assert np.array_equal(a, b)
     assert res[0][1] == res[1][1]
     assert res[0][2] == res[1][2]
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-10), ("mixed", 1e-6)])
+def test_autotune_skin(prec, tol):
+    """The rebuild-interval autotuner undoes its trial (the state is the same
+    bits afterwards), leaves reference-semantics systems' skins alone, keeps
+    the others within [0.5, 2] x their skin, and changes no physics: a run
+    after tuning follows an untuned run within the precision's tolerance
+    (only the list lengths and orders differ)."""
+    systems = [W.cu_crystal(7, 1500.0, seed=61, quirk="fixed"),
+               W.ar_liquid(7, 120.0, seed=62, quirk="fixed"),
+               W.cu_crystal(8, 100.0, seed=63, quirk="fixed"),
+               W.cu_crystal(6, 900.0, seed=64, quirk="ref")]
+    for sp in systems:
+        sp["control"] = dict(sp["control"], out_steps=10)
+    runs = []
+    for tune in (False, True):
+        with nd.Context(0, prec) as ctx:
+            ids = [gpu_from_spec(ctx, sp) for sp in systems]
+            ctx.run(20)
+            skins0 = [ctx.control(i).skin for i in ids]
+            if tune:
+                before = [ctx.state(i) for i in ids]
+                changed = ctx.autotune_skin(40)
+                for i, b in zip(ids, before):
+                    for x, y in zip(ctx.state(i), b):
+                        assert np.array_equal(x, y)
+                skins = [ctx.control(i).skin for i in ids]
+                assert skins[3] == skins0[3]  # reference semantics: untouched
+                for a, b in zip(skins, skins0):
+                    assert 0.5 * b - 1e-12 <= a <= 2.0 * b + 1e-12
+                assert changed == sum(a != b for a, b in zip(skins, skins0))
+            rows = ctx.run(60, cont=True)
+            runs.append(rows)
+    assert [(r["sys"], r["step"]) for r in runs[0]] == [(r["sys"], r["step"]) for r in runs[1]]
+    for a, b in zip(runs[0], runs[1]):
+        assert a["pe"] == pytest.approx(b["pe"], rel=tol)
+        assert a["ke"] == pytest.approx(b["ke"], rel=tol)
 
 
 @pytest.mark.parametrize("quirk", ["ref", "fixed"])
