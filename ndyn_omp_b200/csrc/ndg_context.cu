@@ -128,7 +128,6 @@ struct ndg_ctx {
   size_t cap_xoff = 0;        // caller's concatenated arrays (-1: not a live system)
   int *rb_list = nullptr;  // systems listed for a list rebuild
   PlanEnt *plan = nullptr;  // pair-launch work plan (integrate1's extra block)
-  int *build_ctr = nullptr;  // k_build's tile counter
   int *plan_kb = nullptr;
   PlanHdr *plan_hdr = nullptr;
   double *red = nullptr, *itop = nullptr, *ired = nullptr;
@@ -149,8 +148,6 @@ struct ndg_ctx {
   int any_neimax = 0;  // some system checks the reference's NeiMax at list builds
   int stab_smem = 0;  // staged-table bytes of the pair kernel (0: tables from global)
   int stab_lean = 0;  // the same without the energy table
-  int nb_smem = 0;  // neighbour-build dynamic smem
-  int nb_vcap = 4096;
   std::map<int, cudaGraphExec_t> graphs;
   int captures = 0;  // graphs captured (a changed arena or layout drops them)
   // per-kernel timing of the last profiled block
@@ -208,7 +205,6 @@ DevCtx devctx(ndg_ctx *c) {
   d.bcd = c->bcd;
   d.nbr = c->nbr;
   d.tile_rows = c->tile_rows;
-  d.nb_vcap = c->nb_vcap;
   d.gather = c->gather;
   d.any_spring = c->any_spring;
   d.any_neimax = c->any_neimax;
@@ -243,13 +239,11 @@ DevCtx devctx(ndg_ctx *c) {
   d.ring_count = c->ring_count;
   d.rb_list = c->rb_list;
   d.plan = c->plan;
-  d.build_ctr = c->build_ctr;
   d.plan_kb = c->plan_kb;
   d.plan_hdr = c->plan_hdr;
   d.ring_cap = c->ring_cap;
   d.stab_smem = c->stab_smem;
   d.stab_lean = c->stab_lean;
-  d.nb_smem = c->nb_smem;
   return d;
 }
 
@@ -341,7 +335,6 @@ int grow_sys(ndg_ctx *c, int n) {
   rc |= grow(c, c->plan, 0, 2 * (size_t)n);
   if (!c->plan_kb) rc |= grow(c, c->plan_kb, 0, 2 * (size_t)PLAN_GMAX);
   if (!c->plan_hdr) rc |= grow(c, c->plan_hdr, 0, 1);
-  if (!c->build_ctr) rc |= grow(c, c->build_ctr, 0, 1);
   if (rc) return NDG_ERR_NOMEM;
   drop_graphs(c);
   std::vector<SysParam> z(n - c->nsys_cap);
@@ -490,15 +483,6 @@ int upload_params(ndg_ctx *c) {
   if (stab != c->stab_smem || lean != c->stab_lean) {
     c->stab_smem = stab;
     c->stab_lean = lean;
-    drop_graphs(c);
-  }
-  // neighbour build: 3072 staged candidates (16 B position + 4 B slot each)
-  // and the runs' flat candidate lists (16-bit entries)
-  const int vcap = 4096;
-  const int nbs = 3072 * (16 + 4) + vcap * 2;
-  if (nbs != c->nb_smem) {
-    c->nb_smem = nbs;
-    c->nb_vcap = vcap;
     drop_graphs(c);
   }
   int rc = 0;
@@ -993,7 +977,7 @@ ndg_ctx::~ndg_ctx() {
   drop_graphs(this);
   void *ptrs[] = {dP, dS, chunk_sys, cell_sys, pos, s_pos, pfx, vel, acc, disp, force, s_vel,
                   s_acc, gid, s_gid, s_cell, nnb, hold, bcd, ipos, sprd, atom_cell, atom_slot, perm, tmp_src, tmp_key,
-                  cell_count, cell_start, rb_list, plan, plan_kb, plan_hdr, build_ctr, nbr, tile_rows, red, itop, ired, pairmat, pairg, mass, rc2, rlist2,
+                  cell_count, cell_start, rb_list, plan, plan_kb, plan_hdr, nbr, tile_rows, red, itop, ired, pairmat, pairg, mass, rc2, rlist2,
                   vdr2, rc2f, tabF, tabP, tabF2, tabP2, ring, ring_count};
   for (void *p : ptrs)
     if (p) cudaFree(p);

@@ -7,7 +7,8 @@
 //
 // Kernels of one MD step (src/nd.f90:137-178), all systems in one launch:
 //   [rebuild]  k_bin -> k_scan -> k_scatter -> k_order -> k_permute ->
-//              k_copyback -> k_build        (only systems whose check fired)
+//              k_copyback -> k_build_atoms | k_build_cells -> k_tile_rows
+//              [-> k_neimax]                (only systems whose check fired)
 //   k_integrate1                           (integrate1 + pending mkIso* scales;
 //                                           one more block plans the pair
 //                                           launches' shares of the systems)
@@ -784,7 +785,6 @@ __device__ void scan_system(const DevCtx &c, int s, int counting) {
 // exclusive scan of the cell counts, one listed system at a time per block
 __global__ __launch_bounds__(1024) void k_scan(DevCtx c, int counting) {
   const int nl = c.ring_count[3];
-  if (blockIdx.x == 0 && threadIdx.x == 0) *c.build_ctr = 0;  // k_build's work counter
   for (int k = blockIdx.x; k < nl; k += gridDim.x) {
     scan_system(c, c.rb_list[k], counting);
     __syncthreads();  // carry and wsum are reused by the next system
@@ -883,48 +883,23 @@ __global__ __launch_bounds__(BLOCK) void k_copyback(DevCtx c, int mixed) {
              [&](int s, int u) { copyback_chunk(c, s, u, mixed); });
 }
 
-// Neighbour build, one CTA per 128-atom tile (atoms are sorted by link cell,
-// so a tile covers a short run of cells).
-//   1. The cells its atoms' stencils reach are collected in a shared-memory
-//      hash set, sorted, and given candidate offsets by a block scan.
-//   2. The candidates are staged as 32-bit fixed-point positions; each run
-//      of own atoms in one cell gets one flat list of its stencil entries'
-//      candidates; a warp takes one own atom and tests 32 candidates per
-//      pass.  An FP32 distance decides every pair farther than a 1e-5
-//      relative margin from the cutoff (and from PTrMin); pairs inside the
-//      margin take the reference's exact FP64 test, so membership is
-//      bit-identical to buildVerletList (src/nd.f90:1356-1383 for the cell
-//      itself, :1403-1426 for the neighbour cells).
-//   3. Hits are compacted with __ballot_sync/__popc straight into the own
-//      atom's column of the blocked list (atom slots).
-// A tile whose cells or candidates do not fit the shared buffers takes
-// build_tile_direct (same test, same list order, no staging).
-constexpr int TC_MAX = 256;    // link cells a tile may stage
-constexpr int HSLOTS = 1024;   // shared hash slots for the tile's cell set
+// Neighbour build (buildVerletList, src/nd.f90:1328-1446).  An FP32
+// distance on the 32-bit fixed-point positions decides every candidate
+// farther than a 1e-5 relative margin from the list radius (and from PTrMin
+// in the atom's own cell); candidates inside the margin take the
+// reference's exact FP64 test, so membership is bit-identical to the
+// reference's.  Every atom's list holds its hits in stencil order, then
+// cell order.  Two forms share this test: a warp per atom (k_build_atoms,
+// rebuilds of few atoms: a step's few replicas) and a warp per link cell
+// (k_build_cells, many cells: a prologue, a large system); the number of
+// listed cells, counted by k_scan, picks one on the device.
 constexpr float NB_MARGIN = 1e-5f;
-// The list build takes one of two forms.  By tile (k_build): a CTA per
-// 128-atom tile, a warp per own atom testing 32 staged candidates at a time
-// (plenty of parallelism however few atoms are rebuilt: a step's few
-// replicas).  By cell (k_build_cells): a warp per link cell, a lane per own
-// atom, the cell's candidates broadcast one at a time (far fewer
-// instructions, but a long serial chain per warp, which only pays when every
-// warp has several cells: a prologue, a large system).  Both give every
-// atom the same list in the same order.
 constexpr int CELL_BUILD_MIN = 16384;  // listed cells from which the cell form builds
-constexpr int BUILD_CAP = 3072;  // candidates the build stages per tile
-constexpr int NBT = 256;         // threads of the build CTA (8 warps)
-
-__device__ __forceinline__ int stencil_cell(int cl, int st, int M0, int M1, int M2) {
-  const int cx = cl % M0, cy = (cl / M0) % M1, cz = cl / (M0 * M1);
-  const int dx = (st & 15) - 1, dy = ((st >> 4) & 15) - 1, dz = ((st >> 8) & 15) - 1;
-  const int nx = (cx + dx + M0) % M0, ny = (cy + dy + M1) % M1, nz = (cz + dz + M2) % M2;
-  return nx + ny * M0 + nz * M0 * M1;
-}
 
 // exclusive prefix sum of one int per thread over the whole block, in
 // thread order (wsum: one int per warp of shared scratch)
 __device__ __forceinline__ int block_excl_scan(int v, int *wsum) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int incl = v;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -936,501 +911,7 @@ __device__ __forceinline__ int block_excl_scan(int v, int *wsum) {
   __syncthreads();
   int before = 0;
   for (int w = 0; w < warp; ++w) before += wsum[w];
-  (void)nw;
   return before + incl - v;
-}
-
-__device__ __forceinline__ int find_cell(const int *ucell, int nu, int cell) {
-  int lo = 0, hi = nu - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (ucell[mid] < cell) lo = mid + 1;
-    else hi = mid;
-  }
-  return lo;
-}
-
-// The candidate test of the neighbour build for own atom i (double position
-// pid, fixed-point pi, type ti) and candidate j: FP32 distance on the
-// fixed-point positions, the reference's FP64 test within NB_MARGIN of the
-// list radius (or of PTrMin in the same cell), src/nd.f90:1356-1383,1403-1426.
-__device__ __forceinline__ bool nb_hit(const DevCtx &c, const SysParam *P, const int *pm,
-                                       const double4 &pid, const int4 &pi, int ti, int j,
-                                       bool center, float sb0, float sb1, float sb2, double b0,
-                                       double b1, double b2) {
-  const double4 pjd = c.pos[j];
-  const int4 pj = make_int4(fx32(pjd.x), fx32(pjd.y), fx32(pjd.z), tw_of(pjd.w));
-  const int nt = P->ntypes, tj = tw_type(pj.w);
-  const int a = pm[(ti - 1) + (tj - 1) * nt], b = pm[(tj - 1) + (ti - 1) * nt];
-  const int mx = a > b ? a : b;
-  if (mx <= 0) return false;
-  const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * sb0;
-  const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * sb1;
-  const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * sb2;
-  const float d2f = r0 * r0 + r1 * r1 + r2 * r2;
-  const double rl = c.rlist2[P->pair_off + mx - 1];
-  const float rlf = (float)rl;
-  const double ptrmin = P->ptrmin;
-  const float ptrlo = (float)ptrmin * (1.f - NB_MARGIN), ptrhi = (float)ptrmin * (1.f + NB_MARGIN);
-  const bool near_cut = fabsf(d2f - rlf) <= NB_MARGIN * rlf;
-  const bool near_min = center && d2f >= ptrlo && d2f <= ptrhi;
-  if (!(near_cut || near_min)) return !(center && d2f < ptrlo) && d2f < rlf;
-  double s0 = pid.x - pjd.x, s1 = pid.y - pjd.y, s2 = pid.z - pjd.z;
-  s0 = s0 - round(s0);
-  s1 = s1 - round(s1);
-  s2 = s2 - round(s2);
-  const double x0 = b0 * s0, x1 = b1 * s1, x2 = b2 * s2;
-  double d2 = x0 * x0;
-  d2 = d2 + x1 * x1;
-  d2 = d2 + x2 * x2;
-  return !(center && d2 < ptrmin) && !(d2 > rl);
-}
-
-// the reference's FP64 list test for one candidate (src/nd.f90:1362-1377,
-// 1419-1420): out of line, the build loop calls it only for the rare
-// candidates within NB_MARGIN of the list radius or of PTrMin
-__device__ __noinline__ bool nb_exact(const DevCtx &c, double4 pid, int j, bool center,
-                                      double rl, double ptrmin, double b0, double b1,
-                                      double b2) {
-  const double4 pjd = c.pos[j];
-  double s0 = pid.x - pjd.x, s1 = pid.y - pjd.y, s2 = pid.z - pjd.z;
-  s0 = s0 - round(s0);
-  s1 = s1 - round(s1);
-  s2 = s2 - round(s2);
-  const double x0 = b0 * s0, x1 = b1 * s1, x2 = b2 * s2;
-  double d2 = x0 * x0;
-  d2 = d2 + x1 * x1;
-  d2 = d2 + x2 * x2;
-  return !(center && d2 < ptrmin) && !(d2 > rl);
-}
-
-// Neighbour build of one tile without shared staging, for tiles whose cells
-// or candidates exceed the staged path's buffers (coarse cell grids, dense
-// or shrunk boxes): one warp per own atom walks its stencil cells in order,
-// reading candidates from global memory, with the same test and the same
-// list order (stencil entry, then cell order) as the staged path.
-__device__ __noinline__ void build_tile_direct(const DevCtx &c, int sys, int tile, const int *stc,
-                                               int ne, int *ncnt, int *rows_s) {
-  const SysParam *__restrict__ P = c.P + sys;
-  SysState *S = c.S + sys;
-  const int a0 = tile * TILE, local0 = a0 - P->atom_off;
-  const int nown = min(TILE, P->n - local0);
-  const int M0 = S->mcell[0], M1 = S->mcell[1], M2 = S->mcell[2];
-  const int maxnb = P->maxnb;
-  const int *cst = c.cell_start + P->cell_off;
-  const int *pm = c.pairmat + P->pm_off;
-  const double b0 = S->box[0], b1 = S->box[1], b2 = S->box[2];
-  const float sb0 = (float)(b0 * (1.0 / FX_ONE)), sb1 = (float)(b1 * (1.0 / FX_ONE)),
-              sb2 = (float)(b2 * (1.0 / FX_ONE));
-  int *dst = c.nbr + P->nbr_off + (long long)(local0 / TILE) * maxnb * TILE;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int t = warp; t < nown; t += NBT / 32) {
-    const int i = a0 + t;
-    const int cl = c.atom_cell[i];
-    const double4 pid = c.pos[i];
-    const int4 pi = make_int4(fx32(pid.x), fx32(pid.y), fx32(pid.z), tw_of(pid.w));
-    const int ti = tw_type(pi.w);
-    int cnt = 0;
-    for (int e = 0; e < ne; ++e) {
-      const int nc = stencil_cell(cl, stc[e], M0, M1, M2);
-      const bool center = (stc[e] >> 12) & 1;
-      const int s0 = cst[nc], s1 = cst[nc + 1];
-      for (int vb = s0; vb < s1; vb += 32) {
-        const int v = vb + lane;
-        const int j = P->atom_off + v;
-        const bool hit = v < s1 && j != i &&
-                         nb_hit(c, P, pm, pid, pi, ti, j, center, sb0, sb1, sb2, b0, b1, b2);
-        const unsigned bal = __ballot_sync(0xffffffffu, hit);
-        if (hit) {
-          const int k = cnt + __popc(bal & ((1u << lane) - 1u));
-          if (k < maxnb) list_store(dst + t, P->nb16, P->atom_off, k, j);
-        }
-        cnt += __popc(bal);
-      }
-    }
-    if (lane == 0) ncnt[t] = cnt;
-  }
-  if (threadIdx.x == 0) *rows_s = 0;
-  __syncthreads();
-  if (threadIdx.x < TILE) {
-    const int r = __reduce_max_sync(0xffffffffu,
-                                    (int)threadIdx.x < nown ? min(ncnt[threadIdx.x], maxnb) : 0);
-    if ((threadIdx.x & 31) == 0) atomicMax(rows_s, r);
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    c.tile_rows[tile] = *rows_s;
-    atomicAdd(&S->rows, (unsigned long long)*rows_s);
-  }
-  if (threadIdx.x < nown) {
-    c.nnb[a0 + threadIdx.x] = ncnt[threadIdx.x];
-    if (ncnt[threadIdx.x] > maxnb) set_err(c, S, E_NEIMAX);
-  }
-}
-
-// Squared distance from candidate pj to the box around a run's own atoms is
-// at most rl2.  The box is kept relative to the run's first atom (fixed
-// point, b[0..2]) as offset bounds b[3..5] (low) and b[6..8] (high): atoms
-// of one cell differ by far less than half the box, so their wrap-around
-// differences are exact even where the cell holds the atoms the reference's
-// anint places at +0.5.  A candidate's wrap-around difference from the
-// first atom is its minimum image while it lies within half a box of it,
-// which holds on link-cell grids of five or more cells per axis.
-__device__ __forceinline__ bool near_box(const int4 &pj, const int *b, float sb0, float sb1,
-                                         float sb2, float rl2) {
-  const int pv[3] = {pj.x, pj.y, pj.z};
-  const float sb[3] = {sb0, sb1, sb2};
-  float d2 = 0.f;
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    const int o = (int)((unsigned)pv[d] - (unsigned)b[d]);
-    const float gap = o < b[3 + d] ? (float)b[3 + d] - (float)o
-                                   : (o > b[6 + d] ? (float)o - (float)b[6 + d] : 0.f);
-    d2 = __fmaf_rn(gap * sb[d], gap * sb[d], d2);
-  }
-  return d2 <= rl2;
-}
-
-__device__ void build_tile(const DevCtx &c, int sys, int tile) {
-  extern __shared__ __align__(16) unsigned char dsm[];
-  __syncthreads();  // the block's previous tile is done with shared memory
-  const int a0 = tile * TILE;
-  const SysParam *__restrict__ P = c.P + sys;
-  SysState *S = c.S + sys;
-  const int local0 = a0 - P->atom_off;
-  const int nown = min(TILE, P->n - local0);
-  if (nown <= 0) {
-    if (threadIdx.x == 0) c.tile_rows[tile] = 0;
-    return;
-  }
-  const int M0 = S->mcell[0], M1 = S->mcell[1], M2 = S->mcell[2];
-  const int ne = S->nstencil;
-  const int maxnb = P->maxnb;
-  int4 *cpf = (int4 *)dsm;                                   // BUILD_CAP candidates
-  int *cgid = (int *)(cpf + BUILD_CAP);                       // their atom slots
-  unsigned short *vlist = (unsigned short *)(cgid + BUILD_CAP);  // flat per-run lists
-  const int vcap = c.nb_vcap;
-  __shared__ int hset[HSLOTS];
-  __shared__ int ucell[TC_MAX + 1], coff[TC_MAX + 1], ustart[TC_MAX];
-  __shared__ int stc[MAX_STENCIL];
-  __shared__ int ncnt[TILE];
-  __shared__ short run_of[TILE];               // own atom -> run of equal cells
-  __shared__ int run_cell[TILE];
-  __shared__ short ent_u[TILE * MAX_STENCIL];  // run x stencil entry -> staged cell
-  __shared__ int rbox[TILE][9];                // run -> box of its own atoms (first atom, offsets)
-  __shared__ int vsize[TILE], vstart[TILE], run_t0[TILE + 1];
-  __shared__ int nu, bad, nruns, rows_s;
-  __shared__ int pm_s[16 * 16];
-  __shared__ int scan_w[NBT / 32];
-  __shared__ float2 rlb_s[136];  // FP32 band (1 -+ NB_MARGIN) of each pair's rlist^2
-  __shared__ double rl2_s[136];
-  const int nt = P->ntypes, npr = P->npairs;
-  const bool small = nt <= 16 && npr <= 136;
-  const int *cst = c.cell_start + P->cell_off;
-  for (int k = threadIdx.x; k < HSLOTS; k += NBT) hset[k] = -1;
-  if (threadIdx.x < ne) stc[threadIdx.x] = S->stencil[threadIdx.x];
-  if (threadIdx.x == 0) {
-    nu = 0;
-    bad = 0;
-  }
-  if (small) {
-    for (int k = threadIdx.x; k < nt * nt; k += NBT) pm_s[k] = c.pairmat[P->pm_off + k];
-    for (int k = threadIdx.x; k < npr; k += NBT) {
-      rl2_s[k] = c.rlist2[P->pair_off + k];
-      const float r = (float)rl2_s[k];
-      rlb_s[k] = make_float2(r * (1.f - NB_MARGIN), r * (1.f + NB_MARGIN));
-    }
-  }
-  __syncthreads();
-  // 1. the set of cells the tile's stencils reach
-  {
-    const int t = threadIdx.x;
-    if (t < nown) {
-      const int cl = c.atom_cell[a0 + t];
-      if (t == 0 || cl != c.atom_cell[a0 + t - 1]) {
-        for (int e = 0; e < ne; ++e) {
-          const int nc = stencil_cell(cl, stc[e], M0, M1, M2);
-          int h = (nc * 2654435761u) & (HSLOTS - 1);
-          for (int probe = 0; probe < HSLOTS; ++probe) {
-            const int prev = atomicCAS(&hset[h], -1, nc);
-            if (prev == -1) {
-              atomicAdd(&nu, 1);
-              break;
-            }
-            if (prev == nc) break;
-            h = (h + 1) & (HSLOTS - 1);
-          }
-        }
-      }
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x == 0 && nu >= TC_MAX) bad = 1;  // the scan below sets coff[nu] by thread nu
-  __syncthreads();
-  if (!bad) {
-    // compact and sort the cell ids (bitonic over TC_MAX slots)
-    __shared__ int cursor;
-    if (threadIdx.x == 0) cursor = 0;
-    for (int k = threadIdx.x; k < TC_MAX; k += NBT) ucell[k] = 0x7fffffff;
-    __syncthreads();
-    for (int k = threadIdx.x; k < HSLOTS; k += NBT)
-      if (hset[k] >= 0) ucell[atomicAdd(&cursor, 1)] = hset[k];
-    __syncthreads();
-    for (int size = 2; size <= TC_MAX; size <<= 1)
-      for (int stride = size >> 1; stride > 0; stride >>= 1) {
-        for (int k = threadIdx.x; k < TC_MAX; k += NBT) {
-          const int p = k ^ stride;
-          if (p > k) {
-            const bool up = (k & size) == 0;
-            const int a = ucell[k], b = ucell[p];
-            if ((a > b) == up) {
-              ucell[k] = b;
-              ucell[p] = a;
-            }
-          }
-        }
-        __syncthreads();
-      }
-    // each staged cell's first atom and length, read in parallel; an
-    // exclusive scan of the lengths gives the candidate offsets
-    int len = 0;
-    if (threadIdx.x < nu) {
-      const int s0 = cst[ucell[threadIdx.x]];
-      ustart[threadIdx.x] = s0;
-      len = cst[ucell[threadIdx.x] + 1] - s0;
-    }
-    const int pre = block_excl_scan(len, scan_w);
-    if ((int)threadIdx.x <= nu) coff[threadIdx.x] = pre;  // coff[nu] = all candidates
-    if ((int)threadIdx.x == nu && pre > BUILD_CAP) bad = 1;
-  }
-  __syncthreads();
-  if (bad) {
-    // more cells or candidates than the shared buffers hold
-    build_tile_direct(c, sys, tile, stc, ne, ncnt, &rows_s);
-    return;
-  }
-  const int U = nu, C = coff[nu];
-  // 2. stage the candidates
-  for (int u = threadIdx.x >> 5; u < U; u += NBT / 32) {
-    const int q0 = coff[u], len = coff[u + 1] - q0;
-    const int j0 = P->atom_off + ustart[u];
-    for (int e = threadIdx.x & 31; e < len; e += 32) {
-      const double4 p = c.pos[j0 + e];
-      cpf[q0 + e] = make_int4(fx32(p.x), fx32(p.y), fx32(p.z), tw_of(p.w));
-      cgid[q0 + e] = j0 + e;
-    }
-  }
-  __syncthreads();
-  const int *pm = small ? pm_s : c.pairmat + P->pm_off;
-  const double b0 = S->box[0], b1 = S->box[1], b2 = S->box[2];
-  const float sb0 = (float)(b0 * (1.0 / FX_ONE)), sb1 = (float)(b1 * (1.0 / FX_ONE)),
-              sb2 = (float)(b2 * (1.0 / FX_ONE));
-  const double ptrmin = P->ptrmin;
-  const float ptrlo = (float)ptrmin * (1.f - NB_MARGIN), ptrhi = (float)ptrmin * (1.f + NB_MARGIN);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  // runs of equal own cells (the atoms are sorted by cell): a run starts
-  // where the cell changes; its index is the number of starts before it
-  {
-    const int t = threadIdx.x;
-    int cl = -1, head = 0;
-    if (t < nown) {
-      cl = c.atom_cell[a0 + t];
-      head = t == 0 || cl != c.atom_cell[a0 + t - 1];
-    }
-    const int pre = block_excl_scan(head, scan_w);
-    if (t < nown) {
-      if (head) {
-        run_cell[pre] = cl;
-        run_t0[pre] = t;
-      }
-      run_of[t] = (short)(pre + head - 1);
-    }
-    if (t == nown) {
-      nruns = pre;
-      run_t0[pre] = nown;
-    }
-  }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < nruns * ne; idx += NBT) {
-    const int r = idx / ne, e = idx - r * ne;
-    ent_u[r * MAX_STENCIL + e] =
-        (short)find_cell(ucell, U, stencil_cell(run_cell[r], stc[e], M0, M1, M2));
-  }
-  __syncthreads();
-  // Each run's candidates as one flat list: its stencil entries' staged
-  // ranges back to back, in stencil order (entries repeat where the
-  // reference's half stencil reaches a cell twice), bit 15 marking the run's
-  // own cell (PTrMin test).  On grids of five or more cells per axis a
-  // candidate farther than the list radius from the box around the run's
-  // own atoms is left out: it cannot be a neighbour of any of them, so the
-  // lists are unchanged and each own atom tests fewer candidates.
-  const bool prune = M0 >= 5 && M1 >= 5 && M2 >= 5;
-  const float rl2box = (float)(P->rlist * P->rlist) * (1.f + 4.f * NB_MARGIN);
-  const float sbx = (float)(S->box[0] * (1.0 / FX_ONE)), sby = (float)(S->box[1] * (1.0 / FX_ONE)),
-              sbz = (float)(S->box[2] * (1.0 / FX_ONE));
-  if (prune) {
-    for (int r = threadIdx.x; r < nruns; r += NBT) {
-      const double4 p = c.pos[a0 + run_t0[r]];
-      rbox[r][0] = fx32(p.x);
-      rbox[r][1] = fx32(p.y);
-      rbox[r][2] = fx32(p.z);
-      rbox[r][3] = rbox[r][4] = rbox[r][5] = 0;
-      rbox[r][6] = rbox[r][7] = rbox[r][8] = 0;
-    }
-    __syncthreads();
-    if (threadIdx.x < nown) {
-      const double4 p = c.pos[a0 + threadIdx.x];
-      const int f[3] = {fx32(p.x), fx32(p.y), fx32(p.z)};
-      const int r = run_of[threadIdx.x];
-      for (int d = 0; d < 3; ++d) {
-        const int o = (int)((unsigned)f[d] - (unsigned)rbox[r][d]);
-        atomicMin(&rbox[r][3 + d], o);
-        atomicMax(&rbox[r][6 + d], o);
-      }
-    }
-    __syncthreads();
-  }
-  // pass 1: each run's list length (a warp per run)
-  for (int r = warp; r < nruns; r += NBT / 32) {
-    int kept = 0;
-    for (int e = 0; e < ne; ++e) {
-      const int u = ent_u[r * MAX_STENCIL + e];
-      const int q0 = coff[u], len = coff[u + 1] - q0;
-      if (!prune) {
-        kept += len;
-        continue;
-      }
-      for (int kb = 0; kb < len; kb += 32) {
-        const int k = kb + lane;
-        const bool keep = k < len && near_box(cpf[q0 + k], rbox[r], sbx, sby, sbz, rl2box);
-        kept += __popc(__ballot_sync(0xffffffffu, keep));
-      }
-    }
-    if (lane == 0) vsize[r] = kept;
-  }
-  __syncthreads();
-  const int *__restrict__ pmg = pm;
-  const bool one = nt == 1 && npr == 1 && pm[0] == 1;
-  const float2 band1 = one ? rlb_s[0] : make_float2(0.f, 0.f);
-  int *dst = c.nbr + P->nbr_off + (long long)(local0 / TILE) * maxnb * TILE;
-  const int nb16 = P->nb16, aoff = P->atom_off;
-  for (int rb = 0; rb < nruns;) {
-    // the runs whose lists fit the buffer together
-    __shared__ int re_s;
-    if (threadIdx.x == 0) {
-      int re = rb, tot = 0;
-      while (re < nruns && tot + vsize[re] <= vcap) {
-        vstart[re] = tot;
-        tot += vsize[re];
-        ++re;
-      }
-      re_s = re;
-      if (re == rb) bad = 1;  // one run alone exceeds the buffer
-    }
-    __syncthreads();
-    if (bad) break;
-    const int re = re_s;
-    // pass 2: the runs' lists, compacted in order (a warp per run)
-    for (int r = rb + warp; r < re; r += NBT / 32) {
-      unsigned short *vd = vlist + vstart[r];
-      int at = 0;
-      for (int e = 0; e < ne; ++e) {
-        const int u = ent_u[r * MAX_STENCIL + e];
-        const int q0 = coff[u], len = coff[u + 1] - q0;
-        const unsigned short cflag = ((stc[e] >> 12) & 1) ? 0x8000u : 0u;
-        for (int kb = 0; kb < len; kb += 32) {
-          const int k = kb + lane;
-          const bool keep =
-              k < len && (!prune || near_box(cpf[q0 + k], rbox[r], sbx, sby, sbz, rl2box));
-          const unsigned bal = __ballot_sync(0xffffffffu, keep);
-          if (keep) vd[at + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)(q0 + k) | cflag;
-          at += __popc(bal);
-        }
-      }
-    }
-    __syncthreads();
-    // 3. one warp per own atom, 32 candidates of the flat list per pass;
-    // hits go straight to the atom's column of the blocked list
-    for (int t = run_t0[rb] + warp; t < run_t0[re]; t += NBT / 32) {
-      const int i = a0 + t;
-      const int r = run_of[t];
-      const double4 pid = c.pos[i];
-      const int4 pi = make_int4(fx32(pid.x), fx32(pid.y), fx32(pid.z), tw_of(pid.w));
-      const int ti = tw_type(pi.w);
-      const unsigned short *vl = vlist + vstart[r];
-      const int V = vsize[r];
-      int cnt = 0;
-      for (int vb = 0; vb < V; vb += 32) {
-        const int v = vb + lane;
-        bool hit = false, unsure = false, center = false;
-        int q = 0, mx = 1;
-        if (v < V) {
-          const unsigned short raw = vl[v];
-          q = raw & 0x7fff;
-          center = raw >> 15;
-          const int4 pj = cpf[q];
-          if (!one) {
-            const int tj = tw_type(pj.w);
-            const int a = pmg[(ti - 1) + (tj - 1) * nt];
-            const int b = pmg[(tj - 1) + (ti - 1) * nt];
-            mx = a > b ? a : b;
-          }
-          const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * sb0;
-          const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * sb1;
-          const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * sb2;
-          const float d2f = r0 * r0 + r1 * r1 + r2 * r2;
-          const bool live = cgid[q] != i && mx > 0;
-          float2 band = band1;
-          if (!one && live) {
-            if (small) {
-              band = rlb_s[mx - 1];
-            } else {
-              const float rf = (float)c.rlist2[P->pair_off + mx - 1];
-              band = make_float2(rf * (1.f - NB_MARGIN), rf * (1.f + NB_MARGIN));
-            }
-          }
-          // outside both margins FP32 decides; inside either, FP64 does
-          hit = live && d2f < band.x && !(center && d2f < ptrhi);
-          unsure = live && ((d2f >= band.x && d2f <= band.y) ||
-                            (center && d2f >= ptrlo && d2f <= ptrhi));
-        }
-        if (__any_sync(0xffffffffu, unsure) && unsure) {
-          const double rl = small ? rl2_s[mx - 1] : c.rlist2[P->pair_off + mx - 1];
-          hit = nb_exact(c, pid, cgid[q], center, rl, ptrmin, b0, b1, b2);
-        }
-        const unsigned bal = __ballot_sync(0xffffffffu, hit);
-        if (hit) {
-          const int k = cnt + __popc(bal & ((1u << lane) - 1u));
-          if (k < maxnb) list_store(dst + t, nb16, aoff, k, cgid[q]);
-        }
-        cnt += __popc(bal);
-      }
-      if (lane == 0) ncnt[t] = cnt;
-    }
-    __syncthreads();
-    rb = re;
-  }
-  if (bad) {
-    // a run's candidate list is longer than the flat buffer
-    build_tile_direct(c, sys, tile, stc, ne, ncnt, &rows_s);
-    return;
-  }
-  // 4. the tile's row count (longest list) and each atom's count
-  if (threadIdx.x == 0) rows_s = 0;
-  __syncthreads();
-  if (threadIdx.x < TILE) {
-    const int r = __reduce_max_sync(0xffffffffu, (int)threadIdx.x < nown ? min(ncnt[threadIdx.x], maxnb) : 0);
-    if ((threadIdx.x & 31) == 0) atomicMax(&rows_s, r);
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    c.tile_rows[tile] = rows_s;
-    atomicAdd(&S->rows, (unsigned long long)rows_s);
-  }
-  if (threadIdx.x < nown) {
-    c.nnb[a0 + threadIdx.x] = ncnt[threadIdx.x];
-    if (ncnt[threadIdx.x] > maxnb) set_err(c, S, E_NEIMAX);
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1441,7 +922,7 @@ __device__ void build_tile(const DevCtx &c, int sys, int tile) {
 // lane tests each against its own atom and appends the hits to its own
 // column of the blocked list.  Each list thus has the order of the
 // reference's cell walk (stencil entry, then cell order), and the candidate
-// test is the tile build's: FP32 on the fixed-point positions outside a
+// test is the shared one above: FP32 on the fixed-point positions outside a
 // 1e-5 band around the list radius and PTrMin, the reference's FP64 test
 // inside it.  A candidate costs the warp one broadcast load and one test
 // for all 32 atoms of the cell at once.
@@ -1582,12 +1063,144 @@ __device__ __forceinline__ void build_cell(const DevCtx &c, int sys, int cell, i
   }
 }
 
+// Neighbour build by atom, for rebuilds of few atoms (a step's rebuilds of
+// a few replicas): one warp per own atom, 32 candidates of a stencil cell at
+// a time (one coalesced load of their fixed-point positions, a lane each),
+// hits compacted with __ballot_sync/__popc into the atom's column in
+// stencil order, then cell order, the order of the other two forms.  No
+// shared staging and no barriers, so every warp of the grid works on its
+// own atom; the test is theirs (FP32 outside the 1e-5 band, the
+// reference's FP64 test inside it).
+__device__ __forceinline__ void build_atom(const DevCtx &c, int sys, int local, int lane) {
+  const SysParam *__restrict__ P = c.P + sys;
+  SysState *S = c.S + sys;
+  const int aoff = P->atom_off, i = aoff + local;
+  const int *cst = c.cell_start + P->cell_off;
+  const int ne = S->nstencil;
+  int e_q0 = 0, e_q1 = 0, e_center = 0;  // lane e < ne: stencil entry e
+  if (lane < ne) {
+    const int M0 = S->mcell[0], M1 = S->mcell[1], M2 = S->mcell[2];
+    const int cl = c.atom_cell[i];
+    const int cx = cl % M0, cy = (cl / M0) % M1, cz = cl / (M0 * M1);
+    const int st = S->stencil[lane];
+    const int nc = wrap_step(cx, (st & 15) - 1, M0) +
+                   (wrap_step(cy, ((st >> 4) & 15) - 1, M1) +
+                    wrap_step(cz, ((st >> 8) & 15) - 1, M2) * M1) * M0;
+    e_q0 = cst[nc];
+    e_q1 = cst[nc + 1];
+    e_center = (st >> 12) & 1;
+  }
+  const int nt = P->ntypes, maxnb = P->maxnb, nb16 = P->nb16;
+  const int *pm = c.pairmat + P->pm_off;
+  const double *rl2 = c.rlist2 + P->pair_off;
+  const float sb0 = (float)(S->box[0] * (1.0 / FX_ONE)), sb1 = (float)(S->box[1] * (1.0 / FX_ONE)),
+              sb2 = (float)(S->box[2] * (1.0 / FX_ONE));
+  const float ptrlo = (float)P->ptrmin * (1.f - NB_MARGIN),
+              ptrhi = (float)P->ptrmin * (1.f + NB_MARGIN);
+  const bool one = nt == 1 && P->npairs == 1 && pm[0] == 1;
+  const float rf1 = (float)rl2[0];
+  const float2 band1 = make_float2(rf1 * (1.f - NB_MARGIN), rf1 * (1.f + NB_MARGIN));
+  const int4 pi = c.pfx[i];
+  const int ti = tw_type(pi.w);
+  int *col = c.nbr + P->nbr_off + (long long)(local / TILE) * maxnb * TILE + (local % TILE);
+  const unsigned below = (1u << lane) - 1u;
+  int cnt = 0;
+  for (int e = 0; e < ne; ++e) {
+    const bool center = __shfl_sync(0xffffffffu, e_center, e) != 0;
+    const int q1 = __shfl_sync(0xffffffffu, e_q1, e);
+    for (int qb = __shfl_sync(0xffffffffu, e_q0, e); qb < q1; qb += 32) {
+      const int qq = qb + lane;
+      const int j = aoff + qq;
+      const bool have = qq < q1;
+      const int4 pj = c.pfx[have ? j : i];
+      int mx = 1;
+      if (!one) {
+        const int tj = tw_type(pj.w);
+        const int a = pm[(ti - 1) + (tj - 1) * nt], b = pm[(tj - 1) + (ti - 1) * nt];
+        mx = a > b ? a : b;
+      }
+      const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * sb0;
+      const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * sb1;
+      const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * sb2;
+      const float d2f = r0 * r0 + r1 * r1 + r2 * r2;
+      const bool live = have && j != i && mx > 0;
+      float2 band = band1;
+      if (!one && live) {
+        const float rf = (float)rl2[mx - 1];
+        band = make_float2(rf * (1.f - NB_MARGIN), rf * (1.f + NB_MARGIN));
+      }
+      // outside both margins FP32 decides; inside either, FP64 does
+      bool hit = live && d2f < band.x && !(center && d2f < ptrhi);
+      const bool unsure = live && ((d2f >= band.x && d2f <= band.y) ||
+                                   (center && d2f >= ptrlo && d2f <= ptrhi));
+      if (__any_sync(0xffffffffu, unsure) && unsure) {
+        // the reference's FP64 test (src/nd.f90:1362-1377, 1419-1420)
+        const double4 pid = c.pos[i], pjd = c.pos[j];
+        double s0 = pid.x - pjd.x, s1 = pid.y - pjd.y, s2 = pid.z - pjd.z;
+        s0 = s0 - round(s0);
+        s1 = s1 - round(s1);
+        s2 = s2 - round(s2);
+        const double x0 = S->box[0] * s0, x1 = S->box[1] * s1, x2 = S->box[2] * s2;
+        double d2 = x0 * x0;
+        d2 = d2 + x1 * x1;
+        d2 = d2 + x2 * x2;
+        hit = !(center && d2 < P->ptrmin) && !(d2 > rl2[mx - 1]);
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, hit);
+      if (hit) {
+        const int k = cnt + __popc(bal & below);
+        if (k < maxnb) list_store(col, nb16, aoff, k, j);
+      }
+      cnt += __popc(bal);
+    }
+  }
+  if (lane == 0) {
+    c.nnb[i] = cnt;
+    if (cnt > maxnb) set_err(c, S, E_NEIMAX);
+  }
+}
+
+// the listed systems' atoms, dealt round-robin to every warp of the grid
+__global__ __launch_bounds__(CB_THREADS, 4) void k_build_atoms(DevCtx c) {
+  __shared__ int l_sys[LIST_STAGE], l_pre[LIST_STAGE + 1];
+  __shared__ int wsum[CB_THREADS / 32];
+  if (c.ring_count[2] >= CELL_BUILD_MIN) return;  // many cells: the cell form builds
+  const int n = c.ring_count[3];
+  const int lane = threadIdx.x & 31;
+  const int nw = gridDim.x * (CB_THREADS / 32);
+  const int gw = blockIdx.x * (CB_THREADS / 32) + (threadIdx.x >> 5);
+  for (int k0 = 0; k0 < n; k0 += LIST_STAGE) {
+    const int m = min(LIST_STAGE, n - k0);
+    __syncthreads();  // the previous group's entries are no longer read
+    int cnt = 0;
+    if ((int)threadIdx.x < m) {
+      const int s = c.rb_list[k0 + threadIdx.x];
+      l_sys[threadIdx.x] = s;
+      cnt = c.P[s].n;
+    }
+    const int pre = block_excl_scan(cnt, wsum);
+    if ((int)threadIdx.x < m) l_pre[threadIdx.x] = pre;
+    if ((int)threadIdx.x == m - 1) l_pre[m] = pre + cnt;
+    __syncthreads();
+    const int total = l_pre[m];
+    for (int u = gw; u < total; u += nw) {
+      int lo = 0, hi = m - 1;  // the listed system whose atoms hold unit u
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (l_pre[mid] <= u) lo = mid;
+        else hi = mid - 1;
+      }
+      build_atom(c, l_sys[lo], u - l_pre[lo], lane);
+    }
+  }
+}
+
 // the listed systems' cells, dealt round-robin to every warp of the grid
 __global__ __launch_bounds__(CB_THREADS, 3) void k_build_cells(DevCtx c) {
   __shared__ int l_sys[LIST_STAGE], l_pre[LIST_STAGE + 1];
   __shared__ int wsum[CB_THREADS / 32];
   static_assert(CB_THREADS == LIST_STAGE, "one listed system per thread when staging");
-  if (c.ring_count[2] < CELL_BUILD_MIN) return;  // few cells: the tile build takes them
+  if (c.ring_count[2] < CELL_BUILD_MIN) return;  // few cells: the atom form builds
   const int n = c.ring_count[3];
   const int lane = threadIdx.x & 31;
   const int nw = gridDim.x * (CB_THREADS / 32);
@@ -1622,7 +1235,6 @@ __global__ __launch_bounds__(CB_THREADS, 3) void k_build_cells(DevCtx c) {
 // prefetch) and the system's sum of them (the work plan's tile cost)
 __global__ __launch_bounds__(TILE) void k_tile_rows(DevCtx c) {
   __shared__ int wmax[TILE / 32];
-  if (c.ring_count[2] < CELL_BUILD_MIN) return;  // the tile build counted its own rows
   for_listed(c,
              [&](int s, int &f, int &n) {
                f = c.P[s].atom_off / TILE;
@@ -1643,50 +1255,6 @@ __global__ __launch_bounds__(TILE) void k_tile_rows(DevCtx c) {
                }
                __syncthreads();
              });
-}
-
-// A short rebuild list (a step's rebuilds: a few tiles per block) takes its
-// tiles from a work counter, so that blocks that draw cheap tiles take more
-// of them; a long one (a prologue build) is dealt round-robin.
-__global__ __launch_bounds__(NBT, 2) void k_build(DevCtx c) {
-  if (c.ring_count[2] >= CELL_BUILD_MIN) return;  // many cells: the cell build takes them
-  const int n = c.ring_count[3];
-  if (n >= NBT) {  // (thread n writes the total below)
-    for_listed(c,
-               [&](int s, int &f, int &n) {
-                 f = c.P[s].atom_off / TILE;
-                 n = c.P[s].npad / TILE;
-               },
-               [&](int s, int u) { build_tile(c, s, u); });
-    return;
-  }
-  __shared__ int l_sys[NBT], l_first[NBT], l_pre[NBT + 1];
-  __shared__ int wsum[NBT / 32], unit_s;
-  int cnt = 0;
-  if ((int)threadIdx.x < n) {
-    const int s = c.rb_list[threadIdx.x];
-    l_sys[threadIdx.x] = s;
-    l_first[threadIdx.x] = c.P[s].atom_off / TILE;
-    cnt = c.P[s].npad / TILE;
-  }
-  const int pre = block_excl_scan(cnt, wsum);
-  if ((int)threadIdx.x <= n) l_pre[threadIdx.x] = pre;  // l_pre[n]: all tiles
-  __syncthreads();
-  const int total = l_pre[n];
-  for (;;) {
-    if (threadIdx.x == 0) unit_s = atomicAdd(c.build_ctr, 1);
-    __syncthreads();
-    const int u = unit_s;
-    __syncthreads();  // every thread has read the unit before the next draw
-    if (u >= total) break;
-    int lo = 0, hi = n - 1;  // the entry whose tiles hold unit u
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (l_pre[mid] <= u) lo = mid;
-      else hi = mid - 1;
-    }
-    build_tile(c, l_sys[lo], l_first[lo] + (u - l_pre[lo]));
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -2595,7 +2163,7 @@ void launch_integrate2(const DevCtx &c, cudaStream_t st, int ck) {
 // forward cells of getJcellNP (:1268-1300, folded periodically, so a grid
 // of two cells visits a cell more than once), counted with the reference's
 // FP64 test (:1362-1377, 1405-1420), must not exceed NeiMax.  The lists the
-// pair kernels use are the full ones k_build makes; this pass only counts.
+// pair kernels use are the full ones the build makes; this pass only counts.
 __device__ void neimax_chunk(const DevCtx &c, int sys, int chunk) {
   const SysParam *__restrict__ P = c.P + sys;
   if (P->neimax_stop <= 0) return;
@@ -2659,7 +2227,6 @@ void launch_rebuild(const DevCtx &c, cudaStream_t st, int counting, int mixed) {
   const int nsm = sm_count();
   const int gchunk = std::min(c.nchunks, nsm * 4);
   const int gcell = std::min((c.ncells + BLOCK / 32 - 1) / (BLOCK / 32), nsm * 4);
-  const int gtile = std::min(c.nchunks * (ATOM_ALIGN / TILE), nsm * 2);
   k_bin<<<gchunk, BLOCK, 0, st>>>(c);
   k_scan<<<std::min(c.nsys_cap, nsm), 1024, 0, st>>>(c, counting);
   k_scatter<<<gchunk, BLOCK, 0, st>>>(c);
@@ -2668,12 +2235,13 @@ void launch_rebuild(const DevCtx &c, cudaStream_t st, int counting, int mixed) {
   k_copyback<<<gchunk, BLOCK, 0, st>>>(c, mixed);
   // the two forms of the list build; each returns at once unless the
   // number of listed cells (counted by k_scan) selects it
-  static int cfg = -1;
-  if (c.nb_smem > cfg) {
-    cudaFuncSetAttribute(k_build, cudaFuncAttributeMaxDynamicSharedMemorySize, c.nb_smem);
-    cfg = c.nb_smem;
+  static int gab = 0;
+  if (!gab) {
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_build_atoms, CB_THREADS, 0);
+    gab = nsm * (occ > 0 ? occ : 1);
   }
-  k_build<<<gtile, NBT, c.nb_smem, st>>>(c);
+  k_build_atoms<<<gab, CB_THREADS, 0, st>>>(c);
   static int gcb = 0;
   if (!gcb) {
     int occ = 0;

@@ -29,8 +29,6 @@ struct DevCtx {
   int nchunks, ncells, nsys_cap;
   int stab_smem;  // shared-memory bytes of the staged pair tables, 0 = read from global
   int stab_lean;  // the same without the energy table (kernel without energy/virial)
-  int nb_smem;  // neighbour build dynamic smem
-  int nb_vcap;  // flat candidate-list capacity of the build
   int gather;   // mixed pair loop: neighbour gathers in flight (4 or 8)
   int any_spring;  // some system holds spring pairs: the pair kernels' spring variant
   int any_neimax;  // some system checks the reference's NeiMax after its list builds
@@ -63,7 +61,6 @@ struct DevCtx {
   int *ring_count;  // [0] records written, [1] error bits of any system,
                     // [2] largest tile candidate count, [3] systems on rb_list
   int *rb_list;     // systems whose lists the next rebuild group rebuilds
-  int *build_ctr;   // k_build's tile counter (reset by k_scan)
   PlanEnt *plan;    // 2 x nsys_cap entries
   int *plan_kb;     // 2 x PLAN_GMAX block starts
   PlanHdr *plan_hdr;
