@@ -1079,16 +1079,37 @@ __device__ __forceinline__ void build_atom(const DevCtx &c, int sys, int local, 
   const int ne = S->nstencil;
   int e_q0 = 0, e_q1 = 0, e_center = 0;  // lane e < ne: stencil entry e
   if (lane < ne) {
-    const int M0 = S->mcell[0], M1 = S->mcell[1], M2 = S->mcell[2];
+    const int M[3] = {S->mcell[0], S->mcell[1], S->mcell[2]};
     const int cl = c.atom_cell[i];
-    const int cx = cl % M0, cy = (cl / M0) % M1, cz = cl / (M0 * M1);
+    const int cv[3] = {cl % M[0], (cl / M[0]) % M[1], cl / (M[0] * M[1])};
     const int st = S->stencil[lane];
-    const int nc = wrap_step(cx, (st & 15) - 1, M0) +
-                   (wrap_step(cy, ((st >> 4) & 15) - 1, M1) +
-                    wrap_step(cz, ((st >> 8) & 15) - 1, M2) * M1) * M0;
+    int nv[3];
+    for (int d = 0; d < 3; ++d) nv[d] = wrap_step(cv[d], ((st >> (4 * d)) & 15) - 1, M[d]);
+    const int nc = nv[0] + (nv[1] + nv[2] * M[1]) * M[0];
     e_q0 = cst[nc];
     e_q1 = cst[nc + 1];
     e_center = (st >> 12) & 1;
+    // A stencil cell no part of which lies within the list radius of this
+    // atom holds none of its neighbours: its range is left out.  Cell n
+    // of an axis holds the fractional coordinates sr (sr = x - anint(x))
+    // with int((sr + 0.4999) M) = n (src/nd.f90:1243-1245), an interval
+    // widened here by 2e-4 of the box; the distance to it is the smallest
+    // over the periodic images.
+    const double4 pid = c.pos[i];
+    const double q[3] = {pid.x - round(pid.x), pid.y - round(pid.y), pid.z - round(pid.z)};
+    double d2min = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      const double lo = (nv[d] == 0 ? -0.5 : (double)nv[d] / M[d] - 0.4999) - 2e-4;
+      const double hi = (double)(nv[d] + 1) / M[d] - 0.4999 + 2e-4;
+      double gap = 1.0;
+      for (int k = -1; k <= 1; ++k) {
+        const double g = fmax(0.0, fmax(lo + k - q[d], q[d] - (hi + k)));
+        gap = fmin(gap, g);
+      }
+      const double ga = gap * S->box[d];
+      d2min += ga * ga;
+    }
+    if (d2min > P->rlist * P->rlist) e_q1 = e_q0;
   }
   const int nt = P->ntypes, maxnb = P->maxnb, nb16 = P->nb16;
   const int *pm = c.pairmat + P->pm_off;
@@ -1122,7 +1143,8 @@ __device__ __forceinline__ void build_atom(const DevCtx &c, int sys, int local, 
       const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * sb0;
       const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * sb1;
       const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * sb2;
-      const float d2f = r0 * r0 + r1 * r1 + r2 * r2;
+      // (FMAs: the FP32 rounding stays far inside the 1e-5 band)
+      const float d2f = __fmaf_rn(r0, r0, __fmaf_rn(r1, r1, __fmul_rn(r2, r2)));
       const bool live = have && j != i && mx > 0;
       float2 band = band1;
       if (!one && live) {
