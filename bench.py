@@ -559,7 +559,7 @@ def main():
     ids = [W.add_to_context(ctx, s) for s in specs]
     ctx.set_tuning(args.tpa, args.graph_steps)
     if batch and not args.bare:
-        ctx.autotune(10)
+        ctx.autotune(30)
     # warm-up (includes the dynamics prologue: cell + Verlet list build), then
     # one block of the timed region's size so that its CUDA graph is captured
     # before the clock starts

@@ -7,11 +7,14 @@
 // src/read_input.f90:2-219): Types, Pairs, Model (dump/xyz,
 // src/read_input.f90:277-392), BoxSize, Skin, NeiMax, ReNeighbor,
 // Isokinetic/Isoenergetic/Isobaric and their Aniso* forms, BoxVel /
-// StopBoxVel, Velocity / Seed, OutFreq, StepNumber, Print and Run, and
-// prints the reference's write_thermo lines (src/read_input.f90:433-446).
+// StopBoxVel, Velocity / Seed, OutFreq, StepNumber, ConfOutFreq, Print and
+// Run, and prints the reference's write_thermo lines
+// (src/read_input.f90:433-446) and writes its model files (write_model,
+// src/read_input.f90:394-431).
 // Every Run is one call of ndg_run (the dynamics prologue and loop,
 // src/nd.f90:60-199) on the GPU.  --mixed selects NDG_PREC_MIXED, --fixed
 // the corrected list semantics.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -85,6 +88,37 @@ std::string g14_6(double x) {
   return buf;
 }
 
+// Fortran ENw.d (engineering notation: a mantissa of 1 to 3 digits before
+// the point, an exponent that is a multiple of 3), right-justified in w
+std::string en_format(double x, int w, int d) {
+  char body[64];
+  if (x == 0.0 || !std::isfinite(x)) {
+    if (x == 0.0) std::snprintf(body, sizeof body, "%s%.*fE+00", std::signbit(x) ? "-" : "", d, 0.0);
+    else std::snprintf(body, sizeof body, "%s", std::isnan(x) ? "NaN" : (x > 0 ? "Infinity" : "-Infinity"));
+  } else {
+    int e3 = 3 * (int)std::floor(std::floor(std::log10(std::fabs(x))) / 3.0);
+    double m = x / std::pow(10.0, e3);
+    char mant[48];
+    std::snprintf(mant, sizeof mant, "%.*f", d, m);
+    if (std::fabs(std::atof(mant)) >= 1000.0) {  // rounding carried into a fourth digit
+      e3 += 3;
+      m = x / std::pow(10.0, e3);
+      std::snprintf(mant, sizeof mant, "%.*f", d, m);
+    } else if (std::fabs(std::atof(mant)) < 1.0) {  // log10 landed just below a power of ten
+      e3 -= 3;
+      m = x / std::pow(10.0, e3);
+      std::snprintf(mant, sizeof mant, "%.*f", d, m);
+    }
+    const int ae = e3 < 0 ? -e3 : e3;
+    if (ae <= 99) std::snprintf(body, sizeof body, "%sE%c%02d", mant, e3 < 0 ? '-' : '+', ae);
+    else std::snprintf(body, sizeof body, "%s%c%03d", mant, e3 < 0 ? '-' : '+', ae);
+  }
+  if ((int)std::strlen(body) > w) return std::string(w, '*');
+  char out[64];
+  std::snprintf(out, sizeof out, "%*s", w, body);
+  return out;
+}
+
 void thermo_line(const ndg_thermo *t, void *) {
   std::printf(" %8d %s %s %s %s %s\n", t->step, g14_6(t->potential).c_str(),
               g14_6(t->kinetic).c_str(), g14_6(t->energy_error).c_str(),
@@ -156,6 +190,42 @@ struct Driver {
   bool springs_dirty = false, ipos_pending = false;
   std::vector<double> ipos;
   double ibox[3] = {0, 0, 0};
+  // configuration output (ConfOutFreq [i] [type], src/read_input.f90:196-197)
+  int conf_outs = 0;
+  std::string model_out_type = "NA";
+
+  // write_model, 'xyz' and 'dump' formats (src/read_input.f90:394-431); the
+  // per-atom energy pene of the xyz records is zero (compute0 zeroes it,
+  // src/nd.f90:251, and nothing adds to it)
+  bool write_model(FILE *f, int step) const {
+    const int np = (int)typ.size();
+    if (model_out_type == "XYZ" || model_out_type == "xyz") {
+      std::fprintf(f, "%8d\n\n", np);
+      for (int i = 0; i < np; ++i) {
+        const std::string &tn = tname.at(typ[i] - 1);
+        std::fprintf(f, "%-4.4s ", tn.c_str());
+        for (int k = 0; k < 3; ++k) std::fputs(en_format(pos[3 * (size_t)i + k], 14, 4).c_str(), f);
+        for (int k = 0; k < 3; ++k) std::fputs(en_format(vel[3 * (size_t)i + k], 14, 4).c_str(), f);
+        std::fputs(en_format(0.0, 14, 4).c_str(), f);
+        std::fputc('\n', f);
+      }
+    } else if (model_out_type == "dump" || model_out_type == "trj") {
+      std::fprintf(f, "ITEM: TIMESTEP\n%7d\nITEM: NUMBER OF ATOMS\n%7d\n", step, np);
+      std::fprintf(f, "ITEM: BOX BOUNDS pp pp pp\n");
+      for (int k = 0; k < 3; ++k) std::fprintf(f, "%12.4f%12.4f\n", 0.0, box[k]);
+      std::fprintf(f, "ITEM: ATOMS id type xs ys zs\n");
+      for (int i = 0; i < np; ++i) {
+        // real(pos(1:3,i))+0.0: single precision, f9.5
+        std::fprintf(f, "%7d %2d%9.5f%9.5f%9.5f\n", i + 1, typ[i], (double)(float)pos[3 * (size_t)i],
+                     (double)(float)pos[3 * (size_t)i + 1], (double)(float)pos[3 * (size_t)i + 2]);
+      }
+    } else {
+      std::fprintf(stderr, "ERROR: model out type: %s not supported\n", model_out_type.c_str());
+      return false;
+    }
+    std::fflush(f);
+    return true;
+  }
 
   // positions as the device has them after a run (for domain selections)
   int sync_positions() {
@@ -301,12 +371,40 @@ struct Driver {
       if (rc) return rc;
       holds_dirty = false;
     }
-    rc = ndg_run(ctx, nsteps, thermo_line, nullptr);
+    // dynamics (src/nd.f90:92-172): ConfOuts 0 means once per Run, 'NA'
+    // means xyz (both persist); the model goes to out.<type> (appended) at
+    // the start and wherever mod(step, ConfOuts) = 0.  The loop runs in
+    // pieces that end there: ndg_run, then ndg_run_continue (one run).
+    if (conf_outs == 0) conf_outs = nsteps;
+    if (model_out_type == "NA") model_out_type = "xyz";
+    FILE *mf = std::fopen(("out." + model_out_type).c_str(), "a");
+    if (!mf) {
+      std::fprintf(stderr, "dynamics: cannot open out.%s\n", model_out_type.c_str());
+      return NDG_ERR_ARG;
+    }
+    if (!write_model(mf, c.step)) {
+      std::fclose(mf);
+      return NDG_ERR_ARG;
+    }
+    int done = 0;
+    while (done < nsteps && rc == NDG_OK) {
+      const int at = c.step + done;
+      const int piece = std::min(nsteps - done, conf_outs - (((at % conf_outs) + conf_outs) % conf_outs));
+      rc = done == 0 ? ndg_run(ctx, piece, thermo_line, nullptr)
+                     : ndg_run_continue(ctx, piece, thermo_line, nullptr);
+      done += piece;
+      if (rc == NDG_OK && (c.step + done) % conf_outs == 0) {
+        rc = ndg_get_state(ctx, sys, pos.data(), vel.data(), acc.data(), box);
+        if (rc == NDG_OK && !write_model(mf, c.step + done)) rc = NDG_ERR_ARG;
+      }
+    }
+    std::fclose(mf);
     if (rc) return rc;
     ndg_control after{};
     ndg_get_control(ctx, sys, &after);
-    c.step = after.step;  // StepNumber carries over between Runs
-    c.skin = after.skin;  // the default skin, once set, persists (src/nd.f90:77-79)
+    c.step = after.step;      // StepNumber carries over between Runs
+    c.skin = after.skin;      // the default skin, once set, persists (src/nd.f90:77-79)
+    c.neimax = after.neimax;  // so does the NeiMax estimate (src/nd.f90:84-88)
     return NDG_OK;
   }
 };
@@ -343,7 +441,10 @@ int main(int argc, char **argv) {
     auto w = split(strip_comment(raw));
     if (w.empty()) continue;
     const std::string &k = w[0];
-    if (k == "help" || k == "WritePotentialTable" || k == "ConfOutFreq") {
+    if (k == "ConfOutFreq") {
+      d.conf_outs = std::atoi(arg(w, 1).c_str());
+      if (w.size() >= 3) d.model_out_type = w[2];
+    } else if (k == "help" || k == "WritePotentialTable") {
       // no output on the timestep path
     } else if (k == "BoxSize") {
       for (int q = 0; q < 3; ++q) d.boxset[q] = std::atof(arg(w, q + 1).c_str());

@@ -151,3 +151,71 @@ def test_driver_springs_match_oracle(tmp_path):
         assert _close(float(a[1]), b["pe"], 2e-6, 1e-9), (a, b["text"])
         assert _close(float(a[2]), b["ke"], 2e-6, 0), (a, b["text"])
     assert float(ours[-1][1]) > 0.0  # the springs are strained by the motion
+
+
+def _script(name, nsteps, conf):
+    case = GOLD[name]
+    out = []
+    for ln in case["script"]:
+        w = ln.split()
+        if w[:1] == ["Run"]:
+            ln = " ".join(["Run", str(nsteps)] + w[2:3])
+        elif w[:1] == ["ConfOutFreq"]:
+            ln = conf
+        out.append(ln)
+    return case, out
+
+
+def _drive(case, script, where):
+    os.makedirs(where, exist_ok=True)
+    lattice.materialise(case["model"], where)
+    r = subprocess.run([EXE], input="START\n" + "\n".join(script) + "\n", text=True,
+                       capture_output=True, cwd=where, timeout=600)
+    assert r.returncode == 0, r.stderr
+    return [ln for ln in r.stdout.splitlines() if len(ln.split()) == 6 and ln.split()[0].isdigit()]
+
+
+def test_driver_model_output(tmp_path):
+    """write_model every ConfOutFreq steps (src/read_input.f90:394-431,
+    src/nd.f90:121,172): the run stops where a model is due and carries on
+    (ndg_run_continue), so its thermo lines are the same as one unbroken
+    run's.  The dump frames hold the reference's header, the single
+    precision positions in f9.5 (xs written as the fractional position,
+    the round trip read_model/write_model of the reference), and the xyz
+    frames the EN14.4 fields of positions, velocities and a zero energy."""
+    import re
+    case, one = _script("MorseTest", 200, "ConfOutFreq 0 dump")
+    _, five = _script("MorseTest", 200, "ConfOutFreq 50 dump")
+    rows_one = _drive(case, one, str(tmp_path / "one"))
+    rows_five = _drive(case, five, str(tmp_path / "five"))
+    assert rows_one == rows_five and len(rows_one) >= 5
+    lines = open(tmp_path / "five" / "out.dump").read().splitlines()
+    frames = [k for k, ln in enumerate(lines) if ln == "ITEM: TIMESTEP"]
+    assert [int(lines[k + 1]) for k in frames] == [0, 50, 100, 150, 200]
+    np_ = int(lines[frames[0] + 3])
+    assert np_ == 4000 and lines[frames[0] + 4] == "ITEM: BOX BOUNDS pp pp pp"
+    assert lines[frames[0] + 5] == "%12.4f%12.4f" % (0.0, 36.8)
+    assert lines[frames[0] + 8] == "ITEM: ATOMS id type xs ys zs"
+    model = open(tmp_path / "five" / "model.dump").read().splitlines()
+    xs0 = {int(ln.split()[0]): [float(v) for v in ln.split()[2:5]] for ln in model[9:9 + np_]}
+    for ln in lines[frames[0] + 9:frames[0] + 9 + np_]:
+        assert re.fullmatch(r"[ \d]{7} [ \d]{2}( *-?\d+\.\d{5}){3}", ln), ln
+        i, t = int(ln[:7]), int(ln[8:10])
+        assert t == 1
+        got = [float(ln[10 + 9 * k:19 + 9 * k]) for k in range(3)]
+        for a, b in zip(got, xs0[i]):
+            assert abs(a - (b - 0.5)) <= 1.5e-5
+    _, xyz = _script("MorseTest", 100, "ConfOutFreq 50 xyz")
+    _drive(case, xyz, str(tmp_path / "xyz"))
+    lines = open(tmp_path / "xyz" / "out.xyz").read().splitlines()
+    assert len(lines) == 3 * (2 + 4000) and int(lines[0]) == 4000 and lines[1] == ""
+    en = re.compile(r" *-?\d{1,3}\.\d{4}E[+-]\d{2}")
+    for ln in lines[2:4002] + lines[-4000:]:
+        assert ln[:5] == "Cu   " and len(ln) == 5 + 7 * 14, ln
+        fields = [ln[5 + 14 * k:19 + 14 * k] for k in range(7)]
+        for f in fields:
+            assert en.fullmatch(f), ln
+            m = float(f.strip().split("E")[0])
+            assert m == 0.0 or 1.0 <= abs(m) < 1000.0, f
+        assert fields[6].strip() == "0.0000E+00"
+        assert all(abs(float(f)) <= 0.5001 for f in fields[:3])
