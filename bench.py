@@ -55,6 +55,11 @@ def parse():
                          "force error, plain baseline, e2e, CPU baseline or kernel timing")
     ap.add_argument("--graph-steps", type=int, default=100,
                     help="steps per CUDA graph (1 = eager launches, as ncu needs)")
+    ap.add_argument("--replica-stride", type=int, default=1,
+                    help="c4: every S-th replica only (a smaller case of the same "
+                         "ensemble, for profiler captures)")
+    ap.add_argument("--gather-depth", type=int, default=0,
+                    help="neighbour gathers in flight per thread (0 = library choice)")
     return ap.parse_args()
 
 
@@ -545,6 +550,8 @@ def main():
     from ndyn_omp_b200 import workloads as W
     torch.cuda.set_device(local)
     specs, prec = workload(args.config)
+    if args.config == "c4" and args.replica_stride > 1:
+        specs = specs[::args.replica_stride]
     prec = args.precision or prec
     N = n_atoms(specs)
 
@@ -558,6 +565,8 @@ def main():
     ctx = nd.Context(local, prec)
     ids = [W.add_to_context(ctx, s) for s in specs]
     ctx.set_tuning(args.tpa, args.graph_steps)
+    if args.gather_depth:
+        ctx.set_gather_depth(args.gather_depth)
     if batch and not args.bare:
         ctx.autotune(30)
     # warm-up (includes the dynamics prologue: cell + Verlet list build), then
@@ -723,7 +732,7 @@ def main():
                    "l2": f"inputs larger than L2: ~{touched / 1e6:.0f} MB touched per step "
                          f"vs 126 MB L2" if touched > L2_BYTES else "L2-resident workload",
                    "threads_per_atom": tpa, "gather_depth": ctx.gather_depth(),
-                   "graph_steps": gsteps,
+                   "graph_steps": gsteps, "replica_stride": args.replica_stride,
                    "baseline_metric": "atom-steps/s at 1 GPU, batched mixed vs plain FP64 at "
                                       "stated force error; p50/p99"},
         "force_rel_err_vs_fp64": force_err,
