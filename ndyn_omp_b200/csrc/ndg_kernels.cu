@@ -1478,12 +1478,52 @@ __device__ __noinline__ SpringSum spring_pass(const DevCtx &c, const SysParam *P
 // parameters in registers, others look them up per pair.
 //
 // Mixed precision: each thread sums whole chunks of CHUNK consecutive list
-// entries in FP32, in list order, and adds every chunk's sum to 64-bit
+// entries in FP32 (in list order; a full chunk of a one-potential system
+// in the lean kernel as its even entries' sum plus its odd entries' sum, two
+// entries per f32x2 instruction), and adds every chunk's sum to 64-bit
 // fixed-point totals (the force in registers; with EV, the potential energy
 // and virial in per-thread shared-memory slots).  Chunks are dealt to the
 // TPA threads of an atom round-robin, so every launch shape forms the same
 // chunks and the integer totals, which do not depend on the order of
 // addition, are the same bits for any TPA, grid or batch composition.
+// Packed FP32 pairs (sm_100's f32x2 add/sub/mul/fma: two FP32 operations in
+// one instruction, each rounded as its scalar form): the mixed loop's
+// full-chunk path evaluates two list entries per instruction.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 pk2(float a, float b) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void upk2(f32x2 v, float &a, float &b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 constexpr int CHUNK = 8;   // mixed: list entries per FP32 partial sum
 // mixed: neighbour gathers in flight per thread, 4 or 8 (a tuning choice:
 // 8 hides more latency when the gathers miss L2, 4 keeps more warps resident)
@@ -1683,67 +1723,136 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 /
           const float4 pp1 = ONE ? pair_params<STAB>(tv, 0) : make_float4(0.f, 0.f, 0.f, 0.f);
           for (int m = la; m < nch; m += TPA) {
             const int kb = m * CHUNK;
-            int qq[CHUNK];
-            if (nb16) {
-              // two 16-bit entries per word (CHUNK and kb are even)
-#pragma unroll
-              for (int q = 0; q < CHUNK; q += 2) {
-                const int w = kb + q < cnt ? ld_stream(nb + ((kb + q) >> 1) * TILE, lpol) : 0;
-                qq[q] = kb + q < cnt ? aoff + (w & 0xffff) : -1;
-                qq[q + 1] = kb + q + 1 < cnt ? aoff + (int)((unsigned)w >> 16) : -1;
-              }
-            } else {
-#pragma unroll
-              for (int q = 0; q < CHUNK; ++q)
-                qq[q] = kb + q < cnt ? ld_stream(nb + (kb + q) * TILE, lpol) : -1;
-            }
             float ax = 0.f, ay = 0.f, az = 0.f, ape = 0.f;
             float av0 = 0.f, av1 = 0.f, av2 = 0.f, av3 = 0.f, av4 = 0.f, av5 = 0.f;
             unsigned nm = 0;  // entries of this chunk within FP32 rounding of the cutoff
+            if (ONE && !EV && kb + CHUNK <= cnt) {
+              // a full chunk of a one-potential system: no per-entry masks,
+              // entries 2q and 2q+1 side by side in f32x2 operations, the
+              // chunk's sum as the sum of its even and its odd entries
+              const int4 *__restrict__ pb = nb16 ? c.pfx + aoff : c.pfx;
+              int jj[CHUNK];
+              if (nb16) {
 #pragma unroll
-            for (int h = 0; h < CHUNK; h += GATHER) {
-              int4 pj[GATHER];
-#pragma unroll
-              for (int q = 0; q < GATHER; ++q) pj[q] = c.pfx[qq[h + q] >= 0 ? qq[h + q] : i];
-#pragma unroll
-              for (int q = 0; q < GATHER; ++q) {
-                const int pg = ONE ? 1 : pmr[(tw_type(pj[q].w) - 1) * ntypes];
-                const int pt = pg & PT_MASK;
-                const bool sym = ONE || pg < PT_ASYM;  // energy and virial count
-                const int p1 = ONE ? 0 : (pt > 0 ? pt - 1 : 0);
-                const float4 prm = ONE ? pp1 : pair_params<STAB>(tv, p1);
-                // minimum image by 32-bit wrap-around of the fixed-point difference
-                const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj[q].x) * sb0;
-                const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj[q].y) * sb1;
-                const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj[q].z) * sb2;
-                const float d2 = __fmaf_rn(r0, r0, __fmaf_rn(r1, r1, __fmul_rn(r2, r2)));
-                const bool live = qq[h + q] >= 0 && pt > 0;
-                const bool ok = live && d2 <= prm.x;
-                nm |= (live && d2 > prm.x && d2 <= prm.y) ? (1u << (h + q)) : 0u;
-                // branch-free: every lane evaluates the pair, excluded ones add 0
-                const float rk = __fmaf_rn(d2 - ptrmin, prm.z, 1.0f);
-                int kk = (int)rk;
-                kk = kk < 1 ? 1 : (kk > ptsize ? ptsize : kk);
-                const float w = rk - (float)kk;
-                const int base = p1 * T + kk - 1;
-                const float2 F = tv.tF2[base];
-                const float df = ok ? __fdividef(__fmaf_rn(w, F.y - F.x, F.x), d2) : 0.f;
-                ax = __fmaf_rn(r0, df, ax);
-                ay = __fmaf_rn(r1, df, ay);
-                az = __fmaf_rn(r2, df, az);
-                if (cu && ok && sym) {
-                  const float2 Pp = tv.tP2[base];
-                  ape += __fmaf_rn(w, Pp.y - Pp.x, Pp.x);
+                for (int q = 0; q < CHUNK; q += 2) {
+                  const int w = ld_stream(nb + ((kb + q) >> 1) * TILE, lpol);
+                  jj[q] = w & 0xffff;
+                  jj[q + 1] = (int)((unsigned)w >> 16);
                 }
-                if (cv) {
-                  const float dv = sym ? df : 0.f;
-                  const float r0d = r0 * dv, r1d = r1 * dv;
-                  av0 = __fmaf_rn(r0d, r0, av0);
-                  av1 = __fmaf_rn(r1d, r1, av1);
-                  av2 = __fmaf_rn(r2 * dv, r2, av2);
-                  av3 = __fmaf_rn(r0d, r1, av3);
-                  av4 = __fmaf_rn(r0d, r2, av4);
-                  av5 = __fmaf_rn(r1d, r2, av5);
+              } else {
+#pragma unroll
+                for (int q = 0; q < CHUNK; ++q) jj[q] = ld_stream(nb + (kb + q) * TILE, lpol);
+              }
+              const f32x2 SB0 = pk2(sb0, sb0), SB1 = pk2(sb1, sb1), SB2 = pk2(sb2, sb2);
+              const f32x2 NPT = pk2(-ptrmin, -ptrmin), VDR = pk2(pp1.z, pp1.z),
+                          ONE2 = pk2(1.0f, 1.0f);
+              f32x2 AX = 0ull, AY = 0ull, AZ = 0ull;
+#pragma unroll
+              for (int h = 0; h < CHUNK; h += GATHER) {
+                int4 pj[GATHER];
+#pragma unroll
+                for (int q = 0; q < GATHER; ++q) pj[q] = pb[jj[h + q]];
+#pragma unroll
+                for (int q = 0; q < GATHER; q += 2) {
+                  const int4 pa = pj[q], pc = pj[q + 1];
+                  // minimum image by 32-bit wrap-around of the fixed-point difference
+                  const f32x2 R0 = mul2(pk2((float)(int)((unsigned)pi.x - (unsigned)pa.x),
+                                            (float)(int)((unsigned)pi.x - (unsigned)pc.x)), SB0);
+                  const f32x2 R1 = mul2(pk2((float)(int)((unsigned)pi.y - (unsigned)pa.y),
+                                            (float)(int)((unsigned)pi.y - (unsigned)pc.y)), SB1);
+                  const f32x2 R2 = mul2(pk2((float)(int)((unsigned)pi.z - (unsigned)pa.z),
+                                            (float)(int)((unsigned)pi.z - (unsigned)pc.z)), SB2);
+                  const f32x2 D2 = fma2(R0, R0, fma2(R1, R1, mul2(R2, R2)));
+                  float da, dc;
+                  upk2(D2, da, dc);
+                  const bool oka = da <= pp1.x, okc = dc <= pp1.x;
+                  nm |= (!oka && da <= pp1.y ? 1u << (h + q) : 0u) |
+                        (!okc && dc <= pp1.y ? 2u << (h + q) : 0u);
+                  const f32x2 RK = fma2(add2(D2, NPT), VDR, ONE2);
+                  float rka, rkc;
+                  upk2(RK, rka, rkc);
+                  int ka = (int)rka, kc = (int)rkc;
+                  ka = ka < 1 ? 1 : (ka > ptsize ? ptsize : ka);
+                  kc = kc < 1 ? 1 : (kc > ptsize ? ptsize : kc);
+                  const f32x2 W = sub2(RK, pk2((float)ka, (float)kc));
+                  const float2 Fa = tv.tF2[ka - 1], Fc = tv.tF2[kc - 1];
+                  const f32x2 FX = pk2(Fa.x, Fc.x);
+                  const f32x2 NUM = fma2(W, sub2(pk2(Fa.y, Fc.y), FX), FX);
+                  float na, nc;
+                  upk2(mul2(NUM, pk2(rcp_approx(da), rcp_approx(dc))), na, nc);
+                  const f32x2 DF = pk2(oka ? na : 0.f, okc ? nc : 0.f);
+                  AX = fma2(R0, DF, AX);
+                  AY = fma2(R1, DF, AY);
+                  AZ = fma2(R2, DF, AZ);
+                }
+              }
+              float e0, e1;
+              upk2(AX, e0, e1);
+              ax = e0 + e1;
+              upk2(AY, e0, e1);
+              ay = e0 + e1;
+              upk2(AZ, e0, e1);
+              az = e0 + e1;
+            } else {
+              int qq[CHUNK];
+              if (nb16) {
+                // two 16-bit entries per word (CHUNK and kb are even)
+#pragma unroll
+                for (int q = 0; q < CHUNK; q += 2) {
+                  const int w = kb + q < cnt ? ld_stream(nb + ((kb + q) >> 1) * TILE, lpol) : 0;
+                  qq[q] = kb + q < cnt ? aoff + (w & 0xffff) : -1;
+                  qq[q + 1] = kb + q + 1 < cnt ? aoff + (int)((unsigned)w >> 16) : -1;
+                }
+              } else {
+#pragma unroll
+                for (int q = 0; q < CHUNK; ++q)
+                  qq[q] = kb + q < cnt ? ld_stream(nb + (kb + q) * TILE, lpol) : -1;
+              }
+#pragma unroll
+              for (int h = 0; h < CHUNK; h += GATHER) {
+                int4 pj[GATHER];
+#pragma unroll
+                for (int q = 0; q < GATHER; ++q) pj[q] = c.pfx[qq[h + q] >= 0 ? qq[h + q] : i];
+#pragma unroll
+                for (int q = 0; q < GATHER; ++q) {
+                  const int pg = ONE ? 1 : pmr[(tw_type(pj[q].w) - 1) * ntypes];
+                  const int pt = pg & PT_MASK;
+                  const bool sym = ONE || pg < PT_ASYM;  // energy and virial count
+                  const int p1 = ONE ? 0 : (pt > 0 ? pt - 1 : 0);
+                  const float4 prm = ONE ? pp1 : pair_params<STAB>(tv, p1);
+                  // minimum image by 32-bit wrap-around of the fixed-point difference
+                  const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj[q].x) * sb0;
+                  const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj[q].y) * sb1;
+                  const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj[q].z) * sb2;
+                  const float d2 = __fmaf_rn(r0, r0, __fmaf_rn(r1, r1, __fmul_rn(r2, r2)));
+                  const bool live = qq[h + q] >= 0 && pt > 0;
+                  const bool ok = live && d2 <= prm.x;
+                  nm |= (live && d2 > prm.x && d2 <= prm.y) ? (1u << (h + q)) : 0u;
+                  // branch-free: every lane evaluates the pair, excluded ones add 0
+                  const float rk = __fmaf_rn(d2 - ptrmin, prm.z, 1.0f);
+                  int kk = (int)rk;
+                  kk = kk < 1 ? 1 : (kk > ptsize ? ptsize : kk);
+                  const float w = rk - (float)kk;
+                  const int base = p1 * T + kk - 1;
+                  const float2 F = tv.tF2[base];
+                  const float df = ok ? __fdividef(__fmaf_rn(w, F.y - F.x, F.x), d2) : 0.f;
+                  ax = __fmaf_rn(r0, df, ax);
+                  ay = __fmaf_rn(r1, df, ay);
+                  az = __fmaf_rn(r2, df, az);
+                  if (cu && ok && sym) {
+                    const float2 Pp = tv.tP2[base];
+                    ape += __fmaf_rn(w, Pp.y - Pp.x, Pp.x);
+                  }
+                  if (cv) {
+                    const float dv = sym ? df : 0.f;
+                    const float r0d = r0 * dv, r1d = r1 * dv;
+                    av0 = __fmaf_rn(r0d, r0, av0);
+                    av1 = __fmaf_rn(r1d, r1, av1);
+                    av2 = __fmaf_rn(r2 * dv, r2, av2);
+                    av3 = __fmaf_rn(r0d, r1, av3);
+                    av4 = __fmaf_rn(r0d, r2, av4);
+                    av5 = __fmaf_rn(r1d, r2, av5);
+                  }
                 }
               }
             }
@@ -1918,35 +2027,37 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 /
       }
       if (ck) s_red[KR][g] = ke;
     }
-    __syncthreads();
+    // one warp sums the rows: lane l adds atoms l, l+32, l+64, l+96, then a
+    // butterfly over the lanes, a tree fixed by the atom index (the same bits
+    // for any threads-per-atom); one barrier before it, one after
     const int r0 = (EV && !MIXED) ? 0 : KR, r1 = ck ? NR : KR;
-    if (r1 > r0) {
-#pragma unroll 1
-      for (int sft = TILE / 2; sft > 0; sft >>= 1) {
-        if ((int)threadIdx.x < sft)
-          for (int r = r0; r < r1; ++r) s_red[r][threadIdx.x] += s_red[r][threadIdx.x + sft];
-        __syncthreads();
-      }
-    }
-    if (threadIdx.x == 0) {
+    if (EV || ck) __syncthreads();
+    if (threadIdx.x < 32) {
       double *red = c.red + 8 * (size_t)tile;
-      if (EV) {
-        if (MIXED) {
+      const int lane = threadIdx.x;
+#pragma unroll 1
+      for (int r = r0; r < r1; ++r) {
+        double v = s_red[r][lane];
+#pragma unroll
+        for (int q = 1; q < TILE / 32; ++q) v += s_red[r][lane + 32 * q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) red[r == KR ? 7 : r] = v;
+      }
+      if (lane == 0) {
+        if (EV && MIXED) {
 #pragma unroll
           for (int k = 0; k < 7; ++k) {
             red[k] = __longlong_as_double((long long)s_q[k]);  // bits of the integer sum
             s_q[k] = 0ull;
           }
-        } else {
-#pragma unroll
-          for (int k = 0; k < 7; ++k) red[k] = s_red[k % NR][0];
         }
+        if (!ck) red[7] = 0.0;
+        __threadfence();
+        const unsigned nblk = (unsigned)(P->npad / TILE);
+        const unsigned t = atomicAdd(&S->ticket, 1u);
+        last = (t == nblk - 1);
       }
-      red[7] = ck ? s_red[KR][0] : 0.0;
-      __threadfence();
-      const unsigned nblk = (unsigned)(P->npad / TILE);
-      const unsigned t = atomicAdd(&S->ticket, 1u);
-      last = (t == nblk - 1);
     }
     __syncthreads();
     if (last) {
@@ -1954,8 +2065,8 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 /
       finalize_system<MIXED>(c, sys, P->atom_off / TILE, P->npad / TILE, flags, FUSE, next_h,
                              s_red);
       if (threadIdx.x == 0) S->ticket = 0;
+      __syncthreads();  // finalize's shared values are read before the next tile writes
     }
-    __syncthreads();
   }
 }
 
