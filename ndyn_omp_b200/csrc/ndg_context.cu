@@ -118,6 +118,7 @@ struct ndg_ctx {
   double4 *bcd = nullptr;  // hold groups of all systems
   int *atom_cell = nullptr, *atom_slot = nullptr, *perm = nullptr, *tmp_src = nullptr,
       *tmp_key = nullptr;
+  int *cxyz = nullptr;  // per atom slot: its link cell's grid coordinates (rebuild scratch)
   int *cell_count = nullptr, *cell_start = nullptr;
   int *nbr = nullptr;
   int *tile_rows = nullptr;
@@ -210,6 +211,7 @@ DevCtx devctx(ndg_ctx *c) {
   d.any_neimax = c->any_neimax;
   d.nnb = c->nnb;
   d.atom_cell = c->atom_cell;
+  d.cxyz = c->cxyz;
   d.atom_slot = c->atom_slot;
   d.cell_count = c->cell_count;
   d.cell_start = c->cell_start;
@@ -287,6 +289,7 @@ int grow_atoms(ndg_ctx *c, long long new_chunks) {
   rc |= grow(c, c->s_acc, 0, 3 * n);
   rc |= grow(c, c->s_gid, 0, n);
   rc |= grow(c, c->s_cell, 0, n);
+  rc |= grow(c, c->cxyz, 0, n);
   rc |= grow(c, c->itop, 2 * (size_t)c->atoms.cap, 2 * (size_t)new_chunks);
   rc |= grow(c, c->ired, 0, (size_t)new_chunks);
   rc |= grow(c, c->red, 0, 8 * 32 * (size_t)new_chunks);
@@ -976,7 +979,7 @@ int status_from_words(ndg_ctx *c) {
 ndg_ctx::~ndg_ctx() {
   drop_graphs(this);
   void *ptrs[] = {dP, dS, chunk_sys, cell_sys, pos, s_pos, pfx, vel, acc, disp, force, s_vel,
-                  s_acc, gid, s_gid, s_cell, nnb, hold, bcd, ipos, sprd, atom_cell, atom_slot, perm, tmp_src, tmp_key,
+                  s_acc, gid, s_gid, s_cell, cxyz, nnb, hold, bcd, ipos, sprd, atom_cell, atom_slot, perm, tmp_src, tmp_key,
                   cell_count, cell_start, rb_list, plan, plan_kb, plan_hdr, nbr, tile_rows, red, itop, ired, pairmat, pairg, mass, rc2, rlist2,
                   vdr2, rc2f, tabF, tabP, tabF2, tabP2, ring, ring_count};
   for (void *p : ptrs)
@@ -1917,7 +1920,7 @@ long long ndg_system_bytes(int np, int ntypes, int npairs, int ptsize, double de
   const double r = rlist * 1.1;
   const long long maxnb =
       (long long)(4.0 / 3.0 * 3.141592653589793 * r * r * r * density * 1.2 * 2.0) + 24;
-  const long long per_atom = 2 * 32 + 16 + 4 * 24 + 2 * 24 + 4 * 10;
+  const long long per_atom = 2 * 32 + 16 + 4 * 24 + 2 * 24 + 4 * 11;
   const long long ncell = (long long)(np / std::max(density * rlist * rlist * rlist, 1e-9)) + 8;
   return npad * per_atom + npad * maxnb * 4 + ncell * 12 +
          (long long)npairs * (ptsize + 1) * 32;

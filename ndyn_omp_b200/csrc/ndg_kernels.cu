@@ -875,7 +875,14 @@ __device__ void copyback_chunk(const DevCtx &c, int sys, int chunk, int mixed) {
     c.disp[3 * (size_t)i + d] = 0.0;  // src/nd.f90:1384,1427
   }
   c.gid[i] = c.s_gid[i];
-  c.atom_cell[i] = c.s_cell[i];
+  const int cl = c.s_cell[i];
+  c.atom_cell[i] = cl;
+  // the cell's grid coordinates, once per atom here rather than by every
+  // stencil lane of the list build (grids above 2047 x 2047 x 1023 cells
+  // leave them to the build)
+  const SysState *S = c.S + sys;
+  const int M0 = S->mcell[0], M1 = S->mcell[1];
+  c.cxyz[i] = (cl % M0) | (((cl / M0) % M1) << 11) | ((cl / (M0 * M1)) << 22);
 }
 
 __global__ __launch_bounds__(BLOCK) void k_copyback(DevCtx c, int mixed) {
@@ -1077,11 +1084,22 @@ __device__ __forceinline__ void build_atom(const DevCtx &c, int sys, int local, 
   const int aoff = P->atom_off, i = aoff + local;
   const int *cst = c.cell_start + P->cell_off;
   const int ne = S->nstencil;
+  const int4 pi = c.pfx[i];
   int e_q0 = 0, e_q1 = 0, e_center = 0;  // lane e < ne: stencil entry e
   if (lane < ne) {
     const int M[3] = {S->mcell[0], S->mcell[1], S->mcell[2]};
-    const int cl = c.atom_cell[i];
-    const int cv[3] = {cl % M[0], (cl / M[0]) % M[1], cl / (M[0] * M[1])};
+    int cv[3];
+    if (M[0] < 2048 && M[1] < 2048 && M[2] < 1024) {
+      const int w = c.cxyz[i];
+      cv[0] = w & 2047;
+      cv[1] = (w >> 11) & 2047;
+      cv[2] = (unsigned)w >> 22;
+    } else {
+      const int cl = c.atom_cell[i];
+      cv[0] = cl % M[0];
+      cv[1] = (cl / M[0]) % M[1];
+      cv[2] = cl / (M[0] * M[1]);
+    }
     const int st = S->stencil[lane];
     int nv[3];
     for (int d = 0; d < 3; ++d) nv[d] = wrap_step(cv[d], ((st >> (4 * d)) & 15) - 1, M[d]);
@@ -1093,23 +1111,23 @@ __device__ __forceinline__ void build_atom(const DevCtx &c, int sys, int local, 
     // atom holds none of its neighbours: its range is left out.  Cell n
     // of an axis holds the fractional coordinates sr (sr = x - anint(x))
     // with int((sr + 0.4999) M) = n (src/nd.f90:1243-1245), an interval
-    // widened here by 2e-4 of the box; the distance to it is the smallest
-    // over the periodic images.
-    const double4 pid = c.pos[i];
-    const double q[3] = {pid.x - round(pid.x), pid.y - round(pid.y), pid.z - round(pid.z)};
-    double d2min = 0.0;
+    // widened here by 2e-4 of the box; the distance to it is taken on the
+    // periodic axis (from the interval's middle, minimum image).  A
+    // prefilter only, so FP32 serves: its rounding is ~1e-7 of the box,
+    // far inside the widening.
+    const int pq[3] = {pi.x, pi.y, pi.z};
+    float d2min = 0.f;
     for (int d = 0; d < 3; ++d) {
-      const double lo = (nv[d] == 0 ? -0.5 : (double)nv[d] / M[d] - 0.4999) - 2e-4;
-      const double hi = (double)(nv[d] + 1) / M[d] - 0.4999 + 2e-4;
-      double gap = 1.0;
-      for (int k = -1; k <= 1; ++k) {
-        const double g = fmax(0.0, fmax(lo + k - q[d], q[d] - (hi + k)));
-        gap = fmin(gap, g);
-      }
-      const double ga = gap * S->box[d];
-      d2min += ga * ga;
+      const float im = __fdividef(1.0f, (float)M[d]);
+      const float lo = (nv[d] == 0 ? -0.5f : (float)nv[d] * im - 0.4999f) - 2e-4f;
+      const float hi = (float)(nv[d] + 1) * im - 0.4999f + 2e-4f;
+      const float q = (float)pq[d] * (1.0f / 4294967296.0f);
+      float dm = q - 0.5f * (lo + hi);
+      dm = dm - rintf(dm);
+      const float gap = fmaxf(fabsf(dm) - 0.5f * (hi - lo), 0.f) * (float)S->box[d];
+      d2min = __fmaf_rn(gap, gap, d2min);
     }
-    if (d2min > P->rlist * P->rlist) e_q1 = e_q0;
+    if (d2min > (float)(P->rlist * P->rlist) * (1.f + 1e-5f)) e_q1 = e_q0;
   }
   const int nt = P->ntypes, maxnb = P->maxnb, nb16 = P->nb16;
   const int *pm = c.pairmat + P->pm_off;
@@ -1121,7 +1139,6 @@ __device__ __forceinline__ void build_atom(const DevCtx &c, int sys, int local, 
   const bool one = nt == 1 && P->npairs == 1 && pm[0] == 1;
   const float rf1 = (float)rl2[0];
   const float2 band1 = make_float2(rf1 * (1.f - NB_MARGIN), rf1 * (1.f + NB_MARGIN));
-  const int4 pi = c.pfx[i];
   const int ti = tw_type(pi.w);
   int *col = c.nbr + P->nbr_off + (long long)(local / TILE) * maxnb * TILE + (local % TILE);
   const unsigned below = (1u << lane) - 1u;

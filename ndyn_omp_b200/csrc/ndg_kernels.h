@@ -48,6 +48,7 @@ struct DevCtx {
   double4 *s_pos;
   double *s_vel, *s_acc;
   int *s_gid, *s_cell;
+  int *cxyz;  // per atom slot: link cell grid coordinates, x | y << 11 | z << 22 (rebuild scratch)
   const int *pairmat;  // PairMat per system (the list build)
   const int *pairg;    // gather matrix per system (the pair kernel)
   const double *mass, *rc2, *rlist2;
@@ -116,6 +117,16 @@ NDG_HD int make_stencil(const int *mcell, int quirk, int *out) {
                           {1, -1, 0}, {1, -1, -1}, {1, -1, 1}};
   int n = 0;
   out[n++] = (1) | (1 << 4) | (1 << 8) | (1 << 12);  // the cell itself
+  if (mcell[0] >= 3 && mcell[1] >= 3 && mcell[2] >= 3) {
+    // three or more cells per axis: the 26 neighbours are distinct cells,
+    // and each is one forward offset of the half stencil or the negative of
+    // one (multiplicity 1 in either semantics); the order of the loop below
+    for (int dz = -1; dz <= 1; ++dz)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx)
+          if (dx || dy || dz) out[n++] = (dx + 1) | ((dy + 1) << 4) | ((dz + 1) << 8);
+    return n;
+  }
   int seen[27][3];
   int nseen = 0;
   for (int dz = -1; dz <= 1; ++dz)
