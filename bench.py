@@ -567,8 +567,13 @@ def main():
     ctx.set_tuning(args.tpa, args.graph_steps)
     if args.gather_depth:
         ctx.set_gather_depth(args.gather_depth)
+    skin_changed = None
     if batch and not args.bare:
+        # launch shape (threads per atom, gathers in flight), then the
+        # rebuild interval: a per-system list skin kept only where a second
+        # timed trial confirms it
         ctx.autotune(30)
+        skin_changed = ctx.autotune_skin(40)
     # warm-up (includes the dynamics prologue: cell + Verlet list build), then
     # one block of the timed region's size so that its CUDA graph is captured
     # before the clock starts
@@ -733,6 +738,7 @@ def main():
                          f"vs 126 MB L2" if touched > L2_BYTES else "L2-resident workload",
                    "threads_per_atom": tpa, "gather_depth": ctx.gather_depth(),
                    "graph_steps": gsteps, "replica_stride": args.replica_stride,
+                   "skin_retuned_systems": skin_changed,
                    "baseline_metric": "atom-steps/s at 1 GPU, batched mixed vs plain FP64 at "
                                       "stated force error; p50/p99"},
         "force_rel_err_vs_fp64": force_err,
