@@ -2207,6 +2207,21 @@ static int pair_launch(const DevCtx &c, cudaStream_t st, int hf, unsigned long l
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, TILE * TPA, smem);
     if (occ < 1) occ = 1;
+    // Registers bound the residency; the shared-memory carve-out need only
+    // hold that many blocks, and the rest of the SM's 256 KB stays L1 for
+    // the neighbour gathers (left alone, the carve-out is sized for the
+    // blocks shared memory alone would admit).
+    cudaFuncAttributes fa;
+    int dev = 0, smmax = 0;
+    cudaGetDevice(&dev);
+    if (cudaFuncGetAttributes(&fa, kern) == cudaSuccess &&
+        cudaDeviceGetAttribute(&smmax, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) ==
+            cudaSuccess &&
+        smmax > 0) {
+      const long long need = (long long)occ * (smem + (long long)fa.sharedSizeBytes + 1024);
+      const int pct = (int)std::min<long long>(100, (need * 100 + smmax - 1) / smmax);
+      cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+    }
     cfg_smem = smem;
   }
   const int nsm = sm_count();
