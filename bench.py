@@ -739,6 +739,7 @@ def main():
                    "threads_per_atom": tpa, "gather_depth": ctx.gather_depth(),
                    "graph_steps": gsteps, "replica_stride": args.replica_stride,
                    "skin_retuned_systems": skin_changed,
+                   "list_split": dict(zip(("rows", "threads_per_atom"), ctx.list_split())),
                    "baseline_metric": "atom-steps/s at 1 GPU, batched mixed vs plain FP64 at "
                                       "stated force error; p50/p99"},
         "force_rel_err_vs_fp64": force_err,

@@ -279,9 +279,24 @@ int ndg_get_tuning(ndg_ctx *ctx, int *threads_per_atom, int *graph_steps);
  * pair loop: 4 (more resident warps) or 8 (more latency hidden) */
 int ndg_set_gather_depth(ndg_ctx *ctx, int depth);
 int ndg_get_gather_depth(ndg_ctx *ctx, int *depth);
+/* Atoms to threads by list length: in a dynamics step, systems whose mean
+ * full-list length (entries per atom at their last list build) is at least
+ * `rows` run in pair launches of their own with `tpa_long` threads per atom
+ * (1,2,4,8); the others with the context's threads per atom.  rows = 0: one
+ * class (the default).  Mixed-precision forces do not depend on the split;
+ * FP64 ones change in the last bits (the summation order of an atom's
+ * neighbours follows its threads).  Standalone compute0 is not split.  No
+ * counterpart in the reference (its OpenMP loop splits atoms evenly,
+ * src/nd.f90:269-271). */
+int ndg_set_list_split(ndg_ctx *ctx, int rows, int tpa_long);
+int ndg_get_list_split(ndg_ctx *ctx, int *rows, int *tpa_long);
 /* time candidate launch shapes (threads per atom; gather depth for one
  * thread per atom in mixed precision) on the current systems for a few
- * steps and keep the fastest (state is restored afterwards) */
+ * steps and keep the fastest; then, where the systems' mean list lengths
+ * differ by 1.5x or more, the long-list class (ndg_set_list_split: the
+ * threshold at the geometric middle of the shortest and longest, 2 or 4
+ * threads per atom) is kept if a trial runs faster (state is restored
+ * afterwards) */
 int ndg_autotune(ndg_ctx *ctx, int steps_per_trial);
 /* The rebuild-interval autotuner: choose each fixed-semantics system's list
  * skin (so its rebuild interval).  A trial of `steps` steps from freshly

@@ -53,6 +53,8 @@ SIGNATURES = [
     ("ndg_get_tuning", i, [vp, vp, vp]),
     ("ndg_set_gather_depth", i, [vp, i]),
     ("ndg_get_gather_depth", i, [vp, vp]),
+    ("ndg_set_list_split", i, [vp, i, i]),
+    ("ndg_get_list_split", i, [vp, vp, vp]),
     ("ndg_autotune", i, [vp, i]),
     ("ndg_autotune_skin", i, [vp, i, vp]),
     ("ndg_device_bytes", i, [vp, vp]),

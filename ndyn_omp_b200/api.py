@@ -381,6 +381,18 @@ class Context:
         _ok(self.L.ndg_autotune(self._c, int(steps)), "autotune")
         return self.tuning()
 
+    def set_list_split(self, rows, tpa_long=2):
+        """atoms to threads by list length (ndg_set_list_split): systems whose
+        mean list length reaches `rows` run with `tpa_long` threads per atom;
+        rows = 0: one class"""
+        _ok(self.L.ndg_set_list_split(self._c, int(rows), int(tpa_long)), "set_list_split")
+
+    def list_split(self):
+        """(rows threshold, threads per atom of the long-list class)"""
+        r, t = ctypes.c_int(), ctypes.c_int()
+        _ok(self.L.ndg_get_list_split(self._c, ctypes.byref(r), ctypes.byref(t)), "get_list_split")
+        return r.value, t.value
+
     def autotune_skin(self, steps=60):
         """The rebuild-interval autotuner (ndg_autotune_skin): a list skin
         per fixed-semantics system from a trial of `steps` steps, which is

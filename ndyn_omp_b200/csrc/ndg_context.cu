@@ -145,6 +145,9 @@ struct ndg_ctx {
   // tuning and graphs
   int tpa = 0, graph_steps = 100;
   int gather = 4;  // mixed pair loop gather depth (4 or 8)
+  // atoms to threads by list length: systems whose mean full-list length
+  // reaches rows_split run with tpa_long threads per atom (0: one class)
+  int rows_split = 0, tpa_long = 2;
   int any_spring = 0;  // some system holds spring pairs
   int any_neimax = 0;  // some system checks the reference's NeiMax at list builds
   int stab_smem = 0;  // staged-table bytes of the pair kernel (0: tables from global)
@@ -243,6 +246,9 @@ DevCtx devctx(ndg_ctx *c) {
   d.plan = c->plan;
   d.plan_kb = c->plan_kb;
   d.plan_hdr = c->plan_hdr;
+  // the spring variant is built for one thread per atom: one class
+  d.rows_split = c->any_spring ? 0 : c->rows_split;
+  d.tpa_long = c->tpa_long;
   d.ring_cap = c->ring_cap;
   d.stab_smem = c->stab_smem;
   d.stab_lean = c->stab_lean;
@@ -335,8 +341,8 @@ int grow_sys(ndg_ctx *c, int n) {
   rc |= grow(c, c->dP, (size_t)c->nsys_cap, (size_t)n);
   rc |= grow(c, c->dS, (size_t)c->nsys_cap, (size_t)n);
   rc |= grow(c, c->rb_list, 0, (size_t)n);
-  rc |= grow(c, c->plan, 0, 2 * (size_t)n);
-  if (!c->plan_kb) rc |= grow(c, c->plan_kb, 0, 2 * (size_t)PLAN_GMAX);
+  rc |= grow(c, c->plan, 0, (size_t)PLAN_NL * n);
+  if (!c->plan_kb) rc |= grow(c, c->plan_kb, 0, (size_t)PLAN_NL * PLAN_GMAX);
   if (!c->plan_hdr) rc |= grow(c, c->plan_hdr, 0, 1);
   if (rc) return NDG_ERR_NOMEM;
   drop_graphs(c);
@@ -1895,6 +1901,22 @@ int ndg_get_gather_depth(ndg_ctx *c, int *depth) {
   return NDG_OK;
 }
 
+int ndg_set_list_split(ndg_ctx *c, int rows, int tpa_long) {
+  if (!c || rows < 0 || (tpa_long != 1 && tpa_long != 2 && tpa_long != 4 && tpa_long != 8))
+    return NDG_ERR_ARG;
+  if (rows != c->rows_split || tpa_long != c->tpa_long) drop_graphs(c);
+  c->rows_split = rows;
+  c->tpa_long = tpa_long;
+  return NDG_OK;
+}
+
+int ndg_get_list_split(ndg_ctx *c, int *rows, int *tpa_long) {
+  if (!c) return NDG_ERR_ARG;
+  if (rows) *rows = c->rows_split;
+  if (tpa_long) *tpa_long = c->tpa_long;
+  return NDG_OK;
+}
+
 int ndg_get_tuning(ndg_ctx *c, int *tpa, int *graph_steps) {
   if (!c) return NDG_ERR_ARG;
   if (tpa) *tpa = choose_tpa(c);
@@ -1990,6 +2012,8 @@ int ndg_autotune(ndg_ctx *c, int steps) {
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   const int keep_tpa = c->tpa, keep_gather = c->gather;
+  const int keep_split = c->rows_split, keep_long = c->tpa_long;
+  c->rows_split = 0;  // the launch shapes are timed as one class
   int best = 0, best_g = 4;
   float best_ms = 0.f;
   cudaError_t ce = copy(true);
@@ -2021,11 +2045,59 @@ int ndg_autotune(ndg_ctx *c, int steps) {
     }
     ce = copy(false);
   }
+  c->tpa = best ? best : keep_tpa;
+  c->gather = best ? best_g : keep_gather;
+  // atoms to threads by list length: where the systems' mean list lengths
+  // (rows of a tile at their last build) spread by 1.5x or more, a class of
+  // the long-list systems with 2 or 4 times the threads per atom, kept if
+  // its trial beats the best single shape
+  if (best && ce == cudaSuccess && rc == NDG_OK && !c->any_spring) {
+    std::vector<SysState> S(c->nsys_cap);
+    ce = cudaMemcpy(S.data(), c->dS, S.size() * sizeof(SysState), cudaMemcpyDeviceToHost);
+    double rmin = 1e30, rmax = 0.0;
+    for (size_t s = 0; s < c->sys.size() && ce == cudaSuccess; ++s) {
+      const HostSys &h = c->sys[s];
+      if (!h.alive || h.n == 0) continue;
+      const double nt = (double)h.prm.npad / 128.0;
+      const double r = (double)S[s].rows / nt;
+      rmin = std::min(rmin, r);
+      rmax = std::max(rmax, r);
+    }
+    if (ce == cudaSuccess && rmax > 0.0 && rmax >= 1.5 * rmin) {
+      const int split = (int)std::ceil(std::sqrt(rmin * rmax));
+      int best_long = 0;
+      for (int mul = 2; mul <= 4 && c->tpa * mul <= 8 && rc == NDG_OK && ce == cudaSuccess;
+           mul *= 2) {
+        c->rows_split = split;
+        c->tpa_long = c->tpa * mul;
+        drop_graphs(c);
+        CK(c, cudaMemset(c->ring_count, 0, 4 * sizeof(int)));
+        DevCtx d = devctx(c);
+        launch_arm(d, c->st, c->nsys_cap, -1, 2 * steps, START_NEW);
+        rc = run_blocks(c, steps, nullptr, nullptr);
+        if (rc) break;
+        cudaEventRecord(e0, c->st);
+        rc = run_blocks(c, steps, nullptr, nullptr);
+        cudaEventRecord(e1, c->st);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (!rc && ms < best_ms) {
+          best_ms = ms;
+          best_long = c->tpa_long;
+        }
+        ce = copy(false);
+      }
+      c->rows_split = best_long ? split : 0;
+      c->tpa_long = best_long ? best_long : keep_long;
+    }
+  } else if (!best) {
+    c->rows_split = keep_split;
+    c->tpa_long = keep_long;
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   CK(c, cudaMemset(c->ring_count, 0, 4 * sizeof(int)));
-  c->tpa = best ? best : keep_tpa;
-  c->gather = best ? best_g : keep_gather;
   drop_graphs(c);
   if (ce != cudaSuccess) return cuda_fail(c, ce, "autotune snapshot");
   return rc;

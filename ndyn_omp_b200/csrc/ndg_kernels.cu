@@ -114,13 +114,15 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double *sm /*NV*32*/)
 // over tiles.
 constexpr int TILE_OVH = 16;
 
-__device__ void plan_block(const DevCtx &c, int g0, int g1) {
-  __shared__ long long w_cost[2][32];
-  __shared__ int w_cnt[2][32];
-  __shared__ long long carry_cost[2];
-  __shared__ int carry_cnt[2];
+// NL launches: 2 (energy/virial or not) with one list-length class, 4 with two
+template <int NL>
+__device__ void plan_block(const DevCtx &c, const int *g /*NL grids*/) {
+  __shared__ long long w_cost[NL][32];
+  __shared__ int w_cnt[NL][32];
+  __shared__ long long carry_cost[NL];
+  __shared__ int carry_cnt[NL];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  if (threadIdx.x < 2) {
+  if (threadIdx.x < NL) {
     carry_cost[threadIdx.x] = 0;
     carry_cnt[threadIdx.x] = 0;
   }
@@ -135,59 +137,75 @@ __device__ void plan_block(const DevCtx &c, int g0, int g1) {
       const int f = S->flags;  // F_DONE of the last step is being cleared
       if (P->n > 0 && (f & F_ACTIVE)) {
         const long long nt = P->npad / TILE;
-        L = (f & (F_CU | F_CV)) ? 1 : 0;
-        cpt = (int)((S->rows + nt / 2) / nt) + TILE_OVH;
+        const int rows = (int)((S->rows + nt / 2) / nt);  // mean list rows of a tile
+        // atoms to threads by list length: the long-list class runs with
+        // more threads per atom
+        const int cls = (NL > 2 && rows >= c.rows_split) ? 1 : 0;
+        L = ((f & (F_CU | F_CV)) ? 1 : 0) + 2 * cls;
+        cpt = rows + TILE_OVH;
         cost = nt * cpt;
       }
     }
-    // block-wide inclusive scans of (systems, cost) of both launches
-    int n0 = L == 0, n1 = L == 1;
-    long long q0 = L == 0 ? cost : 0, q1 = L == 1 ? cost : 0;
+    // block-wide inclusive scans of (systems, cost) of every launch
+    int n[NL];
+    long long q[NL];
+#pragma unroll
+    for (int l = 0; l < NL; ++l) {
+      n[l] = L == l;
+      q[l] = L == l ? cost : 0;
+    }
     for (int o = 1; o < 32; o <<= 1) {
-      const int y0 = __shfl_up_sync(0xffffffffu, n0, o), y1 = __shfl_up_sync(0xffffffffu, n1, o);
-      const long long z0 = __shfl_up_sync(0xffffffffu, q0, o);
-      const long long z1 = __shfl_up_sync(0xffffffffu, q1, o);
-      if (lane >= o) {
-        n0 += y0;
-        n1 += y1;
-        q0 += z0;
-        q1 += z1;
+#pragma unroll
+      for (int l = 0; l < NL; ++l) {
+        const int y = __shfl_up_sync(0xffffffffu, n[l], o);
+        const long long z = __shfl_up_sync(0xffffffffu, q[l], o);
+        if (lane >= o) {
+          n[l] += y;
+          q[l] += z;
+        }
       }
     }
     if (lane == 31) {
-      w_cnt[0][warp] = n0;
-      w_cnt[1][warp] = n1;
-      w_cost[0][warp] = q0;
-      w_cost[1][warp] = q1;
+#pragma unroll
+      for (int l = 0; l < NL; ++l) {
+        w_cnt[l][warp] = n[l];
+        w_cost[l][warp] = q[l];
+      }
     }
     __syncthreads();
     if (warp == 0) {
-      int a0 = lane < nw ? w_cnt[0][lane] : 0, a1 = lane < nw ? w_cnt[1][lane] : 0;
-      long long b0 = lane < nw ? w_cost[0][lane] : 0, b1 = lane < nw ? w_cost[1][lane] : 0;
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y0 = __shfl_up_sync(0xffffffffu, a0, o), y1 = __shfl_up_sync(0xffffffffu, a1, o);
-        const long long z0 = __shfl_up_sync(0xffffffffu, b0, o);
-        const long long z1 = __shfl_up_sync(0xffffffffu, b1, o);
-        if (lane >= o) {
-          a0 += y0;
-          a1 += y1;
-          b0 += z0;
-          b1 += z1;
+#pragma unroll
+      for (int l = 0; l < NL; ++l) {
+        int a = lane < nw ? w_cnt[l][lane] : 0;
+        long long b = lane < nw ? w_cost[l][lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, a, o);
+          const long long z = __shfl_up_sync(0xffffffffu, b, o);
+          if (lane >= o) {
+            a += y;
+            b += z;
+          }
         }
+        w_cnt[l][lane] = a;
+        w_cost[l][lane] = b;
       }
-      w_cnt[0][lane] = a0;
-      w_cnt[1][lane] = a1;
-      w_cost[0][lane] = b0;
-      w_cost[1][lane] = b1;
     }
     __syncthreads();
     if (L >= 0) {
-      const int k = carry_cnt[L] + (warp ? w_cnt[L][warp - 1] : 0) + (L ? n1 : n0) - 1;
-      const long long cum = carry_cost[L] + (warp ? w_cost[L][warp - 1] : 0) + (L ? q1 : q0) - cost;
+      int nl = 0;
+      long long ql = 0;
+#pragma unroll
+      for (int l = 0; l < NL; ++l)
+        if (l == L) {
+          nl = n[l];
+          ql = q[l];
+        }
+      const int k = carry_cnt[L] + (warp ? w_cnt[L][warp - 1] : 0) + nl - 1;
+      const long long cum = carry_cost[L] + (warp ? w_cost[L][warp - 1] : 0) + ql - cost;
       c.plan[(size_t)L * c.nsys_cap + k] = PlanEnt{cum, s, cpt};
     }
     __syncthreads();
-    if (threadIdx.x < 2) {
+    if (threadIdx.x < NL) {
       carry_cnt[threadIdx.x] += w_cnt[threadIdx.x][nw - 1];
       carry_cost[threadIdx.x] += w_cost[threadIdx.x][nw - 1];
     }
@@ -195,8 +213,8 @@ __device__ void plan_block(const DevCtx &c, int g0, int g1) {
   }
   // block b of launch L starts in the entry whose cost range holds
   // lo_b = floor(b * tot / G): the blocks with cum * G <= b * tot < end * G
-  for (int L = 0; L < 2; ++L) {
-    const int m = carry_cnt[L], G = L ? g1 : g0;
+  for (int L = 0; L < NL; ++L) {
+    const int m = carry_cnt[L], G = g[L];
     const long long tot = carry_cost[L];
     const PlanEnt *pl = c.plan + (size_t)L * c.nsys_cap;
     for (int k = threadIdx.x; k < m; k += blockDim.x) {
@@ -205,7 +223,7 @@ __device__ void plan_block(const DevCtx &c, int g0, int g1) {
       for (long long b = b0; b < b1 && b < G; ++b) c.plan_kb[L * PLAN_GMAX + b] = k;
     }
   }
-  if (threadIdx.x < 2) {
+  if (threadIdx.x < NL) {
     c.plan_hdr->tot[threadIdx.x] = carry_cost[threadIdx.x];
     c.plan_hdr->m[threadIdx.x] = carry_cnt[threadIdx.x];
   }
@@ -217,10 +235,12 @@ __device__ void plan_block(const DevCtx &c, int g0, int g1) {
 // Emits each chunk's two largest displacement measures for the next
 // CheckListUpdate.  A dynamics step's launch has one more block, which
 // plans the step's pair launches.
-__global__ __launch_bounds__(BLOCK) void k_integrate1(DevCtx c, int standalone, int mixed, int g0,
-                                                     int g1) {
+__global__ __launch_bounds__(BLOCK) void k_integrate1(DevCtx c, int standalone, int mixed,
+                                                     int4 grids) {
   if (blockIdx.x == c.nchunks) {  // the extra block of a dynamics step
-    plan_block(c, g0, g1);
+    const int g[PLAN_NL] = {grids.x, grids.y, grids.z, grids.w};
+    if (c.rows_split > 0) plan_block<4>(c, g);
+    else plan_block<2>(c, g);
     return;
   }
   const int chunk = blockIdx.x;
@@ -1560,7 +1580,7 @@ template <int TPA, bool MIXED, bool FUSE, bool STAB, bool EV, int GATHER, bool S
 __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 / (TILE * TPA)) > 0
                                              ? pair_ctas<MIXED, EV, GATHER>() * 128 / (TILE * TPA)
                                              : 1) void k_pair(DevCtx c, int host_flags, int ntiles,
-                                                     unsigned long long next_h) {
+                                                     unsigned long long next_h, int cls) {
   constexpr int NT = TILE * TPA;
   extern __shared__ __align__(16) unsigned char dsm[];
   // mixed EV: 7 fixed-point slots (energy, virial) per thread, after the tables
@@ -1571,7 +1591,7 @@ __global__ __launch_bounds__(TILE * TPA, (pair_ctas<MIXED, EV, GATHER>() * 128 /
   // one or two systems), in standalone compute0 an even split of all tiles
   // (only tcur, tend and the plan entry kk stay live across tiles; the
   // block's cost range is worked out again where a system starts)
-  constexpr int L = EV ? 1 : 0;
+  const int L = (EV ? 1 : 0) + 2 * cls;  // this launch's plan
   int tcur = 0, tend = 0, kk = -1;
   if (FUSE) {
     const long long tot = c.plan_hdr->tot[L];
@@ -2176,12 +2196,12 @@ static void pair_grids(const DevCtx &c, int tpa, int mixed, int *g);
 
 void launch_integrate1(const DevCtx &c, cudaStream_t st, int standalone, int mixed, int tpa) {
   if (standalone || !c.plan_hdr) {
-    k_integrate1<<<c.nchunks, BLOCK, 0, st>>>(c, standalone, mixed, 0, 0);
+    k_integrate1<<<c.nchunks, BLOCK, 0, st>>>(c, standalone, mixed, make_int4(0, 0, 0, 0));
     return;
   }
-  int g[2];
+  int g[PLAN_NL] = {0, 0, 0, 0};
   pair_grids(c, tpa, mixed, g);
-  k_integrate1<<<c.nchunks + 1, BLOCK, 0, st>>>(c, 0, mixed, g[0], g[1]);
+  k_integrate1<<<c.nchunks + 1, BLOCK, 0, st>>>(c, 0, mixed, make_int4(g[0], g[1], g[2], g[3]));
 }
 
 static int sm_count() {
@@ -2199,7 +2219,7 @@ static int sm_count() {
 // set, also launches it
 template <int TPA, bool MIXED, bool FUSE, bool STAB, bool EV, int GATHER, bool SPRING = false>
 static int pair_launch(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh,
-                       bool launch) {
+                       bool launch, int cls) {
   auto kern = k_pair<TPA, MIXED, FUSE, STAB, EV, GATHER, SPRING>;
   const int smem = (STAB ? c.stab_lean : 0) + ((MIXED && EV) ? 7 * 8 * TILE * TPA : 0);
   static int cfg_smem = -1, occ = 0;
@@ -2227,69 +2247,81 @@ static int pair_launch(const DevCtx &c, cudaStream_t st, int hf, unsigned long l
   const int nsm = sm_count();
   const int ntiles = c.nchunks * (ATOM_ALIGN / TILE);
   const int grid = std::min(std::min(ntiles, nsm * occ), PLAN_GMAX);
-  if (launch) kern<<<grid, TILE * TPA, smem, st>>>(c, hf, ntiles, nh);
+  if (launch) kern<<<grid, TILE * TPA, smem, st>>>(c, hf, ntiles, nh, cls);
   return grid;
 }
 
 // the deeper gather only for the mixed one-thread-per-atom loop
 template <int TPA, bool MIXED, bool FUSE, bool STAB, bool EV>
-static int pair_go(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh,
-                   bool launch = true) {
+static int pair_go(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh, bool launch,
+                   int cls) {
   if constexpr (TPA == 1) {
-    if (c.any_spring) return pair_launch<1, MIXED, FUSE, STAB, EV, 4, true>(c, st, hf, nh, launch);
+    if (c.any_spring)
+      return pair_launch<1, MIXED, FUSE, STAB, EV, 4, true>(c, st, hf, nh, launch, cls);
   }
   if (MIXED && TPA == 1 && c.gather > 4)
-    return pair_launch<TPA, MIXED, FUSE, STAB, EV, 8>(c, st, hf, nh, launch);
-  return pair_launch<TPA, MIXED, FUSE, STAB, EV, 4>(c, st, hf, nh, launch);
+    return pair_launch<TPA, MIXED, FUSE, STAB, EV, 8>(c, st, hf, nh, launch, cls);
+  return pair_launch<TPA, MIXED, FUSE, STAB, EV, 4>(c, st, hf, nh, launch, cls);
 }
 
 // FUSE (a dynamics step, after the integrate1 that planned it): the kernel
-// without energy/virial takes the systems whose step needs neither, the EV
-// kernel the others.  Standalone compute0: the host flags choose.  With g
-// set, only the two dynamics grids are worked out.
+// without energy/virial takes the class's systems whose step needs neither,
+// the EV kernel the others.  Standalone compute0: the host flags choose.
+// With g set, only the class's two dynamics grids are worked out.
 template <int TPA, bool MIXED, bool FUSE, bool STAB>
-static void pair_ev(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh, int *g) {
+static void pair_ev(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh, int *g,
+                    int cls) {
   if (g) {
-    g[0] = pair_go<TPA, MIXED, FUSE, STAB, false>(c, st, hf, nh, false);
-    g[1] = pair_go<TPA, MIXED, FUSE, STAB, true>(c, st, hf, nh, false);
+    g[2 * cls] = pair_go<TPA, MIXED, FUSE, STAB, false>(c, st, hf, nh, false, cls);
+    g[2 * cls + 1] = pair_go<TPA, MIXED, FUSE, STAB, true>(c, st, hf, nh, false, cls);
   } else if (FUSE) {
     if (!c.plan_hdr) return;  // no system was ever added
-    pair_go<TPA, MIXED, FUSE, STAB, false>(c, st, hf, nh);
-    pair_go<TPA, MIXED, FUSE, STAB, true>(c, st, hf, nh);
+    pair_go<TPA, MIXED, FUSE, STAB, false>(c, st, hf, nh, true, cls);
+    pair_go<TPA, MIXED, FUSE, STAB, true>(c, st, hf, nh, true, cls);
   } else if (hf & (F_CU | F_CV)) {
-    pair_go<TPA, MIXED, FUSE, STAB, true>(c, st, hf, nh);
+    pair_go<TPA, MIXED, FUSE, STAB, true>(c, st, hf, nh, true, 0);
   } else {
-    pair_go<TPA, MIXED, FUSE, STAB, false>(c, st, hf, nh);
+    pair_go<TPA, MIXED, FUSE, STAB, false>(c, st, hf, nh, true, 0);
   }
 }
 
 template <int TPA, bool MIXED, bool FUSE>
-static void pair_mode(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh, int *g) {
-  if (c.stab_smem <= 0) pair_ev<TPA, MIXED, FUSE, false>(c, st, hf, nh, g);
-  else pair_ev<TPA, MIXED, FUSE, true>(c, st, hf, nh, g);
+static void pair_mode(const DevCtx &c, cudaStream_t st, int hf, unsigned long long nh, int *g,
+                      int cls) {
+  if (c.stab_smem <= 0) pair_ev<TPA, MIXED, FUSE, false>(c, st, hf, nh, g, cls);
+  else pair_ev<TPA, MIXED, FUSE, true>(c, st, hf, nh, g, cls);
 }
 
 template <int TPA>
 static void pair_tpa(const DevCtx &c, cudaStream_t st, int mixed, int fuse, int hf,
-                     unsigned long long nh, int *g) {
+                     unsigned long long nh, int *g, int cls) {
   if (mixed) {
-    if (fuse) pair_mode<TPA, true, true>(c, st, hf, nh, g);
-    else pair_mode<TPA, true, false>(c, st, hf, nh, g);
+    if (fuse) pair_mode<TPA, true, true>(c, st, hf, nh, g, cls);
+    else pair_mode<TPA, true, false>(c, st, hf, nh, g, cls);
   } else {
-    if (fuse) pair_mode<TPA, false, true>(c, st, hf, nh, g);
-    else pair_mode<TPA, false, false>(c, st, hf, nh, g);
+    if (fuse) pair_mode<TPA, false, true>(c, st, hf, nh, g, cls);
+    else pair_mode<TPA, false, false>(c, st, hf, nh, g, cls);
   }
 }
 
-static void pair_dispatch(const DevCtx &c, cudaStream_t st, int tpa, int mixed, int fuse, int hf,
-                          unsigned long long next_h, int *g) {
+static void pair_class(const DevCtx &c, cudaStream_t st, int tpa, int mixed, int fuse, int hf,
+                       unsigned long long next_h, int *g, int cls) {
   if (c.any_spring) tpa = 1;  // the spring variant is built for one thread per atom
   switch (tpa) {
-    case 1: pair_tpa<1>(c, st, mixed, fuse, hf, next_h, g); break;
-    case 2: pair_tpa<2>(c, st, mixed, fuse, hf, next_h, g); break;
-    case 4: pair_tpa<4>(c, st, mixed, fuse, hf, next_h, g); break;
-    default: pair_tpa<8>(c, st, mixed, fuse, hf, next_h, g); break;
+    case 1: pair_tpa<1>(c, st, mixed, fuse, hf, next_h, g, cls); break;
+    case 2: pair_tpa<2>(c, st, mixed, fuse, hf, next_h, g, cls); break;
+    case 4: pair_tpa<4>(c, st, mixed, fuse, hf, next_h, g, cls); break;
+    default: pair_tpa<8>(c, st, mixed, fuse, hf, next_h, g, cls); break;
   }
+}
+
+// A dynamics step launches each list-length class (the long-list class
+// only while a threshold is set: DevCtx::rows_split, DevCtx::tpa_long);
+// standalone compute0 one launch over all tiles.
+static void pair_dispatch(const DevCtx &c, cudaStream_t st, int tpa, int mixed, int fuse, int hf,
+                          unsigned long long next_h, int *g) {
+  pair_class(c, st, tpa, mixed, fuse, hf, next_h, g, 0);
+  if (fuse && c.rows_split > 0) pair_class(c, st, c.tpa_long, mixed, fuse, hf, next_h, g, 1);
 }
 
 void launch_pair(const DevCtx &c, cudaStream_t st, int tpa, int mixed, int fuse, int hf,
@@ -2297,7 +2329,7 @@ void launch_pair(const DevCtx &c, cudaStream_t st, int tpa, int mixed, int fuse,
   pair_dispatch(c, st, tpa, mixed, fuse, hf, next_h, nullptr);
 }
 
-// the grids of a dynamics step's two pair launches
+// the grids of a dynamics step's pair launches
 static void pair_grids(const DevCtx &c, int tpa, int mixed, int *g) {
   pair_dispatch(c, 0, tpa, mixed, 1, 0, 0ull, g);
 }

@@ -14,9 +14,13 @@ struct PlanEnt {
   long long cum;  // cost of the launch's earlier systems
   int sys, cpt;   // system, cost of one of its tiles
 };
+// A dynamics step's pair launches: (energy/virial or not) x (list-length
+// class: 1 for systems whose mean list length reaches DevCtx::rows_split,
+// which run with DevCtx::tpa_long threads per atom); launch L = ev + 2 cls.
+constexpr int PLAN_NL = 4;
 struct PlanHdr {
-  long long tot[2];  // total cost of each launch
-  int m[2];          // systems of each launch
+  long long tot[PLAN_NL];  // total cost of each launch
+  int m[PLAN_NL];          // systems of each launch
 };
 constexpr int PLAN_GMAX = 8192;  // largest pair-kernel grid the plan covers
 
@@ -63,7 +67,9 @@ struct DevCtx {
                     // [2] largest tile candidate count, [3] systems on rb_list
   int *rb_list;     // systems whose lists the next rebuild group rebuilds
   PlanEnt *plan;    // 2 x nsys_cap entries
-  int *plan_kb;     // 2 x PLAN_GMAX block starts
+  int *plan_kb;     // PLAN_NL x PLAN_GMAX block starts
+  int rows_split;   // list-length class threshold (mean entries per atom; 0: one class)
+  int tpa_long;     // threads per atom of the long-list class
   PlanHdr *plan_hdr;
   int ring_cap;
 };

@@ -493,6 +493,62 @@ def test_large_system_run_follows_oracle(large_liquid):
         assert a["ke"] == pytest.approx(b["ke"], rel=1e-5)
 
 
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
+def test_list_split_by_length(specs, prec):
+    """Atoms to threads by list length: a context of an Ar liquid (~70
+    entries per atom), a Cu crystal (~90) and a rocksalt solid (~130), its
+    long-list systems in launches of their own with 2 or 4 threads per atom.
+    Mixed precision: the same bits as one class (the fixed-point chunk sums
+    do not depend on the threads); FP64: within the summation-order bar."""
+    systems = [specs["ar_fixed"], specs["cu_ref"], specs["nacl_fixed"]]
+    out = []
+    for split, tl in ((0, 2), (100, 2), (100, 4)):
+        with nd.Context(0, prec) as ctx:
+            ids = [gpu_from_spec(ctx, sp) for sp in systems]
+            ctx.set_tuning(1, 100)
+            ctx.set_list_split(split, tl)
+            assert ctx.list_split() == (split, tl)
+            rows = ctx.run(40)
+            out.append(([ctx.state(i) for i in ids], rows))
+    for k in (1, 2):
+        for sa, sb in zip(out[0][0], out[k][0]):
+            for a, b in zip(sa, sb):
+                if prec == "mixed":
+                    assert np.array_equal(a, b)
+                else:
+                    assert np.allclose(a, b, rtol=1e-9, atol=1e-11)
+        if prec == "mixed":
+            assert out[0][1] == out[k][1]
+        else:
+            for ra, rb in zip(out[0][1], out[k][1]):
+                assert ra["pe"] == pytest.approx(rb["pe"], rel=1e-10)
+
+
+def test_autotune_split_restores_state(specs):
+    """The autotuner's list-length trials leave no trace either (systems of
+    mean list lengths 1.5x apart), and the split it keeps, if any, changes no
+    bit of a mixed run."""
+    systems = [specs["ar_fixed"], specs["nacl_fixed"]]
+    res = []
+    for tune in (False, True):
+        with nd.Context(0, "mixed") as ctx:
+            ids = [gpu_from_spec(ctx, sp) for sp in systems]
+            ctx.run(20)
+            before = [ctx.state(i) for i in ids]
+            if tune:
+                ctx.autotune(10)
+                for i, b in zip(ids, before):
+                    for x, y in zip(ctx.state(i), b):
+                        assert np.array_equal(x, y)
+                r, t = ctx.list_split()
+                assert r >= 0 and t in (1, 2, 4, 8)
+            res.append(([ctx.state(i) for i in ids], ctx.run(30, cont=True)))
+    for sa, sb in zip(res[0][0], res[1][0]):
+        for a, b in zip(sa, sb):
+            assert np.array_equal(a, b)
+    assert res[0][1] == res[1][1]
+
+
 def test_autotune_restores_state(specs):
     """The autotuner's trial steps leave no trace: the state after tuning
     equals the state before it, and a continued run equals one without
