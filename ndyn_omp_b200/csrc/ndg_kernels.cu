@@ -235,8 +235,10 @@ __device__ void plan_block(const DevCtx &c, const int *g /*NL grids*/) {
 // Emits each chunk's two largest displacement measures for the next
 // CheckListUpdate.  A dynamics step's launch has one more block, which
 // plans the step's pair launches.
-__global__ __launch_bounds__(BLOCK) void k_integrate1(DevCtx c, int standalone, int mixed,
-                                                     int4 grids) {
+// (six blocks per SM: the streaming body's registers; the planning block's
+// scans may spill, one block of the launch)
+__global__ __launch_bounds__(BLOCK, 6) void k_integrate1(DevCtx c, int standalone, int mixed,
+                                                        int4 grids) {
   if (blockIdx.x == c.nchunks) {  // the extra block of a dynamics step
     const int g[PLAN_NL] = {grids.x, grids.y, grids.z, grids.w};
     if (c.rows_split > 0) plan_block<4>(c, g);
