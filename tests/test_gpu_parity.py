@@ -493,6 +493,39 @@ def test_large_system_run_follows_oracle(large_liquid):
         assert a["ke"] == pytest.approx(b["ke"], rel=1e-5)
 
 
+@pytest.mark.parametrize("quirk", ["ref", "fixed"])
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-10), ("mixed", 1e-5)])
+def test_cutoff_shell_decided_like_the_oracle(prec, tol, quirk):
+    """Pairs on the cutoff: an FCC Morse lattice stretched so that its fourth
+    neighbour shell (12 atoms at a*sqrt(2)) lies at the 6.0 A cutoff, the
+    atoms displaced by at most 1e-7 A.  Every such pair's FP32 squared
+    distance is within the mixed loop's 1e-5 band, so the reference's FP64
+    test (compute0, src/nd.f90:283-296) must decide it, in the full chunks'
+    f32x2 path and in the masked tail alike (54 list entries per atom).  A
+    pair decided the other way would move two forces by the Morse force at
+    the cutoff, ~1.3e-2 eV/A; the bar is 1e-5 eV/A (1e-10 in FP64)."""
+    rng = np.random.default_rng(31)
+    a = 6.0 / np.sqrt(2.0)
+    pos, box = W.lattice((6, 6, 6), a, W.FCC_BASIS)
+    pos = W.jitter(pos, box, 1e-7, rng)
+    n = len(pos)
+    spec = dict(masses=W.CU_MORSE["masses"], pairs=W.CU_MORSE["pairs"],
+                typ=np.ones(n, np.int32), pos=pos, box=box, vel=np.zeros((n, 3)),
+                control=dict(dt=0.1, skin=0.5, out_steps=100, quirk=quirk))
+    o = oracle_from_spec(spec)
+    assert o.setup_lists() == 0
+    o.compute(1, 1)
+    fo, peo, _, _ = o.forces()
+    with nd.Context(0, prec) as ctx:
+        sid = gpu_from_spec(ctx, spec)
+        ctx.setup_lists()
+        assert ctx.neighbor_count(sid) == 54 * n  # shells 1-4 within rcut + skin
+        ctx.compute0(True, True)
+        fg, peg, _, _ = ctx.forces(sid)
+    assert np.max(np.abs(np.asarray(fg) - np.asarray(fo))) < tol
+    assert abs(peg - peo) <= (1e-12 if prec == "fp64" else 1e-7) * abs(peo)
+
+
 @pytest.mark.parametrize("prec", ["mixed", "fp64"])
 def test_list_split_by_length(specs, prec):
     """Atoms to threads by list length: a context of an Ar liquid (~70
