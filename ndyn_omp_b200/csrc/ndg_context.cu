@@ -969,7 +969,13 @@ int run_blocks(ndg_ctx *c, int nsteps, ndg_thermo_cb cb, void *user, bool flush_
 
 int flush_pending(ndg_ctx *c, int sys = -1) {
   DevCtx d = devctx(c);
-  launch_flush(d, c->st, c->nsys_cap, sys);
+  if (sys >= 0) {
+    // the system's own chunks only (a context may hold thousands of systems)
+    const HostSys &h = c->sys[sys];
+    launch_flush(d, c->st, c->nsys_cap, sys, (int)h.atoms.off, (int)h.atoms.len);
+  } else {
+    launch_flush(d, c->st, c->nsys_cap, -1);
+  }
   CK(c, cudaGetLastError());
   CK(c, cudaStreamSynchronize(c->st));
   return NDG_OK;

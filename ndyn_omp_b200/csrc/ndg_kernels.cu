@@ -572,8 +572,8 @@ __global__ void k_begin_block(DevCtx c, int nsys_cap, int K) {
 }
 
 // apply pending mkIsoKE/mkIsoE velocity scales at the end of a run
-__global__ __launch_bounds__(BLOCK) void k_flush(DevCtx c, int only) {
-  const int chunk = blockIdx.x;
+__global__ __launch_bounds__(BLOCK) void k_flush(DevCtx c, int only, int chunk0) {
+  const int chunk = chunk0 + blockIdx.x;
   const int sys = c.chunk_sys[chunk];
   if (sys < 0 || (only >= 0 && sys != only)) return;
   const SysParam *__restrict__ P = c.P + sys;
@@ -2461,8 +2461,10 @@ void launch_begin_block(const DevCtx &c, cudaStream_t st, int nsys_cap, int K) {
 }
 
 // apply and clear the pending velocity scales of every system (sys < 0) or one
-void launch_flush(const DevCtx &c, cudaStream_t st, int nsys_cap, int sys) {
-  k_flush<<<c.nchunks, BLOCK, 0, st>>>(c, sys);
+// sys >= 0: only that system's chunks [chunk0, chunk0 + nch) are launched
+void launch_flush(const DevCtx &c, cudaStream_t st, int nsys_cap, int sys, int chunk0, int nch) {
+  if (sys >= 0 && nch > 0) k_flush<<<nch, BLOCK, 0, st>>>(c, sys, chunk0);
+  else if (sys < 0) k_flush<<<c.nchunks, BLOCK, 0, st>>>(c, -1, 0);
   k_clear_pend<<<(nsys_cap + 127) / 128, 128, 0, st>>>(c, nsys_cap, sys);
 }
 

@@ -87,7 +87,8 @@ void launch_integrate2(const DevCtx &c, cudaStream_t st, int ck);
 void launch_rebuild(const DevCtx &c, cudaStream_t st, int counting, int mixed);
 void launch_arm(const DevCtx &c, cudaStream_t st, int nsys_cap, int sys, int nsteps, int start);
 void launch_begin_block(const DevCtx &c, cudaStream_t st, int nsys_cap, int K);
-void launch_flush(const DevCtx &c, cudaStream_t st, int nsys_cap, int sys);
+void launch_flush(const DevCtx &c, cudaStream_t st, int nsys_cap, int sys, int chunk0 = 0,
+                  int nch = 0);
 void launch_check(const DevCtx &c, cudaStream_t st, int nsys_cap);
 void launch_scale_vel(const DevCtx &c, cudaStream_t st, int sys, double lam);
 void launch_refresh_pfx(const DevCtx &c, cudaStream_t st);
