@@ -86,7 +86,12 @@ template <class T>
 T *dalloc(size_t n) {
   void *p = nullptr;
   if (n == 0) n = 1;
-  if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
+  if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) {
+    // the caller reports NDG_ERR_NOMEM; the failed call must not stay the
+    // runtime's last error for the next launch's check to pick up
+    cudaGetLastError();
+    return nullptr;
+  }
   return (T *)p;
 }
 
@@ -305,12 +310,14 @@ int grow_atoms(ndg_ctx *c, long long new_chunks) {
     rc |= grow(c, c->tile_rows, t_old, t_new);
     if (!rc) cudaMemset(c->tile_rows + t_old, 0, (t_new - t_old) * sizeof(int));
   }
+  // arrays reallocated before a failure have moved too: no captured graph
+  // may keep their old addresses
+  drop_graphs(c);
   if (rc) return NDG_ERR_NOMEM;
   c->chunk_sys_h.resize(new_chunks, -1);
   cudaMemcpy(c->chunk_sys + c->atoms.cap, c->chunk_sys_h.data() + c->atoms.cap,
              (new_chunks - c->atoms.cap) * sizeof(int), cudaMemcpyHostToDevice);
   c->atoms.cap = new_chunks;
-  drop_graphs(c);
   return NDG_OK;
 }
 
@@ -319,18 +326,21 @@ int grow_cells(ndg_ctx *c, long long n) {
   rc |= grow(c, c->cell_count, (size_t)c->cells.cap, (size_t)n);
   rc |= grow(c, c->cell_start, (size_t)c->cells.cap, (size_t)n);
   rc |= grow(c, c->cell_sys, (size_t)c->cells.cap, (size_t)n);
+  drop_graphs(c);  // arrays reallocated before a failure have moved too
   if (rc) return NDG_ERR_NOMEM;
   cudaMemset(c->cell_count + c->cells.cap, 0, (n - c->cells.cap) * sizeof(int));
   c->cell_sys_h.resize(n, -1);
   cudaMemcpy(c->cell_sys + c->cells.cap, c->cell_sys_h.data() + c->cells.cap,
              (n - c->cells.cap) * sizeof(int), cudaMemcpyHostToDevice);
   c->cells.cap = n;
-  drop_graphs(c);
   return NDG_OK;
 }
 
 int grow_nbr(ndg_ctx *c, long long n) {
-  if (grow(c, c->nbr, (size_t)c->nbrs.cap, (size_t)n)) return NDG_ERR_NOMEM;
+  if (grow(c, c->nbr, (size_t)c->nbrs.cap, (size_t)n)) {
+    drop_graphs(c);
+    return NDG_ERR_NOMEM;
+  }
   c->nbrs.cap = n;
   drop_graphs(c);
   return NDG_OK;
@@ -367,12 +377,31 @@ int grow_sys(ndg_ctx *c, int n) {
 }
 
 // Allocate `len` units in an arena, growing the device buffers if needed.
+// grow an arena of capacity cap to hold need: 2x, else 1.5x, 1.25x, the
+// exact need, the first that the device can allocate
+template <class F>
+int grow_ladder(long long need, long long cap, F grow_to) {
+  static const double steps[] = {2.0, 1.5, 1.25};
+  for (double f : steps) {
+    const long long want = (long long)(f * (double)cap);
+    if (want <= need) break;
+    const int rc = grow_to(want);
+    if (rc != NDG_ERR_NOMEM) return rc;
+  }
+  return grow_to(need);
+}
+
 long long arena_take(ndg_ctx *c, Arena &a, long long len, int which) {
   long long off = a.find(len);
   if (off < 0) {
-    long long want = std::max(a.end_used() + len, 2 * a.cap);  // each growth copies and
-                                                                 // re-captures: double
-    int rc = which == 0 ? grow_atoms(c, want) : which == 1 ? grow_cells(c, want) : grow_nbr(c, want);
+    // each growth copies and re-captures: double, or where the doubled
+    // arena does not fit the device, the largest of 1.5x, 1.25x and the
+    // exact need that does (headroom keeps later admissions from growing
+    // again, each a copy of the whole arena)
+    const long long need = a.end_used() + len;
+    const int rc = grow_ladder(need, a.cap, [&](long long want) {
+      return which == 0 ? grow_atoms(c, want) : which == 1 ? grow_cells(c, want) : grow_nbr(c, want);
+    });
     if (rc) return -1;
     off = a.find(len);
     if (off < 0) return -1;
@@ -1042,7 +1071,7 @@ int reserve_atoms(ndg_ctx *c, long long atoms) {
   const long long need = c->atoms.end_used() + (atoms + ATOM_ALIGN - 1) / ATOM_ALIGN;
   if (need <= c->atoms.cap) return NDG_OK;
   cudaSetDevice(c->device);
-  return grow_atoms(c, std::max(need, 2 * c->atoms.cap));
+  return grow_ladder(need, c->atoms.cap, [&](long long want) { return grow_atoms(c, want); });
 }
 
 int take_system_error(ndg_ctx *c, int sys, int *err) {
