@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
@@ -82,10 +83,22 @@ struct HostSys {
   SysParam prm{};
 };
 
+// Test hook (host-side fault injection): NDG_TEST_ALLOC_LIMIT=<bytes> in the
+// environment makes every device allocation above that size fail as if the
+// device were full, so the growth fallbacks run without filling a GPU.
+size_t alloc_limit() {
+  static const size_t lim = [] {
+    const char *e = getenv("NDG_TEST_ALLOC_LIMIT");
+    return e ? (size_t)strtoull(e, nullptr, 10) : (size_t)0;
+  }();
+  return lim;
+}
+
 template <class T>
 T *dalloc(size_t n) {
   void *p = nullptr;
   if (n == 0) n = 1;
+  if (alloc_limit() && n * sizeof(T) > alloc_limit()) return nullptr;
   if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) {
     // the caller reports NDG_ERR_NOMEM; the failed call must not stay the
     // runtime's last error for the next launch's check to pick up
