@@ -233,19 +233,22 @@ __device__ void plan_block(const DevCtx &c, const int *g /*NL grids*/) {
 // scales left pending by the previous step's mkIsoKE/mkIsoE first
 // (src/nd.f90:1145-1155,1173-1180).
 // Emits each chunk's two largest displacement measures for the next
-// CheckListUpdate.  A dynamics step's launch has one more block, which
-// plans the step's pair launches.
+// CheckListUpdate.  A dynamics step's launch has one more block (its first),
+// which plans the step's pair launches.
 // (six blocks per SM: the streaming body's registers; the planning block's
 // scans may spill, one block of the launch)
 __global__ __launch_bounds__(BLOCK, 6) void k_integrate1(DevCtx c, int standalone, int mixed,
                                                         int4 grids) {
-  if (blockIdx.x == c.nchunks) {  // the extra block of a dynamics step
+  // a dynamics step's launch has one block more, its first, so that the
+  // plan's serial scan runs beside the integration rather than after it
+  const int lead = (!standalone && (int)gridDim.x > c.nchunks) ? 1 : 0;
+  if (lead && blockIdx.x == 0) {
     const int g[PLAN_NL] = {grids.x, grids.y, grids.z, grids.w};
     if (c.rows_split > 0) plan_block<4>(c, g);
     else plan_block<2>(c, g);
     return;
   }
-  const int chunk = blockIdx.x;
+  const int chunk = blockIdx.x - lead;
   const int sys = c.chunk_sys[chunk];
   double t1 = 0.0, t2 = 0.0;
   if (sys >= 0) {
@@ -304,7 +307,7 @@ __global__ __launch_bounds__(BLOCK, 6) void k_integrate1(DevCtx c, int standalon
     }
   }
   // this step's rebuild group is done with the rebuild list
-  if (!standalone && blockIdx.x == 0 && threadIdx.x == 0) c.ring_count[3] = 0;
+  if (!standalone && chunk == 0 && threadIdx.x == 0) c.ring_count[3] = 0;
   // a new step: the system's pair kernel has not run yet (only the block of
   // the system's first chunk writes; the others read flag bits this leaves)
   if (!standalone && sys >= 0 && threadIdx.x == 0 && chunk == c.P[sys].atom_off / ATOM_ALIGN)
