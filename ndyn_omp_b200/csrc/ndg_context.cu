@@ -389,7 +389,6 @@ int grow_sys(ndg_ctx *c, int n) {
   return NDG_OK;
 }
 
-// Allocate `len` units in an arena, growing the device buffers if needed.
 // grow an arena of capacity cap to hold need: 2x, else 1.5x, 1.25x, the
 // exact need, the first that the device can allocate
 template <class F>
@@ -404,6 +403,7 @@ int grow_ladder(long long need, long long cap, F grow_to) {
   return grow_to(need);
 }
 
+// Allocate `len` units in an arena, growing the device buffers if needed.
 long long arena_take(ndg_ctx *c, Arena &a, long long len, int which) {
   long long off = a.find(len);
   if (off < 0) {
