@@ -965,6 +965,19 @@ __device__ __forceinline__ int wrap_step(int x, int d, int M) {
   return y < 0 ? y + M : (y >= M ? y - M : y);
 }
 
+// Stencil entries whose candidate ranges follow one another in memory (an
+// entry's first candidate right after the previous entry's last: the cells
+// of one row of the stencil, or a left-out or empty range between them)
+// pass as one range: the same candidates in the same order, in fuller
+// batches of 32.  The own cell, the one entry that tests PTrMin, stays a
+// range of its own.  Lane e < ne holds entry e; bit e of the result marks
+// the first entry of a range, which runs to the entry before the next mark.
+__device__ __forceinline__ unsigned range_heads(int q0, int q1, int center, int lane, int ne) {
+  const int pq1 = __shfl_up_sync(0xffffffffu, q1, 1);
+  const int pcen = __shfl_up_sync(0xffffffffu, center, 1);
+  return __ballot_sync(0xffffffffu, lane < ne && (lane == 0 || center || pcen || q0 != pq1));
+}
+
 __device__ __forceinline__ void build_cell(const DevCtx &c, int sys, int cell, int lane) {
   const SysParam *__restrict__ P = c.P + sys;
   SysState *S = c.S + sys;
@@ -986,6 +999,7 @@ __device__ __forceinline__ void build_cell(const DevCtx &c, int sys, int cell, i
     e_q1 = cst[nc + 1];
     e_center = (st >> 12) & 1;
   }
+  const unsigned heads = range_heads(e_q0, e_q1, e_center, lane, ne);
   const int aoff = P->atom_off, nt = P->ntypes, maxnb = P->maxnb, nb16 = P->nb16;
   const int *pm = c.pairmat + P->pm_off;
   const double *rl2 = c.rlist2 + P->pair_off;
@@ -1020,9 +1034,12 @@ __device__ __forceinline__ void build_cell(const DevCtx &c, int sys, int cell, i
               hz = __reduce_max_sync(0xffffffffu, own ? oz : INT_MIN);
     int *col = c.nbr + P->nbr_off + (long long)(li / TILE) * maxnb * TILE + (li % TILE);
     int cnt = 0;
-    for (int e = 0; e < ne; ++e) {
+    for (unsigned hd = heads; hd;) {
+      const int e = __ffs(hd) - 1;
+      hd &= hd - 1;
+      const int last = hd ? __ffs(hd) - 2 : ne - 1;
       const bool center = __shfl_sync(0xffffffffu, e_center, e) != 0;
-      const int q1 = __shfl_sync(0xffffffffu, e_q1, e);
+      const int q1 = __shfl_sync(0xffffffffu, e_q1, last);
       for (int qb = __shfl_sync(0xffffffffu, e_q0, e); qb < q1; qb += 32) {
         // 32 candidates at once, one per lane; the lanes test their own
         // candidate against the own atoms' box, then the kept ones pass
@@ -1154,6 +1171,7 @@ __device__ __forceinline__ void build_atom(const DevCtx &c, int sys, int local, 
     }
     if (d2min > (float)(P->rlist * P->rlist) * (1.f + 1e-5f)) e_q1 = e_q0;
   }
+  const unsigned heads = range_heads(e_q0, e_q1, e_center, lane, ne);
   const int nt = P->ntypes, maxnb = P->maxnb, nb16 = P->nb16;
   const int *pm = c.pairmat + P->pm_off;
   const double *rl2 = c.rlist2 + P->pair_off;
@@ -1168,9 +1186,12 @@ __device__ __forceinline__ void build_atom(const DevCtx &c, int sys, int local, 
   int *col = c.nbr + P->nbr_off + (long long)(local / TILE) * maxnb * TILE + (local % TILE);
   const unsigned below = (1u << lane) - 1u;
   int cnt = 0;
-  for (int e = 0; e < ne; ++e) {
+  for (unsigned hd = heads; hd;) {
+    const int e = __ffs(hd) - 1;
+    hd &= hd - 1;
+    const int last = hd ? __ffs(hd) - 2 : ne - 1;
     const bool center = __shfl_sync(0xffffffffu, e_center, e) != 0;
-    const int q1 = __shfl_sync(0xffffffffu, e_q1, e);
+    const int q1 = __shfl_sync(0xffffffffu, e_q1, last);
     for (int qb = __shfl_sync(0xffffffffu, e_q0, e); qb < q1; qb += 32) {
       const int qq = qb + lane;
       const int j = aoff + qq;
