@@ -965,6 +965,11 @@ __device__ __forceinline__ int wrap_step(int x, int d, int M) {
   return y < 0 ? y + M : (y >= M ? y - M : y);
 }
 
+template <bool B>
+struct BoolTag {
+  static constexpr bool value = B;
+};
+
 // Stencil entries whose candidate ranges follow one another in memory (an
 // entry's first candidate right after the previous entry's last: the cells
 // of one row of the stencil, or a left-out or empty range between them)
@@ -1186,59 +1191,74 @@ __device__ __forceinline__ void build_atom(const DevCtx &c, int sys, int local, 
   int *col = c.nbr + P->nbr_off + (long long)(local / TILE) * maxnb * TILE + (local % TILE);
   const unsigned below = (1u << lane) - 1u;
   int cnt = 0;
-  for (unsigned hd = heads; hd;) {
-    const int e = __ffs(hd) - 1;
-    hd &= hd - 1;
-    const int last = hd ? __ffs(hd) - 2 : ne - 1;
-    const bool center = __shfl_sync(0xffffffffu, e_center, e) != 0;
-    const int q1 = __shfl_sync(0xffffffffu, e_q1, last);
-    for (int qb = __shfl_sync(0xffffffffu, e_q0, e); qb < q1; qb += 32) {
-      const int qq = qb + lane;
-      const int j = aoff + qq;
-      const bool have = qq < q1;
-      const int4 pj = c.pfx[have ? j : i];
-      int mx = 1;
-      if (!one) {
-        const int tj = tw_type(pj.w);
-        const int a = pm[(ti - 1) + (tj - 1) * nt], b = pm[(tj - 1) + (ti - 1) * nt];
-        mx = a > b ? a : b;
-      }
-      const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * sb0;
-      const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * sb1;
-      const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * sb2;
-      // (FMAs: the FP32 rounding stays far inside the 1e-5 band)
-      const float d2f = __fmaf_rn(r0, r0, __fmaf_rn(r1, r1, __fmul_rn(r2, r2)));
-      const bool live = have && j != i && mx > 0;
-      float2 band = band1;
-      if (!one && live) {
-        const float rf = (float)rl2[mx - 1];
-        band = make_float2(rf * (1.f - NB_MARGIN), rf * (1.f + NB_MARGIN));
-      }
-      // outside both margins FP32 decides; inside either, FP64 does
-      bool hit = live && d2f < band.x && !(center && d2f < ptrhi);
-      const bool unsure = live && ((d2f >= band.x && d2f <= band.y) ||
-                                   (center && d2f >= ptrlo && d2f <= ptrhi));
-      if (__any_sync(0xffffffffu, unsure) && unsure) {
-        // the reference's FP64 test (src/nd.f90:1362-1377, 1419-1420)
-        const double4 pid = c.pos[i], pjd = c.pos[j];
-        double s0 = pid.x - pjd.x, s1 = pid.y - pjd.y, s2 = pid.z - pjd.z;
-        s0 = s0 - round(s0);
-        s1 = s1 - round(s1);
-        s2 = s2 - round(s2);
-        const double x0 = S->box[0] * s0, x1 = S->box[1] * s1, x2 = S->box[2] * s2;
-        double d2 = x0 * x0;
-        d2 = d2 + x1 * x1;
-        d2 = d2 + x2 * x2;
-        hit = !(center && d2 < P->ptrmin) && !(d2 > rl2[mx - 1]);
-      }
-      const unsigned bal = __ballot_sync(0xffffffffu, hit);
-      if (hit) {
-        const int k = cnt + __popc(bal & below);
-        if (k < maxnb) list_store(col, nb16, aoff, k, j);
-      }
-      cnt += __popc(bal);
+  // one pass of 32 candidates [qb, qb + 32) of a range ending at q1; only
+  // the own cell (CEN) tests PTrMin and holds the atom itself (the other
+  // entries are other cells), and a system of one type and one pair (ONE)
+  // takes no pair-matrix lookup
+  auto pass = [&](auto cen, auto onet, int qb, int q1) {
+    constexpr bool CEN = decltype(cen)::value, ONE = decltype(onet)::value;
+    const int qq = qb + lane;
+    const int j = aoff + qq;
+    const bool have = qq < q1;
+    const int4 pj = c.pfx[have ? j : i];
+    int mx = 1;
+    if (!ONE) {
+      const int tj = tw_type(pj.w);
+      const int a = pm[(ti - 1) + (tj - 1) * nt], b = pm[(tj - 1) + (ti - 1) * nt];
+      mx = a > b ? a : b;
     }
-  }
+    const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * sb0;
+    const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * sb1;
+    const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * sb2;
+    // (FMAs: the FP32 rounding stays far inside the 1e-5 band)
+    const float d2f = __fmaf_rn(r0, r0, __fmaf_rn(r1, r1, __fmul_rn(r2, r2)));
+    const bool live = have && (!CEN || j != i) && (ONE || mx > 0);
+    float2 band = band1;
+    if (!ONE && live) {
+      const float rf = (float)rl2[mx - 1];
+      band = make_float2(rf * (1.f - NB_MARGIN), rf * (1.f + NB_MARGIN));
+    }
+    // outside both margins FP32 decides; inside either, FP64 does
+    bool hit = live && d2f < band.x && !(CEN && d2f < ptrhi);
+    const bool unsure = live && ((d2f >= band.x && d2f <= band.y) ||
+                                 (CEN && d2f >= ptrlo && d2f <= ptrhi));
+    if (__any_sync(0xffffffffu, unsure) && unsure) {
+      // the reference's FP64 test (src/nd.f90:1362-1377, 1419-1420)
+      const double4 pid = c.pos[i], pjd = c.pos[j];
+      double s0 = pid.x - pjd.x, s1 = pid.y - pjd.y, s2 = pid.z - pjd.z;
+      s0 = s0 - round(s0);
+      s1 = s1 - round(s1);
+      s2 = s2 - round(s2);
+      const double x0 = S->box[0] * s0, x1 = S->box[1] * s1, x2 = S->box[2] * s2;
+      double d2 = x0 * x0;
+      d2 = d2 + x1 * x1;
+      d2 = d2 + x2 * x2;
+      hit = !(CEN && d2 < P->ptrmin) && !(d2 > rl2[mx - 1]);
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, hit);
+    if (hit) {
+      const int k = cnt + __popc(bal & below);
+      if (k < maxnb) list_store(col, nb16, aoff, k, j);
+    }
+    cnt += __popc(bal);
+  };
+  auto ranges = [&](auto onet) {
+    for (unsigned hd = heads; hd;) {
+      const int e = __ffs(hd) - 1;
+      hd &= hd - 1;
+      const int last = hd ? __ffs(hd) - 2 : ne - 1;
+      const bool center = __shfl_sync(0xffffffffu, e_center, e) != 0;
+      const int q0 = __shfl_sync(0xffffffffu, e_q0, e), q1 = __shfl_sync(0xffffffffu, e_q1, last);
+      if (center)
+        for (int qb = q0; qb < q1; qb += 32) pass(BoolTag<true>{}, onet, qb, q1);
+      else
+        for (int qb = q0; qb < q1; qb += 32) pass(BoolTag<false>{}, onet, qb, q1);
+    }
+  };
+  if (one)
+    ranges(BoolTag<true>{});
+  else
+    ranges(BoolTag<false>{});
   if (lane == 0) {
     c.nnb[i] = cnt;
     if (cnt > maxnb) set_err(c, S, E_NEIMAX);
