@@ -1039,77 +1039,91 @@ __device__ __forceinline__ void build_cell(const DevCtx &c, int sys, int cell, i
               hz = __reduce_max_sync(0xffffffffu, own ? oz : INT_MIN);
     int *col = c.nbr + P->nbr_off + (long long)(li / TILE) * maxnb * TILE + (li % TILE);
     int cnt = 0;
-    for (unsigned hd = heads; hd;) {
-      const int e = __ffs(hd) - 1;
-      hd &= hd - 1;
-      const int last = hd ? __ffs(hd) - 2 : ne - 1;
-      const bool center = __shfl_sync(0xffffffffu, e_center, e) != 0;
-      const int q1 = __shfl_sync(0xffffffffu, e_q1, last);
-      for (int qb = __shfl_sync(0xffffffffu, e_q0, e); qb < q1; qb += 32) {
-        // 32 candidates at once, one per lane; the lanes test their own
-        // candidate against the own atoms' box, then the kept ones pass
-        // the warp in cell order
-        const int qq = qb + lane;
-        const bool have = qq < q1;
-        const int4 pc = c.pfx[aoff + (have ? qq : qb)];
-        bool keep = have;
-        if (prune && keep) {
-          const int dx = (int)((unsigned)pc.x - (unsigned)ax), dy = (int)((unsigned)pc.y - (unsigned)ay),
-                    dz = (int)((unsigned)pc.z - (unsigned)az);
-          const float gx = dx < lx ? (float)lx - (float)dx : (dx > hx ? (float)dx - (float)hx : 0.f);
-          const float gy = dy < ly ? (float)ly - (float)dy : (dy > hy ? (float)dy - (float)hy : 0.f);
-          const float gz = dz < lz ? (float)lz - (float)dz : (dz > hz ? (float)dz - (float)hz : 0.f);
-          const float d2b = (gx * sb0) * (gx * sb0) + (gy * sb1) * (gy * sb1) + (gz * sb2) * (gz * sb2);
-          keep = d2b <= rlbox;
+    // one pass of 32 candidates [qb, qb + 32) of a range ending at q1; only
+    // the own cell (CEN) tests PTrMin and holds the own atoms, and a system
+    // of one type and one pair (ONE) takes no pair-matrix lookup
+    auto pass = [&](auto cen, auto onet, int qb, int q1) {
+      constexpr bool CEN = decltype(cen)::value, ONE = decltype(onet)::value;
+      // 32 candidates at once, one per lane; the lanes test their own
+      // candidate against the own atoms' box, then the kept ones pass
+      // the warp in cell order
+      const int qq = qb + lane;
+      const bool have = qq < q1;
+      const int4 pc = c.pfx[aoff + (have ? qq : qb)];
+      bool keep = have;
+      if (prune && keep) {
+        const int dx = (int)((unsigned)pc.x - (unsigned)ax), dy = (int)((unsigned)pc.y - (unsigned)ay),
+                  dz = (int)((unsigned)pc.z - (unsigned)az);
+        const float gx = dx < lx ? (float)lx - (float)dx : (dx > hx ? (float)dx - (float)hx : 0.f);
+        const float gy = dy < ly ? (float)ly - (float)dy : (dy > hy ? (float)dy - (float)hy : 0.f);
+        const float gz = dz < lz ? (float)lz - (float)dz : (dz > hz ? (float)dz - (float)hz : 0.f);
+        const float d2b = (gx * sb0) * (gx * sb0) + (gy * sb1) * (gy * sb1) + (gz * sb2) * (gz * sb2);
+        keep = d2b <= rlbox;
+      }
+      unsigned m = __ballot_sync(0xffffffffu, keep);
+      while (m) {
+        const int k = __ffs(m) - 1;
+        m &= m - 1;
+        const int4 pj = make_int4(__shfl_sync(0xffffffffu, pc.x, k), __shfl_sync(0xffffffffu, pc.y, k),
+                                  __shfl_sync(0xffffffffu, pc.z, k), __shfl_sync(0xffffffffu, pc.w, k));
+        const int j = aoff + qb + k;
+        int mx = 1;
+        if (!ONE) {
+          const int tj = tw_type(pj.w);
+          const int a = pm[(ti - 1) + (tj - 1) * nt], b = pm[(tj - 1) + (ti - 1) * nt];
+          mx = a > b ? a : b;
         }
-        unsigned m = __ballot_sync(0xffffffffu, keep);
-        while (m) {
-          const int k = __ffs(m) - 1;
-          m &= m - 1;
-          const int4 pj = make_int4(__shfl_sync(0xffffffffu, pc.x, k), __shfl_sync(0xffffffffu, pc.y, k),
-                                    __shfl_sync(0xffffffffu, pc.z, k), __shfl_sync(0xffffffffu, pc.w, k));
-          const int j = aoff + qb + k;
-          int mx = 1;
-          if (!one) {
-            const int tj = tw_type(pj.w);
-            const int a = pm[(ti - 1) + (tj - 1) * nt], b = pm[(tj - 1) + (ti - 1) * nt];
-            mx = a > b ? a : b;
-          }
-          const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * sb0;
-          const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * sb1;
-          const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * sb2;
-          const float d2f = r0 * r0 + r1 * r1 + r2 * r2;
-          const bool live = own && j != i && mx > 0;
-          float2 band = band1;
-          if (!one && live) {
-            const float rf = (float)rl2[mx - 1];
-            band = make_float2(rf * (1.f - NB_MARGIN), rf * (1.f + NB_MARGIN));
-          }
-          // outside both margins FP32 decides; inside either, FP64 does
-          bool hit = live && d2f < band.x && !(center && d2f < ptrhi);
-          const bool unsure = live && ((d2f >= band.x && d2f <= band.y) ||
-                                       (center && d2f >= ptrlo && d2f <= ptrhi));
-          if (unsure) {
-            // the reference's FP64 test (src/nd.f90:1362-1377, 1419-1420),
-            // its operands read again on this rare path
-            const double4 pid = c.pos[i], pjd = c.pos[j];
-            double s0 = pid.x - pjd.x, s1 = pid.y - pjd.y, s2 = pid.z - pjd.z;
-            s0 = s0 - round(s0);
-            s1 = s1 - round(s1);
-            s2 = s2 - round(s2);
-            const double x0 = S->box[0] * s0, x1 = S->box[1] * s1, x2 = S->box[2] * s2;
-            double d2 = x0 * x0;
-            d2 = d2 + x1 * x1;
-            d2 = d2 + x2 * x2;
-            hit = !(center && d2 < P->ptrmin) && !(d2 > rl2[mx - 1]);
-          }
-          if (hit) {
-            if (cnt < maxnb) list_store(col, nb16, aoff, cnt, j);
-            ++cnt;
-          }
+        const float r0 = (float)(int)((unsigned)pi.x - (unsigned)pj.x) * sb0;
+        const float r1 = (float)(int)((unsigned)pi.y - (unsigned)pj.y) * sb1;
+        const float r2 = (float)(int)((unsigned)pi.z - (unsigned)pj.z) * sb2;
+        const float d2f = r0 * r0 + r1 * r1 + r2 * r2;
+        const bool live = own && (!CEN || j != i) && (ONE || mx > 0);
+        float2 band = band1;
+        if (!ONE && live) {
+          const float rf = (float)rl2[mx - 1];
+          band = make_float2(rf * (1.f - NB_MARGIN), rf * (1.f + NB_MARGIN));
+        }
+        // outside both margins FP32 decides; inside either, FP64 does
+        bool hit = live && d2f < band.x && !(CEN && d2f < ptrhi);
+        const bool unsure = live && ((d2f >= band.x && d2f <= band.y) ||
+                                     (CEN && d2f >= ptrlo && d2f <= ptrhi));
+        if (unsure) {
+          // the reference's FP64 test (src/nd.f90:1362-1377, 1419-1420),
+          // its operands read again on this rare path
+          const double4 pid = c.pos[i], pjd = c.pos[j];
+          double s0 = pid.x - pjd.x, s1 = pid.y - pjd.y, s2 = pid.z - pjd.z;
+          s0 = s0 - round(s0);
+          s1 = s1 - round(s1);
+          s2 = s2 - round(s2);
+          const double x0 = S->box[0] * s0, x1 = S->box[1] * s1, x2 = S->box[2] * s2;
+          double d2 = x0 * x0;
+          d2 = d2 + x1 * x1;
+          d2 = d2 + x2 * x2;
+          hit = !(CEN && d2 < P->ptrmin) && !(d2 > rl2[mx - 1]);
+        }
+        if (hit) {
+          if (cnt < maxnb) list_store(col, nb16, aoff, cnt, j);
+          ++cnt;
         }
       }
-    }
+    };
+    auto ranges = [&](auto onet) {
+      for (unsigned hd = heads; hd;) {
+        const int e = __ffs(hd) - 1;
+        hd &= hd - 1;
+        const int last = hd ? __ffs(hd) - 2 : ne - 1;
+        const bool center = __shfl_sync(0xffffffffu, e_center, e) != 0;
+        const int q0 = __shfl_sync(0xffffffffu, e_q0, e), q1 = __shfl_sync(0xffffffffu, e_q1, last);
+        if (center)
+          for (int qb = q0; qb < q1; qb += 32) pass(BoolTag<true>{}, onet, qb, q1);
+        else
+          for (int qb = q0; qb < q1; qb += 32) pass(BoolTag<false>{}, onet, qb, q1);
+      }
+    };
+    if (one)
+      ranges(BoolTag<true>{});
+    else
+      ranges(BoolTag<false>{});
     if (own) {
       c.nnb[aoff + li] = cnt;
       if (cnt > maxnb) set_err(c, S, E_NEIMAX);
