@@ -1208,9 +1208,9 @@ __device__ __forceinline__ void build_atom(const DevCtx &c, int sys, int local, 
   // one pass of 32 candidates [qb, qb + 32) of a range ending at q1; only
   // the own cell (CEN) tests PTrMin and holds the atom itself (the other
   // entries are other cells), and a system of one type and one pair (ONE)
-  // takes no pair-matrix lookup
-  auto pass = [&](auto cen, auto onet, int qb, int q1) {
-    constexpr bool CEN = decltype(cen)::value, ONE = decltype(onet)::value;
+  // takes no pair-matrix lookup; NB16: the list's 16-bit entries
+  auto pass = [&](auto cen, auto onet, auto nbt, int qb, int q1) {
+    constexpr bool CEN = decltype(cen)::value, ONE = decltype(onet)::value, NB16 = decltype(nbt)::value;
     const int qq = qb + lane;
     const int j = aoff + qq;
     const bool have = qq < q1;
@@ -1252,11 +1252,11 @@ __device__ __forceinline__ void build_atom(const DevCtx &c, int sys, int local, 
     const unsigned bal = __ballot_sync(0xffffffffu, hit);
     if (hit) {
       const int k = cnt + __popc(bal & below);
-      if (k < maxnb) list_store(col, nb16, aoff, k, j);
+      if (k < maxnb) list_store(col, NB16, aoff, k, j);
     }
     cnt += __popc(bal);
   };
-  auto ranges = [&](auto onet) {
+  auto ranges = [&](auto onet, auto nbt) {
     for (unsigned hd = heads; hd;) {
       const int e = __ffs(hd) - 1;
       hd &= hd - 1;
@@ -1264,15 +1264,22 @@ __device__ __forceinline__ void build_atom(const DevCtx &c, int sys, int local, 
       const bool center = __shfl_sync(0xffffffffu, e_center, e) != 0;
       const int q0 = __shfl_sync(0xffffffffu, e_q0, e), q1 = __shfl_sync(0xffffffffu, e_q1, last);
       if (center)
-        for (int qb = q0; qb < q1; qb += 32) pass(BoolTag<true>{}, onet, qb, q1);
+        for (int qb = q0; qb < q1; qb += 32) pass(BoolTag<true>{}, onet, nbt, qb, q1);
       else
-        for (int qb = q0; qb < q1; qb += 32) pass(BoolTag<false>{}, onet, qb, q1);
+        for (int qb = q0; qb < q1; qb += 32) pass(BoolTag<false>{}, onet, nbt, qb, q1);
     }
   };
-  if (one)
-    ranges(BoolTag<true>{});
-  else
-    ranges(BoolTag<false>{});
+  if (one) {
+    if (nb16)
+      ranges(BoolTag<true>{}, BoolTag<true>{});
+    else
+      ranges(BoolTag<true>{}, BoolTag<false>{});
+  } else {
+    if (nb16)
+      ranges(BoolTag<false>{}, BoolTag<true>{});
+    else
+      ranges(BoolTag<false>{}, BoolTag<false>{});
+  }
   if (lane == 0) {
     c.nnb[i] = cnt;
     if (cnt > maxnb) set_err(c, S, E_NEIMAX);
