@@ -260,9 +260,10 @@ int ndg_get_neighbor_count(ndg_ctx *ctx, int sys, long long *entries);
  * loading the library keeps until the process exits.  Limits: 32768 atoms,
  * 32768 link cells, 8 types, 36 pairs; larger inputs return NDG_ERR_ARG
  * with a message on stderr.  The first call on each device looks up the
- * array's device address (cudaGetSymbolAddress), so make that first call
- * before capturing a stream.  All calls share the array: calls that overlap
- * on the GPU (other streams or threads) corrupt each other; order them. */
+ * array's device address (cudaGetSymbolAddress).  The call waits for its
+ * stream, so it cannot be recorded into a CUDA graph by stream capture.
+ * All calls share the array: calls that overlap on the GPU (other streams
+ * or threads) corrupt each other; order them. */
 int ndg_compute0_static(int np, int ntypes, int npairs, int ptsize, double ptrmin,
                         const int *pairmat, const double *rcpair, double skin,
                         int quirk, const double *box, const double *fpair_d,
