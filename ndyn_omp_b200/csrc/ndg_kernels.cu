@@ -7,7 +7,7 @@
 //
 // Kernels of one MD step (src/nd.f90:137-178), all systems in one launch:
 //   [rebuild]  k_bin -> k_scan -> k_scatter -> k_order -> k_permute ->
-//              k_copyback -> k_build_atoms | k_build_cells -> k_tile_rows
+//              k_copyback -> k_build_atoms | k_build_cells
 //              [-> k_neimax]                (only systems whose check fired)
 //   k_integrate1                           (integrate1 + pending mkIso* scales;
 //                                           one more block plans the pair
@@ -51,6 +51,16 @@ __device__ __forceinline__ void list_store(int *col, int nb16, int atom_off, int
 // 32-bit words a tile's list of `rows` rows occupies
 __device__ __forceinline__ int list_words(int rows, int nb16) {
   return nb16 ? (rows + 1) >> 1 : rows;
+}
+
+// An atom's list has landed: its tile's rows (the tile's longest list,
+// capped at maxnb; the pair kernel's L2 prefetch size) and the system's sum
+// of them (the work plan's list-length measure) follow it.  atomicMax
+// returns the tile's previous maximum, so the increments added to the sum
+// add up to the final maximum of every tile, whatever the order.
+__device__ __forceinline__ void note_rows(const DevCtx &c, SysState *S, int i, int r) {
+  const int old = atomicMax(c.tile_rows + i / TILE, r);
+  if (r > old) atomicAdd(&S->rows, (unsigned long long)(r - old));
 }
 
 // record an error on the system and in the context-wide error word
@@ -1127,6 +1137,7 @@ __device__ __forceinline__ void build_cell(const DevCtx &c, int sys, int cell, i
     if (own) {
       c.nnb[aoff + li] = cnt;
       if (cnt > maxnb) set_err(c, S, E_NEIMAX);
+      note_rows(c, S, aoff + li, min(cnt, maxnb));
     }
   }
 }
@@ -1283,6 +1294,7 @@ __device__ __forceinline__ void build_atom(const DevCtx &c, int sys, int local, 
   if (lane == 0) {
     c.nnb[i] = cnt;
     if (cnt > maxnb) set_err(c, S, E_NEIMAX);
+    note_rows(c, S, i, min(cnt, maxnb));
   }
 }
 
@@ -1355,32 +1367,6 @@ __global__ __launch_bounds__(CB_THREADS, 3) void k_build_cells(DevCtx c) {
       build_cell(c, l_sys[lo], u - l_pre[lo], lane);
     }
   }
-}
-
-// each rebuilt tile's row count (its longest list, for the pair kernel's L2
-// prefetch) and the system's sum of them (the work plan's tile cost)
-__global__ __launch_bounds__(TILE) void k_tile_rows(DevCtx c) {
-  __shared__ int wmax[TILE / 32];
-  for_listed(c,
-             [&](int s, int &f, int &n) {
-               f = c.P[s].atom_off / TILE;
-               n = c.P[s].npad / TILE;
-             },
-             [&](int s, int tile) {
-               const SysParam *P = c.P + s;
-               const int i = tile * TILE + threadIdx.x;
-               int r = i - P->atom_off < P->n ? min(c.nnb[i], P->maxnb) : 0;
-               r = __reduce_max_sync(0xffffffffu, r);
-               if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = r;
-               __syncthreads();
-               if (threadIdx.x == 0) {
-                 int rows = 0;
-                 for (int w = 0; w < TILE / 32; ++w) rows = max(rows, wmax[w]);
-                 c.tile_rows[tile] = rows;
-                 atomicAdd(&c.S[s].rows, (unsigned long long)rows);
-               }
-               __syncthreads();
-             });
 }
 
 // ---------------------------------------------------------------------------
@@ -2513,7 +2499,6 @@ void launch_rebuild(const DevCtx &c, cudaStream_t st, int counting, int mixed) {
     gcb = nsm * (occ > 0 ? occ : 1);
   }
   k_build_cells<<<gcb, CB_THREADS, 0, st>>>(c);
-  k_tile_rows<<<std::min(c.nchunks * (ATOM_ALIGN / TILE), nsm * 8), TILE, 0, st>>>(c);
   if (c.any_neimax) k_neimax<<<gchunk, BLOCK, 0, st>>>(c);
 }
 
