@@ -748,10 +748,11 @@ def main():
         "serving": serving,
         "list_rebuilds_in_timed_region": rebuilds,
         # per step integrate1 (with the work plan) and the two pair kernels; per
-        # graph block k_begin_block and k_decide; the 7 rebuild kernels on
-        # steps whose conditional node fires (at most one per step, at most
-        # one per list update)
-        "gpu_launches": 3 * args.steps + 2 * -(-args.steps // gsteps) + 7 * min(args.steps, rebuilds),
+        # graph block k_begin_block and k_decide; the 8 rebuild kernels (the
+        # six of the counting sort and both forms of the list build) on steps
+        # whose conditional node fires (at most one per step, at most one per
+        # list update)
+        "gpu_launches": 3 * args.steps + 2 * -(-args.steps // gsteps) + 8 * min(args.steps, rebuilds),
         "clocks": clocks,
         "roofline": roof,
         "cpu_baseline": cpu,
