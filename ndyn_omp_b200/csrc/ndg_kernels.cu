@@ -1334,7 +1334,7 @@ __global__ __launch_bounds__(CB_THREADS, 4) void k_build_atoms(DevCtx c) {
 }
 
 // the listed systems' cells, dealt round-robin to every warp of the grid
-__global__ __launch_bounds__(CB_THREADS, 3) void k_build_cells(DevCtx c) {
+__global__ __launch_bounds__(CB_THREADS, 4) void k_build_cells(DevCtx c) {
   __shared__ int l_sys[LIST_STAGE], l_pre[LIST_STAGE + 1];
   __shared__ int wsum[CB_THREADS / 32];
   static_assert(CB_THREADS == LIST_STAGE, "one listed system per thread when staging");
